@@ -1,0 +1,336 @@
+"""Benchmark of the CUDA-RP simulation path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload axisym_1024x2048|axisym_256x512] [--chunk S] [--preroll P]
+
+One bench step is S mixture time steps (default 100, one save interval of the
+workload) of the full hot path: fused FDTD/PML update, bubble motion and
+binning, and every Picard iteration of Rayleigh-Plesset + void-fraction
+gather + pressure re-evaluation the step needs.  The timed window starts after
+P untimed mixture steps (default: the burst has reached the bubble cloud) plus
+W untimed bench steps, so it measures the driven regime.  The state (about
+200 MB at 1024 x 2048) is larger than L2, so no flush is needed between steps.
+
+metric: Mcell-upd/s — interior cells x mixture steps / device time (CUDA events
+on the simulation's stream, max over ranks).  Also reported: bubble-steps/s,
+the roofline of the fused FDTD kernel, a bounded CPU-oracle baseline and the
+error of the GPU state against the FP64 oracle on that sample, an end-to-end
+number through the C ABI with host buffers, clocks sampled during the timed
+region.
+
+Multi-GPU (--gpus N under torchrun): independent replicas, one per GPU, no
+data-path collective ("replicas only": the simulation does not shard across
+GPUs here); value = all ranks' cell updates / max rank time.
+
+--impl reference: the reference simulator has no CPU implementation (its
+simulation is CUDA-only), so the reference arm times the FP64 host oracle —
+the restatement of the reference's kernels — on all host cores, each bench
+step one mixture step of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "cuda-rp_b200")
+sys.path[:0] = [PKG, os.path.join(ROOT, "tests")]
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    "axisym_1024x2048": os.path.join(PKG, "configs", "axisym_1024x2048.conf"),
+    "axisym_256x512": os.path.join(PKG, "configs", "axisym_256x512.conf"),
+}
+# Mixture steps before the burst's leading edge reaches the bubble cloud
+# (about (focus depth - cloud half length - source row depth) / c / dt).
+PREROLL = {"axisym_1024x2048": 1200, "axisym_256x512": 250}
+BYTES_PER_CELL_FP64 = 96  # compulsory traffic of the fused FDTD pass
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="axisym_1024x2048", choices=list(WORKLOADS))
+    ap.add_argument("--chunk", type=int, default=100)
+    ap.add_argument("--preroll", type=int, default=None)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[0]))
+                smax.append(float(s[1]))
+                for n, v in zip(names, s[4:8]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+def load_workload(name):
+    import crp
+
+    cfg = crp.parse_file(WORKLOADS[name])
+    bub = crp.seed_bubbles(cfg) if cfg.ext_bubble_count > 0 else None
+    return cfg, bub
+
+
+def cpu_baseline(cfg, bub, seconds, threads):
+    """Oracle on the host cores: returns (cell-updates/s, steps, wall s, oracle sim)."""
+    import _bind as B
+
+    o = B.OracleSim(cfg, bub, threads=threads)
+    t0 = time.perf_counter()
+    o.step(1)
+    t1 = time.perf_counter()
+    n = max(1, min(200, int(seconds / max(t1 - t0, 1e-6))))
+    t2 = time.perf_counter()
+    o.step(n)
+    t3 = time.perf_counter()
+    rate = cfg.grid_x * cfg.grid_y * n / (t3 - t2)
+    return rate, n + 1, t3 - t2, o
+
+
+def oracle_error(gpu_sim_factory, oracle, steps):
+    """Relative errors of a fresh GPU run of `steps` steps against the oracle state."""
+    with gpu_sim_factory() as g:
+        g.step(steps)
+        out = {}
+        for k in ("p0", "vx", "vy", "f_g"):
+            a, b = g.field(k), oracle.field(k)
+            nrm = np.linalg.norm(b)
+            out[k] = {"rel_l2": float(np.linalg.norm(a - b) / nrm) if nrm > 0 else float(np.linalg.norm(a)),
+                      "rel_max": float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))}
+        if g.dims.num_bubbles:
+            a, b = g.bubbles("R_t"), oracle.bubbles("R_t")
+            out["R_t"] = {"rel_l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+                          "rel_max": float(np.abs(a - b).max() / np.abs(b).max())}
+        out["steps"] = steps
+        return out
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the host oracle on all cores, one mixture step per bench step."""
+    if rank != 0:
+        return None
+    import _bind as B
+
+    cfg, bub = load_workload(args.workload)
+    threads = os.cpu_count() or 1
+    o = B.OracleSim(cfg, bub, threads=threads)
+    for _ in range(args.warmup):
+        o.step(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step(1)
+    dt = time.perf_counter() - t0
+    cells = cfg.grid_x * cfg.grid_y
+    value = cells * args.steps / dt / 1e6
+    return {
+        "impl": "reference", "metric": "Mcell-upd/s", "value": value, "unit": "Mcell-upd/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bubbles)",
+        "config": {"workload": args.workload, "grid": [cfg.grid_x, cfg.grid_y], "bubbles": o.dims.num_bubbles,
+                   "mixture_steps_per_step": 1, "start": "t=0"},
+        "bubble_steps_per_s": o.dims.num_bubbles * args.steps / dt,
+        "cpu_baseline": {"value": value, "unit": "Mcell-upd/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.warmup}+{args.steps} mixture steps of {args.workload} from t=0"},
+        "e2e": {"value": value, "unit": "Mcell-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def run_ours(args, rank, world, dist):
+    import torch
+
+    import crp
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    cfg, bub = load_workload(args.workload)
+    cells = cfg.grid_x * cfg.grid_y
+    preroll = PREROLL[args.workload] if args.preroll is None else args.preroll
+    S = args.chunk
+
+    sim = crp.Sim(cfg, bub)
+    nb = sim.dims.num_bubbles
+    stream = torch.cuda.ExternalStream(sim.stream)
+    sim.step(preroll)
+    for _ in range(args.warmup):
+        sim.step(S)
+    s0 = sim.stats()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            sim.step(S)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    s1 = sim.stats()
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    mix_steps = args.steps * S
+    value = cells * mix_steps * world / (ms * 1e-3) / 1e6
+    launches = s1.kernel_launches - s0.kernel_launches
+    picard = s1.picard_total - s0.picard_total
+
+    # Roofline of the fused FDTD kernel: device time per launch from profiling events.
+    sim.set_profiling(True)
+    p0 = sim.stats()
+    sim.step(S)
+    p1 = sim.stats()
+    sim.set_profiling(False)
+    n_fdtd = p1.fdtd_launches - p0.fdtd_launches
+    fdtd_ms = (p1.ms_fdtd - p0.ms_fdtd) / max(n_fdtd, 1)
+    prof = {k: (getattr(p1, k) - getattr(p0, k)) for k in ("ms_fdtd", "ms_rp", "ms_couple", "ms_other")}
+    hbm, kind = peaks()
+    achieved = BYTES_PER_CELL_FP64 * cells / (fdtd_ms * 1e-3) / 1e9
+    result = None
+    if rank == 0:
+        result = {
+            "metric": "Mcell-upd/s", "value": value, "unit": "Mcell-upd/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bubbles, Philox-4x32-10)",
+            "config": {"workload": args.workload, "grid": [cfg.grid_x, cfg.grid_y], "bubbles": nb,
+                       "mixture_steps_per_step": S, "preroll_steps": preroll, "precision": "fp64",
+                       "parallelism": f"replicas x{world}", "l2": "state > L2 (no flush needed)"},
+            "bubble_steps_per_s": nb * mix_steps * world / (ms * 1e-3),
+            "picard_iterations_per_step": picard / mix_steps,
+            "gpu_launches": int(launches),
+            "roofline": {"kernel": "fdtd_step", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_kind": kind, "traffic": None,
+                         "bytes_per_cell": BYTES_PER_CELL_FP64, "ms_per_launch": fdtd_ms},
+            "kernel_ms_per_chunk": prof,
+            "clocks": clk.summary(),
+        }
+    sim.close()
+
+    # End to end through the C ABI: host inputs in, host rawdata arrays out.
+    if rank == 0 and not args.no_e2e:
+        t0 = time.perf_counter()
+        e2e_steps = 0
+        with crp.Sim(cfg, bub) as s2:
+            d = s2.dims
+            h2d = 4 * 8 * nb
+            for _ in range(args.steps):
+                s2.step(S)
+                e2e_steps += S
+                s2.field("p0")
+                s2.bubbles("R_t")
+        wall = time.perf_counter() - t0
+        result["e2e"] = {"value": cells * e2e_steps / wall / 1e6, "unit": "Mcell-upd/s",
+                         "h2d_bytes_per_step": h2d // max(args.steps, 1),
+                         "d2h_bytes_per_step": 8 * (d.i1m * d.j1m + nb),
+                         "note": "wall clock: crp_create (seeded bubbles uploaded) + steps from t=0 + p0 and R_t "
+                                 "read back every bench step"}
+
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, n, wall, oracle = cpu_baseline(cfg, bub, args.cpu_seconds, threads)
+        result["cpu_baseline"] = {"value": rate / 1e6, "unit": "Mcell-upd/s", "cores": threads, "kind": "port",
+                                  "sample": f"{n} mixture steps of {args.workload} from t=0 "
+                                            f"({wall:.1f} s, OpenMP)"}
+        result["oracle_error"] = oracle_error(lambda: crp.Sim(cfg, bub), oracle, n)
+    return result
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    dist = None
+    if args.impl == "reference":
+        # The CPU reference arm runs on rank 0 only; other ranks exit without work.
+        res = run_reference(args, rank, world)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    try:
+        res = run_ours(args, rank, world, dist)
+        if rank == 0 and res is not None:
+            print(json.dumps(res), flush=True)
+    finally:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,213 @@
+// `bubbles <conf>`: the reference program's command line (src/bubbles.cpp:18-310)
+// on top of the crp C ABI.
+//
+//   bubbles [-h|--help] [--help-all] [-a|--ascii] [-s|--sph] [-d|--directory DIR] <input-file>
+//
+// Same options, configuration keys, defaults, output directory (./rawdata/),
+// rawdata files and *_minmax.txt / runtime.txt.  Differences, all outside the
+// simulated path: the output directory is created if missing and never cleared
+// (the reference runs `rm -rf` on it); SPH files, T_step files, the focal-point
+// tracker files and the PID passes are not produced (the run uses a fixed focus).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <filesystem>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "crp.h"
+
+namespace {
+
+const char* kHelp =
+    "Options:\n\n"
+    "Command line options:\n"
+    "  -h [ --help ]                         Output this help message.\n"
+    "  --help-all                            Output a complete list of options.\n\n"
+    "Generic options:\n"
+    "  -a [ --ascii ]                        Save plaintext files.\n"
+    "  -s [ --sph ]                          Save sph files. This option has\n"
+    "                                        precedence over --ascii.\n"
+    "  -d [ --directory ] arg (=./rawdata/)  Save into a target directory.\n";
+
+const char* kFileKeys =
+    "\nConfiguration file options:\n"
+    "  grid.x grid.y grid.lx grid.ly\n"
+    "  pml.x0 pml.x1 pml.y0 pml.y1 pml.grid_number pml.sigma pml.order\n"
+    "  simulation.cfl simulation.dt0 simulation.n_step_max simulation.t_step_max\n"
+    "  simulation.save_interval simulation.order simulation.smooth_delta_band\n"
+    "  transducer.amp transducer.freq transducer.focal_dist transducer.pid\n"
+    "  transducer.pid_start_step transducer.init_control transducer.pid_iterate\n"
+    "  transducer.box_size transducer.cylindrical transducer.on_wave transducer.off_wave\n"
+    "  transducer.transducer_v transducer.transducer_p transducer.focused_wave_v\n"
+    "  transducer.focused_wave_p\n"
+    "  bubbles.enable bubbles.fg0 bubbles.R0 bubbles.P0 bubbles.T0 bubbles.gamma\n"
+    "  bubbles.liquid_surface_tension bubbles.liquid_viscosity bubbles.liquid_density bubbles.K0\n"
+    "  debug.display_dim debug.fg debug.fg_min debug.fg_max debug.T debug.T_min debug.T_max\n"
+    "  debug.p debug.p_max debug.v debug.v_min debug.v_max debug.bubbles\n"
+    "  ext.rho_inf ext.c_inf ext.p_inf ext.source_row ext.ramp_cycles ext.precision\n"
+    "  ext.picard_cap ext.rp_step_cap ext.bubble_count ext.bubble_seed ext.r0_sigma_ln\n"
+    "  ext.cloud_shape ext.cloud_r ext.cloud_h ext.n_b\n";
+
+// Optional overrides of the *_minmax.txt values (src/bubbles.cpp:275-294).  The
+// reference registers the p_min key as "debug p_min" (a typo), so only
+// debug.fg_min, debug.fg_max and debug.p_max can take effect.
+bool lookup_key(const std::string& path, const std::string& full, double* out) {
+  std::ifstream in(path);
+  std::string line, section;
+  while (std::getline(in, line)) {
+    size_t h = line.find('#');
+    if (h != std::string::npos) line = line.substr(0, h);
+    size_t a = line.find_first_not_of(" \t\r"), b = line.find_last_not_of(" \t\r");
+    if (a == std::string::npos) continue;
+    line = line.substr(a, b - a + 1);
+    if (line[0] == '[' && line.back() == ']') {
+      section = line.substr(1, line.size() - 2);
+      continue;
+    }
+    size_t eq = line.find('=');
+    if (eq == std::string::npos) continue;
+    std::string k = line.substr(0, eq), v = line.substr(eq + 1);
+    k = k.substr(0, k.find_last_not_of(" \t") + 1);
+    v = v.substr(v.find_first_not_of(" \t") == std::string::npos ? v.size() : v.find_first_not_of(" \t"));
+    if ((section.empty() ? k : section + "." + k) == full) {
+      *out = std::strtod(v.c_str(), nullptr);
+      return true;
+    }
+  }
+  return false;
+}
+
+void write_minmax(const std::string& path, double lo, double hi) {
+  std::ofstream f(path.c_str());
+  f << lo << std::endl << hi << std::endl;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  time_t start_time = time(nullptr);
+  std::string in_file, target_dir = "./rawdata/";
+  bool ascii = false, sph = false;
+  for (int k = 1; k < argc; k++) {
+    std::string a = argv[k];
+    if (a == "-h" || a == "--help") {
+      std::cout << kHelp << std::endl;
+      return 0;
+    }
+    if (a == "--help-all") {
+      std::cout << kHelp << kFileKeys << std::endl;
+      return 0;
+    }
+    if (a == "-a" || a == "--ascii") {
+      ascii = true;
+    } else if (a == "-s" || a == "--sph") {
+      sph = true;
+    } else if (a == "-d" || a == "--directory") {
+      if (k + 1 >= argc) {
+        std::cerr << "the required argument for option '--directory' is missing" << std::endl;
+        return 1;
+      }
+      target_dir = argv[++k];
+    } else if (a.rfind("--directory=", 0) == 0) {
+      target_dir = a.substr(12);
+    } else if (!a.empty() && a[0] == '-') {
+      // unregistered options are ignored (allow_unregistered)
+    } else if (in_file.empty()) {
+      in_file = a;
+    }
+  }
+  if (in_file.empty()) {
+    std::cout << "Please specify an input configuration file" << std::endl;
+    return 1;
+  }
+  if (target_dir.find_last_of('/') != target_dir.length() - 1) target_dir += "/";
+
+  crp_config cfg;
+  crp_config_defaults(&cfg);
+  char err[512] = {0};
+  crp_status st = crp_config_parse_file(in_file.c_str(), &cfg, err, sizeof(err));
+  if (st != CRP_OK) {
+    std::cerr << "error: " << (err[0] ? err : crp_status_string(st)) << std::endl;
+    return 1;
+  }
+  ascii = ascii || cfg.opt_ascii;
+  sph = sph || cfg.opt_sph;
+
+  std::cout << "Input file is " << in_file << std::endl;
+  std::cout << "Saving results to " << target_dir << std::endl;
+  std::cout << "Save format is " << (sph && !ascii ? "sph" : "ASCII plaintext");
+  std::cout << std::endl << std::endl;
+  if (sph) std::cout << "note: SPH output is not produced by this build; ASCII is written when -a is given" << std::endl;
+  if (cfg.tr_pid) std::cout << "note: the PID focal controller is not part of this build; the focus stays fixed" << std::endl;
+
+  std::error_code ec;
+  std::filesystem::create_directories(target_dir, ec);
+  if (ec) {
+    std::cerr << "error: cannot create " << target_dir << ": " << ec.message() << std::endl;
+    return 1;
+  }
+
+  crp_sim* sim = nullptr;
+  st = crp_create(&cfg, nullptr, nullptr, &sim);
+  if (st != CRP_OK) {
+    std::cerr << "error: " << crp_status_string(st) << std::endl;
+    return 1;
+  }
+  crp_stats stats;
+  int64_t nstep = 0;
+  double tstep = 0.0;
+  const int save = cfg.sim_save_interval > 0 ? cfg.sim_save_interval : 0;
+  while (((cfg.sim_n_step_max != 0) && (nstep < cfg.sim_n_step_max)) ||
+         ((cfg.sim_t_step_max != 0) && (tstep < cfg.sim_t_step_max))) {
+    st = crp_step(sim, 1);
+    if (st != CRP_OK) {
+      std::cerr << "\nerror at step " << nstep + 1 << ": " << crp_status_string(st) << ": " << crp_last_error(sim)
+                << std::endl;
+      crp_destroy(sim);
+      return 1;
+    }
+    crp_get_stats(sim, &stats);
+    nstep = stats.steps;
+    tstep = stats.time;
+    if (save && nstep % save == 0) {
+      if (ascii) {
+        st = crp_write_rawdata(sim, target_dir.c_str());
+        if (st != CRP_OK) {
+          std::cerr << "\nerror writing rawdata: " << crp_status_string(st) << std::endl;
+          crp_destroy(sim);
+          return 1;
+        }
+      }
+      if (cfg.sim_n_step_max != 0)
+        printf("\rRunning the simulation...\t\tnstep : %5lld / %i\t", (long long)nstep, cfg.sim_n_step_max);
+      else
+        printf("\rRunning the simulation...\t\ttstep : %4.2E / %4.2E\t", tstep, cfg.sim_t_step_max);
+      fflush(stdout);
+    }
+  }
+  printf("\rRunning the simulation...\t\tdone\n\n");
+
+  // *_minmax.txt (src/bubbles.cpp:273-296) for the fields written above.
+  double fg_min = 1e10, fg_max = -1e10, p0_min = 1e10, p0_max = -1e10;
+  crp_minmax(sim, &fg_min, &fg_max, &p0_min, &p0_max);
+  double v;
+  if (cfg.dbg_p) {
+    if (lookup_key(in_file, "debug.p_max", &v)) p0_max = v;
+    write_minmax(target_dir + "p0_minmax.txt", p0_min, p0_max);
+  }
+  if (cfg.dbg_fg) {
+    if (lookup_key(in_file, "debug.fg_min", &v)) fg_min = v;
+    if (lookup_key(in_file, "debug.fg_max", &v)) fg_max = v;
+    write_minmax(target_dir + "fg_minmax.txt", fg_min, fg_max);
+  }
+  crp_destroy(sim);
+  std::cout << "The program took " << time(nullptr) - start_time << " seconds to run" << std::endl;
+  std::ofstream runtime((target_dir + "runtime.txt").c_str());
+  runtime << "Finished in " << time(nullptr) - start_time << " seconds" << std::endl;
+  return 0;
+}

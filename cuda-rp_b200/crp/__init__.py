@@ -1,0 +1,246 @@
+"""Python binding of the crp C ABI (include/crp.h), for tests and benchmarks.
+
+The simulation itself runs in the CUDA library ``libcrp.so`` built from
+``cuda-rp_b200/csrc``; this module only loads it with ctypes and converts
+arrays.  There is no Python or CPU fallback: if the library is missing,
+``load()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(_HERE)
+LIB_PATH = os.path.join(PKG_ROOT, "build", "libcrp.so")
+
+c_int = ctypes.c_int32
+c_dbl = ctypes.c_double
+
+
+class Config(ctypes.Structure):
+    """Mirror of struct crp_config."""
+
+    _fields_ = [
+        ("grid_x", c_int), ("grid_y", c_int), ("grid_lx", c_dbl), ("grid_ly", c_dbl),
+        ("pml_x0", c_int), ("pml_x1", c_int), ("pml_y0", c_int), ("pml_y1", c_int),
+        ("pml_grid_number", c_int), ("pml_sigma", c_dbl), ("pml_order", c_int),
+        ("sim_cfl", c_dbl), ("sim_dt0", c_dbl), ("sim_n_step_max", c_int), ("sim_t_step_max", c_dbl),
+        ("sim_save_interval", c_int), ("sim_order", c_int), ("sim_smooth_delta_band", c_int),
+        ("tr_amp", c_dbl), ("tr_freq", c_dbl), ("tr_focal_dist", c_dbl),
+        ("tr_pid", c_int), ("tr_pid_start_step", c_int), ("tr_init_control", c_dbl),
+        ("tr_pid_iterate", c_int), ("tr_box_size", c_dbl), ("tr_cylindrical", c_int),
+        ("tr_on_wave", c_int), ("tr_off_wave", c_int),
+        ("tr_plane_v", c_int), ("tr_plane_p", c_int), ("tr_focused_v", c_int), ("tr_focused_p", c_int),
+        ("bub_enable", c_int), ("bub_fg0", c_dbl), ("bub_R0", c_dbl), ("bub_P0", c_dbl),
+        ("bub_T0", c_dbl), ("bub_gamma", c_dbl), ("bub_sigma", c_dbl), ("bub_mu", c_dbl),
+        ("bub_rho", c_dbl), ("bub_K0", c_dbl),
+        ("dbg_display", c_int), ("dbg_fg", c_int), ("dbg_T", c_int), ("dbg_p", c_int),
+        ("dbg_v", c_int), ("dbg_bubbles", c_int),
+        ("opt_ascii", c_int), ("opt_sph", c_int),
+        ("ext_rho_inf", c_dbl), ("ext_c_inf", c_dbl), ("ext_p_inf", c_dbl),
+        ("ext_source_row", c_int), ("ext_ramp_cycles", c_dbl), ("ext_precision", c_int),
+        ("ext_picard_cap", c_int), ("ext_rp_step_cap", c_int), ("ext_bubble_count", c_int),
+        ("ext_bubble_seed", ctypes.c_uint64), ("ext_r0_sigma_ln", c_dbl), ("ext_cloud_shape", c_int),
+        ("ext_cloud_r", c_dbl), ("ext_cloud_h", c_dbl), ("ext_n_b", c_dbl),
+    ]
+
+
+class Dims(ctypes.Structure):
+    _fields_ = [("i1m", c_int), ("j1m", c_int), ("i2m", c_int), ("j2m", c_int), ("i2n", c_int),
+                ("j2n", c_int), ("num_bubbles", c_int), ("dx", c_dbl), ("dy", c_dbl), ("dt", c_dbl)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int64), ("time", c_dbl), ("picard_total", ctypes.c_int64),
+                ("picard_last", c_int), ("picard_max", c_int), ("rp_substeps_max", ctypes.c_int64),
+                ("residual_last", c_dbl), ("kernel_launches", ctypes.c_int64), ("fdtd_launches", ctypes.c_int64),
+                ("rp_launches", ctypes.c_int64), ("couple_launches", ctypes.c_int64),
+                ("ms_fdtd", c_dbl), ("ms_rp", c_dbl), ("ms_couple", c_dbl), ("ms_other", c_dbl)]
+
+
+class BubblesIn(ctypes.Structure):
+    _fields_ = [("n", c_int), ("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("r0", ctypes.c_void_p),
+                ("n_b", ctypes.c_void_p)]
+
+
+FIELDS = {"p0": 0, "px": 1, "py": 2, "pnx": 3, "pny": 4, "vx": 5, "vy": 6, "f_g": 7, "f_gn": 8,
+          "f_gm": 9, "rho_m": 10}
+BUBBLE_FIELDS = {"x": 0, "y": 1, "R_t": 2, "R_p": 3, "R_n": 4, "d1_R_p": 5, "PG_p": 6, "PL_p": 7,
+                 "PL_n": 8, "PL_m": 9, "dt": 10, "re": 11, "Q_B": 12, "n_B": 13, "R0": 14, "v_x": 15,
+                 "v_y": 16, "ibm_x": 17, "ibm_y": 18, "ibn_x": 19, "ibn_y": 20}
+
+
+class CrpError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"crp status {status}: {msg}")
+        self.status = status
+
+
+def field_shape(dims, name: str) -> tuple[int, int]:
+    """(height, width) of a field's dense array in the reference's layout."""
+    if name in ("p0", "px", "py", "pnx", "pny", "rho_m"):
+        return dims.j1m, dims.i1m
+    if name == "vx":
+        return dims.j2m, dims.i2n
+    if name == "vy":
+        return dims.j2n, dims.i2m
+    return dims.j2m, dims.i2m
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+_lib = None
+
+
+def load(path: str | None = None) -> ctypes.CDLL:
+    """Load libcrp.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise RuntimeError(f"libcrp.so not built at {path}; run __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    P = ctypes.POINTER
+    vp = ctypes.c_void_p
+    sigs = {
+        "crp_config_defaults": (c_int, [P(Config)]),
+        "crp_config_parse_file": (c_int, [ctypes.c_char_p, P(Config), ctypes.c_char_p, ctypes.c_size_t]),
+        "crp_config_parse_string": (c_int, [ctypes.c_char_p, P(Config), ctypes.c_char_p, ctypes.c_size_t]),
+        "crp_seed_bubbles": (c_int, [P(Config), vp, vp, vp, vp]),
+        "crp_create": (c_int, [P(Config), P(BubblesIn), vp, P(vp)]),
+        "crp_step": (c_int, [vp, c_int]),
+        "crp_get_dims": (c_int, [vp, P(Dims)]),
+        "crp_get_stats": (c_int, [vp, P(Stats)]),
+        "crp_read_field": (c_int, [vp, c_int, vp]),
+        "crp_read_bubbles": (c_int, [vp, c_int, vp]),
+        "crp_write_rawdata": (c_int, [vp, ctypes.c_char_p]),
+        "crp_stream": (vp, [vp]),
+        "crp_set_profiling": (c_int, [vp, c_int]),
+        "crp_minmax": (c_int, [vp, P(c_dbl), P(c_dbl), P(c_dbl), P(c_dbl)]),
+        "crp_last_error": (ctypes.c_char_p, [vp]),
+        "crp_status_string": (ctypes.c_char_p, [c_int]),
+        "crp_destroy": (None, [vp]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def defaults() -> Config:
+    cfg = Config()
+    load().crp_config_defaults(ctypes.byref(cfg))
+    return cfg
+
+
+def parse_string(text: str, cfg: Config | None = None) -> Config:
+    cfg = cfg if cfg is not None else defaults()
+    err = ctypes.create_string_buffer(512)
+    st = load().crp_config_parse_string(text.encode(), ctypes.byref(cfg), err, 512)
+    if st:
+        raise CrpError(st, err.value.decode())
+    return cfg
+
+
+def parse_file(path: str, cfg: Config | None = None) -> Config:
+    cfg = cfg if cfg is not None else defaults()
+    err = ctypes.create_string_buffer(512)
+    st = load().crp_config_parse_file(path.encode(), ctypes.byref(cfg), err, 512)
+    if st:
+        raise CrpError(st, err.value.decode())
+    return cfg
+
+
+@dataclass
+class Bubbles:
+    x: np.ndarray
+    y: np.ndarray
+    r0: np.ndarray
+    n_b: np.ndarray
+
+    def as_c(self) -> BubblesIn:
+        for a in (self.x, self.y, self.r0, self.n_b):
+            assert a.dtype == np.float64 and a.flags.c_contiguous
+        return BubblesIn(len(self.x), _ptr(self.x), _ptr(self.y), _ptr(self.r0), _ptr(self.n_b))
+
+
+def seed_bubbles(cfg: Config) -> Bubbles:
+    n = cfg.ext_bubble_count
+    arrs = [np.zeros(n) for _ in range(4)]
+    st = load().crp_seed_bubbles(ctypes.byref(cfg), *[_ptr(a) for a in arrs])
+    if st:
+        raise CrpError(st, "crp_seed_bubbles")
+    return Bubbles(*arrs)
+
+
+class Sim:
+    """A simulation on the current CUDA device (one crp_sim handle)."""
+
+    def __init__(self, cfg: Config, bubbles: Bubbles | None = None, stream: int | None = None):
+        self.lib = load()
+        self._keep = (cfg, bubbles)
+        h = ctypes.c_void_p()
+        bin_ = bubbles.as_c() if bubbles is not None else None
+        st = self.lib.crp_create(ctypes.byref(cfg), ctypes.byref(bin_) if bin_ is not None else None,
+                                 ctypes.c_void_p(stream) if stream else None, ctypes.byref(h))
+        if st:
+            raise CrpError(st, self.lib.crp_status_string(st).decode())
+        self.h = h
+        self.dims = Dims()
+        self._check(self.lib.crp_get_dims(self.h, ctypes.byref(self.dims)))
+
+    def _check(self, st: int):
+        if st:
+            msg = self.lib.crp_last_error(self.h)
+            raise CrpError(st, (msg or b"").decode() or self.lib.crp_status_string(st).decode())
+
+    def step(self, n: int = 1):
+        self._check(self.lib.crp_step(self.h, n))
+
+    def stats(self) -> Stats:
+        s = Stats()
+        self._check(self.lib.crp_get_stats(self.h, ctypes.byref(s)))
+        return s
+
+    def field(self, name: str) -> np.ndarray:
+        out = np.empty(field_shape(self.dims, name), dtype=np.float64)
+        self._check(self.lib.crp_read_field(self.h, FIELDS[name], _ptr(out)))
+        return out
+
+    def bubbles(self, name: str) -> np.ndarray:
+        out = np.empty(self.dims.num_bubbles, dtype=np.float64)
+        self._check(self.lib.crp_read_bubbles(self.h, BUBBLE_FIELDS[name], _ptr(out)))
+        return out
+
+    def write_rawdata(self, directory: str):
+        self._check(self.lib.crp_write_rawdata(self.h, directory.encode()))
+
+    def set_profiling(self, on: bool):
+        self._check(self.lib.crp_set_profiling(self.h, 1 if on else 0))
+
+    @property
+    def stream(self) -> int:
+        return self.lib.crp_stream(self.h) or 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.crp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,271 @@
+// Device-side data layout, parameters and physics of the simulation path.
+//
+// HBM layout.  Every grid field is one 2-D array on a common padded frame
+// covering logical i in [-1, X+2] and j in [-1, Y+2]; element (i, j) sits at
+// (j + 1) * pitch + (i + 1), pitch a multiple of 32 elements, base 256-byte
+// aligned.  The reference's differently-sized staggered arrays (vx over
+// i2n x j2m, vy over i2m x j2n, p/f_g over i1m/i2m x j1m/j2m) are windows of this
+// frame, so one index expression serves every field.  The mixture pressure is
+// stored only as its split components (px, py); p0 = px + py and the boundary
+// values of p0 are evaluated where they are read (p0_at).  The mixture density
+// is derived from the previous void fraction, rho_m = (1 - f_g^{n-1}) rho_inf,
+// exactly the value MixturePropertiesKernel stores
+// (inc/bubble_CUDA_kernel.cuh:1122), so neither p0 nor rho_m occupies HBM.
+#pragma once
+#include <cstdint>
+
+namespace crp {
+
+struct Frame {
+  int X, Y;
+  int pitch;  // elements
+  __host__ __device__ __forceinline__ long idx(int i, int j) const { return (long)(j + 1) * pitch + (i + 1); }
+};
+
+// Scalars of grid_t, PML_t, transducer_t, mix_params_t and the [ext] keys the
+// kernels read (inc/bubble_CUDA.h:71-164).
+struct GridParams {
+  Frame f;
+  double dx, dy, rdx, rdy;
+  double dt;
+  double rho_inf, c_inf, P_inf;
+  int pml_x0, pml_x1, pml_y0, pml_y1;
+  int cyl;
+  int plane_p, focused_p, plane_v, focused_v;
+  int source_row;     // 0: ghost row y=0 when pml.y0 is off (reference); >0: forced row
+  double amp, pamp, freq, omega;
+  double on_time, period, ramp_time;
+  double ctl_x, ctl_y, focal_dist;  // focal_point_c, focal_dist_c
+  // PML profiles and cylindrical metrics, indexed by logical i or j:
+  // mx[i] i in [0,X+1], my[j] j in [0,Y+1], nx[i+1] i in [-1,X+1], ny[j+1] j in [-1,Y+1],
+  // xu[i+1] i in [-1,X+1], rxp[i] i in [0,X+1].
+  const double* mx;
+  const double* my;
+  const double* nx;
+  const double* ny;
+  const double* xu;
+  const double* rxp;
+};
+
+// bub_params_t scalars shared by every bubble (inc/bubble_CUDA.h:135-154); the
+// per-bubble R0-derived values live in the bubble arrays.
+struct BubbleParams {
+  double PL0, T0, gam, sig, mu, rho, K0, dt0;
+  double pi, pi4r3;
+  double dcx, dcy, dcz;  // delta_coef (src/bubble_CUDA.cu:1469-1471)
+  long long step_cap;
+};
+
+__host__ __device__ __forceinline__ bool src_pressure(const GridParams& g) { return g.plane_p || g.focused_p; }
+__host__ __device__ __forceinline__ bool src_velocity(const GridParams& g) { return g.plane_v || g.focused_v; }
+
+// Burst envelope of the [ext] cosine ramp (1 when ramp_time is 0).
+__device__ __forceinline__ double burst_ramp(const GridParams& g, double tau) {
+  if (!(g.ramp_time > 0.0)) return 1.0;
+  const double pi = 3.14159265358979323846;
+  double w = 1.0;
+  if (tau < g.ramp_time) w = fmin(w, 0.5 * (1.0 - cos(pi * tau / g.ramp_time)));
+  double rest = g.on_time - tau;
+  if (rest < g.ramp_time) w = fmin(w, rest > 0.0 ? 0.5 * (1.0 - cos(pi * rest / g.ramp_time)) : 0.0);
+  return w;
+}
+
+// Transducer value at (xm, ym), time t.  Plane source then focused source, as
+// inc/bubble_CUDA_kernel.cuh:749-787 (velocity) and :889-925 (pressure).  Returns
+// false when no source of that kind is configured.
+__device__ __forceinline__ bool source_value(const GridParams& g, bool pressure, double xm, double ym, double t,
+                                             double& out) {
+  double amp = pressure ? g.pamp : g.amp;
+  bool set = false;
+  if (pressure ? g.plane_p : g.plane_v) {
+    double tau = fmod(t, g.period);
+    out = (tau <= g.on_time) ? amp * burst_ramp(g, tau) * sin(g.omega * t) : 0.0;
+    set = true;
+  }
+  if (pressure ? g.focused_p : g.focused_v) {
+    double s1 = sqrt((g.ctl_x - xm) * (g.ctl_x - xm) + (g.ctl_y - ym) * (g.ctl_y - ym));
+    if (s1 <= g.focal_dist) {
+      s1 = fmax(t - (g.focal_dist - s1) / g.c_inf, 0.0);
+      double s2 = fmod(s1, g.period);
+      out = (s2 < g.on_time) ? amp * burst_ramp(g, s2) * sin(g.omega * s2) : 0.0;
+    } else {
+      out = 0.0;
+    }
+    set = true;
+  }
+  return set;
+}
+
+// Mixture pressure p0 at logical (i, j), i in [0, X+1], j in [0, Y+1], from the
+// split components of one pressure buffer, with the boundary values that
+// MixtureBoundaryPressureKernel (inc/bubble_CUDA_kernel.cuh:870-952) leaves in
+// p0: its y-face section is applied before its x-face section, PML faces keep
+// p0 = 0, and the y1 mirror is p0(Y+1) = p0(Y).  t is the time of the pressure
+// evaluation that produced the buffer (the source value on the forced row).
+template <typename T>
+__device__ __forceinline__ double p0_at(const GridParams& g, const T* __restrict__ px, const T* __restrict__ py,
+                                        int i, int j, double t) {
+  const int X = g.f.X, Y = g.f.Y;
+  if (i == 0 || i == X + 1) {
+    if (i == 0 ? g.pml_x0 : g.pml_x1) return 0.0;
+    i = (i == 0) ? 1 : X;
+  }
+  if (j == 0) {
+    if (g.pml_y0) return 0.0;
+    double v;
+    if (g.source_row == 0 && source_value(g, true, ((double)i - 0.5) * g.dx, -0.5 * g.dy, t, v)) return v;
+    j = 1;
+  } else if (j == Y + 1) {
+    if (g.pml_y1) return 0.0;
+    j = Y;
+  }
+  if (g.source_row > 0 && j == g.source_row) {
+    double v;
+    if (source_value(g, true, ((double)i - 0.5) * g.dx, ((double)g.source_row - 0.5) * g.dy, t, v)) return v;
+  }
+  long k = g.f.idx(i, j);
+  return (double)px[k] + (double)py[k];
+}
+
+// ---------------------------------------------------------------------------
+// Bubble physics (inc/bubble_CUDA_kernel.cuh:227-340, inc/complex.cuh) in FP64.
+struct C64 {
+  double re, im;
+};
+__device__ __forceinline__ C64 cmul(C64 a, C64 b) { return {a.re * b.re - a.im * b.im, a.im * b.re + a.re * b.im}; }
+__device__ __forceinline__ C64 cdiv(C64 a, C64 b) {
+  double c = b.re * b.re + b.im * b.im;
+  return {(a.re * b.re + a.im * b.im) / c, (a.im * b.re - a.re * b.im) / c};
+}
+__device__ __forceinline__ C64 rdiv(double a, C64 b) {
+  double c = b.re * b.re + b.im * b.im;
+  return {a * b.re / c, -a * b.im / c};
+}
+__device__ __forceinline__ C64 cscl(C64 a, double s) { return {a.re * s, a.im * s}; }
+__device__ __forceinline__ double cabs64(C64 a) { return sqrt(a.re * a.re + a.im * a.im); }
+__device__ __forceinline__ C64 ccoth(C64 a) {
+  double x = tanh(a.re), y = tan(a.im);
+  return cdiv(C64{1.0, x * y}, C64{x, y});
+}
+
+// Per-bubble constants derived from its R0 (init_bub_params, src/bubble_CUDA.cu:666-670).
+struct BubbleR0 {
+  double R0, PG0, R03, coeff_alpha;
+};
+__device__ __forceinline__ BubbleR0 bubble_r0(const BubbleParams& b, double R0) {
+  BubbleR0 r;
+  r.R0 = R0;
+  r.R03 = R0 * R0 * R0;
+  r.PG0 = b.PL0 + 2.0 * b.sig / R0;
+  r.coeff_alpha = b.gam * r.PG0 * r.R03 / (2.0 * (b.gam - 1.0) * b.T0 * b.K0);
+  return r;
+}
+
+// Upsilon (:297-307).
+__device__ __forceinline__ C64 upsilon(C64 a, double gam) {
+  C64 aa = cmul(a, a);
+  C64 t;
+  if (cabs64(a) > 1.0e-1) {
+    C64 ac = cmul(a, ccoth(a));
+    t = cdiv(C64{ac.re - 1.0, ac.im}, aa);
+  } else {
+    C64 q = cmul(aa, C64{2.0 / 945.0 - aa.re / 4725.0, -aa.im / 4725.0});
+    C64 m = cmul(aa, C64{-1.0 / 45.0 + q.re, q.im});
+    t = C64{1.0 / 3.0 + m.re, m.im};
+  }
+  C64 d = cscl(cscl(t, gam - 1.0), 3.0);
+  return rdiv(3.0 * gam, C64{1.0 + d.re, d.im});
+}
+
+// solveLp (:310-323).
+__device__ __forceinline__ C64 lp_n(C64 a, double R) {
+  C64 aa = cmul(a, a);
+  C64 c;
+  if (cabs64(a) > 1.0e-1) {
+    C64 ac = cmul(a, ccoth(a));
+    c = C64{ac.re - 1.0, ac.im};
+    c = cdiv(C64{aa.re - 3.0 * c.re, aa.im - 3.0 * c.im}, cmul(aa, c));
+  } else {
+    C64 a37 = cscl(aa, 37.0);
+    C64 q = cmul(aa, C64{2.0 / 7875.0 - a37.re / 3031875.0, -a37.im / 3031875.0});
+    C64 m = cmul(aa, C64{-1.0 / 175.0 + q.re, q.im});
+    c = C64{1.0 / 5.0 + m.re, m.im};
+  }
+  return cscl(c, R);
+}
+
+// solveOmegaN (:263-288).
+__device__ __forceinline__ double omega_n(C64& alpha, double PG, double R, const BubbleParams& b,
+                                          const BubbleR0& r) {
+  const double eps = 2.22044604925031308e-016;
+  double Rx = R / r.R0;
+  double coef1 = r.PG0 / (PG * Rx * Rx * Rx);
+  double coef2 = PG * b.rho;
+  double coef3 = 4.0 / (R * R);
+  double value1 = -2.0 * b.sig * b.rho / R;
+  double ups_re = 3.0 * b.gam * coef1;
+  double mu_eff = b.mu;
+  double eta = ups_re * coef2 + value1 - mu_eff * mu_eff * coef3;
+  double omega = sqrt(fmax(eta, 1.0e-6 * eps)) / (b.rho * R);
+  for (int k = 0; k < 3; k++) {
+    double s = sqrt(r.coeff_alpha / R * omega);
+    C64 u = cscl(upsilon(C64{s, s}, b.gam), coef1);
+    mu_eff = b.mu + u.im * PG / (4.0 * omega);
+    eta = u.re * coef2 + value1 - mu_eff * mu_eff * coef3;
+    omega = sqrt(fmax(eta, 1.0e-6 * eps)) / (b.rho * R);
+  }
+  double s = sqrt(r.coeff_alpha / R * omega);
+  alpha = C64{s, s};
+  return omega;
+}
+
+// solvePG (:326-340).
+__device__ __forceinline__ double gas_pressure(double PGn, double Rp, double Rn, double omega, double dt, C64 lp,
+                                               const BubbleParams& b, const BubbleR0& r) {
+  double R = 0.5 * (Rp + Rn);
+  double Rx = R / r.R0;
+  double Rpx = Rp / r.R0;
+  double Rnx = Rn / r.R0;
+  double den = lp.re * lp.re + lp.im * lp.im;
+  double lpr = lp.re / den;
+  double lpi = lp.im / den;
+  double c0 = dt * 3.0 * (b.gam - 1.0) * b.K0 * b.T0 / (R * r.PG0);
+  double c3 = 1.5 * b.gam * (Rp - Rn) / R + c0 * lpr * 0.5 * Rx * Rx * Rx;
+  double c1 = 1.0 + c3 - c0 * lpi / (omega * dt) * Rpx * Rpx * Rpx;
+  double c2 = 1.0 - c3 - c0 * lpi / (omega * dt) * Rnx * Rnx * Rnx;
+  return (c2 * PGn + c0 * lpr * r.PG0) / c1;
+}
+
+// solveRayleighPlesset (:227-260): one variable sub-step of the three-level scheme.
+__device__ __forceinline__ void rp_substep(double& Rt, double& Rp, double& Rn, double& d1R, double PG, double PL,
+                                           double& dt, double& remain, const BubbleParams& b) {
+  const double eps = 2.22044604925031308e-016;
+  double Rm = Rn;
+  Rn = Rp;
+  double acc = (PG - PL - 2.0 * b.sig / Rn - 4.0 * b.mu / Rn * d1R) / b.rho - 1.5 * d1R * d1R;
+  double dtm = dt;
+  double dtp = fmin(1.01 * dt, b.dt0);
+  if (fabs(d1R) > eps) dtp = fmin(dtp, 0.01 * Rn / fabs(d1R));
+  if (fabs(acc) > eps) dtp = fmin(dtp, 0.1 * Rn / sqrt(fabs(acc)));
+  double q = dtp / dtm;
+  Rt = Rp = (1.0 + q) * Rn - q * Rm + (dtp / Rn) * (0.5 * (dtp + dtm) * acc);
+  d1R = (dtm * dtm * Rp + (-dtm * dtm + dtp * dtp) * Rn - dtp * dtp * Rm) / (dtm * dtp * (dtm + dtp)) +
+        (dtp / Rn) * acc;
+  dt = dtp;
+  if (dtp >= remain) {
+    dtp = remain;
+    double qr = dtp / dtm;
+    Rt = (1.0 + qr) * Rn - qr * Rm + (dtp / Rn) * (0.5 * (dtp + dtm) * acc);
+  }
+  remain -= dtp;
+}
+
+// Smooth delta (inc/bubble_CUDA_kernel.cuh:214-222).
+__device__ __forceinline__ double delta_x(const BubbleParams& b, const GridParams& g, int pos, double bx) {
+  return b.dcx * (1.0 + cos(b.dcy * (((double)pos - 0.5) * g.dx - bx)));
+}
+__device__ __forceinline__ double delta_y(const BubbleParams& b, const GridParams& g, int pos, double by) {
+  return b.dcx * (1.0 + cos(b.dcz * (((double)pos - 0.5) * g.dy - by)));
+}
+
+}  // namespace crp

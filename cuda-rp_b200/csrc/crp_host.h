@@ -1,0 +1,52 @@
+// Host-side set-up shared by the CUDA library and the `bubbles` program:
+// derived scalars, PML profiles, cylindrical metrics and the bubble population.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "crp.h"
+
+namespace crp {
+
+// Scalars derived once from the configuration (init_grid_size, init_transducer,
+// init_mix, mix_set_time_increment, init_bub_params: src/bubble_CUDA.cu:487-518).
+struct Derived {
+  double dx, dy, rdx, rdy;
+  double dt;
+  double rho_inf, c_inf, P_inf, T_inf;
+  double omega;
+  double fpx, fpy;      // transducer focal point (seeding box centre)
+  double ctl_x, ctl_y;  // focus handed to the source kernels
+  double focal_dist;
+  double bub_dt0;
+  double pi, pi4r3;
+  double dcx, dcy, dcz;  // smooth-delta coefficients
+};
+
+struct HostSetup {
+  Derived d{};
+  // mx, my, nx, ny, xu, rxp concatenated; offsets in elements.
+  std::vector<double> sigma_block;
+  size_t off_mx = 0, off_my = 0, off_nx = 0, off_ny = 0, off_xu = 0, off_rxp = 0;
+  int nb = 0;
+  std::vector<double> bx, by, r0, nb_w;
+};
+
+// Validate the configuration and compute everything crp_create uploads.
+crp_status host_setup(const crp_config& cfg, const crp_bubbles_in* bubbles, HostSetup* out, std::string* err);
+
+// Rawdata writer (rawdata.cpp) and the accessors it uses (sim.cu).
+crp_status write_rawdata(crp_sim* sim, const char* dir);
+crp_status sim_read_field(crp_sim* h, crp_field f, double* host);
+crp_status sim_read_bubbles(crp_sim* h, crp_bubble_field w, double* host);
+const crp_config& sim_config(const crp_sim* h);
+int64_t sim_step_count(const crp_sim* h);
+
+// Running min/max of the values written to rawdata files (the globals of
+// src/bubbles.cpp:11-13 that save_ascii updates), per simulation.
+struct MinMax {
+  double fg_min = 1e10, fg_max = -1e10, p0_min = 1e10, p0_max = -1e10;
+};
+MinMax& sim_minmax(crp_sim* h);
+
+}  // namespace crp

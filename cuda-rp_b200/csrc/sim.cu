@@ -1,0 +1,1233 @@
+// B200 implementation of CUDA-RP's simulation path behind the crp C ABI.
+//
+// One mixture time step (the main loop of solve_bubbles, src/bubble_CUDA.cu:206-285):
+//   fdtd_step      fused: void-fraction prediction (VFPredictionKernel), velocity
+//                  update with its boundary overrides (VelocityKernel,
+//                  VelocityBoundaryKernel), first pressure evaluation
+//                  (MixturePressureKernel) and its residual, one HBM pass
+//   vghost         velocity ghost cells (the rest of VelocityBoundaryKernel)
+//   bubble_move    bubble state rotation (store_variables), velocity gather,
+//                  motion, cell indices, bin counts
+//   bin_scan/fill/sort  counting sort of bubbles by cell (deterministic order)
+//   Picard loop while max|dp0|/P_inf > 1e-7 (src/bubble_CUDA.cu:243):
+//     bubble_rp    pressure gather + Rayleigh-Plesset sub-stepping + the void
+//                  fraction contribution of each bubble to its four cells
+//     couple_press gather of the void fraction per cell (no atomics), axis fold,
+//                  pressure re-evaluation and residual
+// Buffers rotate instead of being copied: velocity and pressure ping-pong, the
+// void-fraction history is a three-buffer ring.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "crp.h"
+#include "crp_device.cuh"
+#include "crp_host.h"
+
+namespace crp {
+
+// ---------------------------------------------------------------------------
+// Kernels, FP64 fields.
+
+constexpr int kFdtdThreads = 128;  // columns per CTA incl. one halo column each side
+constexpr int kFdtdRows = 32;      // rows per CTA
+
+struct FdtdArgs {
+  const double* vx_old;
+  const double* vy_old;
+  double* vx_new;
+  double* vy_new;
+  const double* pnx;  // pressure of the previous step
+  const double* pny;
+  double* px;         // pressure of this step
+  double* py;
+  const double* fgA;  // f_g of the previous step (becomes f_gn)
+  const double* fgB;  // f_gn of the previous step
+  double* fgC;        // f_gm of the previous step; receives the predicted f_g
+  double t_prev, t_cur;
+  int rho_const;      // first step: the mixture density is still rho_inf everywhere
+  unsigned long long* residual;
+};
+
+__device__ __forceinline__ void block_max_to(double v, unsigned long long* out) {
+  // Non-negative doubles order like their bit patterns; NaN (|NaN|) sorts above all.
+  unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+  __shared__ unsigned long long s_red[32];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int lane = tid & 31, w = tid >> 5;
+  if (lane == 0) s_red[w] = b;
+  __syncthreads();
+  if (w == 0) {
+    int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    b = lane < nw ? s_red[lane] : 0ull;
+    for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+    if (lane == 0 && b) atomicMax(out, b);
+  }
+}
+
+// Velocity update of VelocityKernel (inc/bubble_CUDA_kernel.cuh:658-676) for one
+// face, with the coefficients of the reference.
+__device__ __forceinline__ double velocity_face(const GridParams& g, double v_old, double p0a, double p0b, double rhoa,
+                                                double rhob, double sigma) {
+  double s1 = (rhoa + rhob) * 0.5;
+  double s2 = (-p0a + p0b) * g.rdx;  // rdx on both faces, as :661 and :671
+  double s3 = (g.c_inf + g.c_inf) * 0.5;
+  s3 = s3 * 0.5 * g.dt * sigma;
+  return (v_old * (1.0 - s3) - g.dt / s1 * s2) / (1.0 + s3);
+}
+
+__global__ void __launch_bounds__(kFdtdThreads) fdtd_step(const __grid_constant__ GridParams g, const FdtdArgs a) {
+  __shared__ double s_p0[kFdtdThreads];
+  __shared__ double s_rho[kFdtdThreads];
+  __shared__ double s_vx[kFdtdThreads];
+  const Frame& f = g.f;
+  const int X = f.X, Y = f.Y;
+  constexpr int W = kFdtdThreads - 2;
+  const int t = threadIdx.x;
+  const int i0 = 1 + blockIdx.x * W;
+  const int ic = i0 - 1 + t;
+  const int j0 = 1 + blockIdx.y * kFdtdRows;
+  const int j1 = min(j0 + kFdtdRows - 1, Y);
+  const bool col_ok = ic <= X + 1;
+  const bool own = col_ok && ((ic >= i0 && ic <= i0 + W - 1) || ic == 0 || ic == X + 1);
+  const bool interior_col = ic >= 1 && ic <= X;
+  const bool forced_p = g.source_row > 0 && src_pressure(g);
+  const double s3p = g.dt * g.rho_inf * g.c_inf * g.c_inf;
+  const double s4p = 0.5 * g.dt * g.c_inf;
+  const double xm = ((double)ic - 0.5) * g.dx;
+  const double mxi = interior_col ? g.mx[ic] : 0.0;
+  const double nxi = (col_ok && ic <= X) ? g.nx[ic + 1] : 0.0;
+
+  auto rho_at = [&](int j) -> double {
+    if (!col_ok) return g.rho_inf;
+    return a.rho_const ? g.rho_inf : (1.0 - a.fgA[f.idx(ic, j)]) * g.rho_inf;
+  };
+  auto p0_old = [&](int j) -> double { return col_ok ? p0_at(g, a.pnx, a.pny, ic, j, a.t_prev) : 0.0; };
+  // vy at face (ic, j) with the overrides of VelocityBoundaryKernel's vy
+  // section (:734-798): y0 wall/source, [ext] source row, y1 wall.  pre is the
+  // value the y0 ghost mirror copies (before a velocity source is applied).
+  auto vy_face = [&](int j, double p0a, double p0b, double rhoa, double rhob, double& pre) -> double {
+    double v = velocity_face(g, a.vy_old[f.idx(ic, j)], p0a, p0b, rhoa, rhob, g.ny[j + 1]);
+    pre = v;
+    if (j == 0 && !g.pml_y0) {
+      if (!src_pressure(g)) v = 0.0;
+      pre = v;
+      double s;
+      if (g.source_row == 0 && source_value(g, false, xm, 0.0, a.t_cur, s)) v = s;
+    }
+    if (g.source_row > 0 && j == g.source_row) {
+      double s;
+      if (source_value(g, false, xm, (double)g.source_row * g.dy, a.t_cur, s)) v = s;
+    }
+    if (j == Y && !g.pml_y1) v = 0.0;
+    return v;
+  };
+  auto predict = [&](int j) -> double {
+    long k = f.idx(ic, j);
+    return 3.0 * a.fgA[k] - 3.0 * a.fgB[k] + a.fgC[k];
+  };
+
+  double res = 0.0;
+  // Row j0-1: the vy face below the first row of this block.
+  double p0c = p0_old(j0 - 1), rhoc = rho_at(j0 - 1);
+  double p0n = p0_old(j0), rhon = rho_at(j0);
+  double vy_prev = 0.0;
+  if (own && interior_col) {
+    double pre;
+    vy_prev = vy_face(j0 - 1, p0c, p0n, rhoc, rhon, pre);
+    if (j0 == 1) {
+      a.vy_new[f.idx(ic, 0)] = vy_prev;
+      if (!g.pml_y0) a.vy_new[f.idx(ic, -1)] = pre;
+    }
+  }
+  if (own && j0 == 1) a.fgC[f.idx(ic, 0)] = predict(0);
+  p0c = p0n;
+  rhoc = rhon;
+
+  for (int j = j0; j <= j1; j++) {
+    p0n = p0_old(j + 1);
+    rhon = rho_at(j + 1);
+    s_p0[t] = p0c;
+    s_rho[t] = rhoc;
+    __syncthreads();
+    double vx_new = 0.0;
+    if (col_ok && ic <= X && t < kFdtdThreads - 1) {
+      vx_new = velocity_face(g, a.vx_old[f.idx(ic, j)], p0c, s_p0[t + 1], rhoc, s_rho[t + 1], nxi);
+      if ((ic == 0 && !g.pml_x0) || (ic == X && !g.pml_x1)) vx_new = 0.0;
+    }
+    double vy_new = 0.0;
+    if (own && interior_col) {
+      double pre;
+      vy_new = vy_face(j, p0c, p0n, rhoc, rhon, pre);
+    }
+    s_vx[t] = vx_new;
+    __syncthreads();
+    if (own) {
+      long k = f.idx(ic, j);
+      double fgp = predict(j);
+      if (interior_col) {
+        double vxl = s_vx[t - 1];
+        double s1x = g.cyl ? (-g.xu[ic] * vxl + g.xu[ic + 1] * vx_new) * g.rdx * g.rxp[ic]
+                           : (-vxl + vx_new) * g.rdx;
+        double s1y = (-vy_prev + vy_new) * g.rdy;
+        double fgn = a.fgA[k];
+        double s5 = -(fgp - fgn) / g.dt / (1.0 - 0.5 * (fgp + fgn));
+        double s2x = s4p * mxi, s2y = s4p * g.my[j];
+        double h = 0.5 * s5;
+        double qx = a.pnx[k] * (1.0 - s2x) - s3p * (s1x + h) / (1.0 + s2x);
+        double qy = a.pny[k] * (1.0 - s2y) - s3p * (s1y + h) / (1.0 + s2y);
+        a.px[k] = qx;
+        a.py[k] = qy;
+        double p0new = qx + qy;
+        if (forced_p && j == g.source_row) {
+          double s;
+          source_value(g, true, xm, ((double)g.source_row - 0.5) * g.dy, a.t_cur, s);
+          p0new = s;
+        }
+        res = fmax(res, fabs(p0c - p0new));
+        a.vy_new[k] = vy_new;
+      }
+      if (ic <= X) a.vx_new[k] = vx_new;
+      a.fgC[k] = fgp;
+    }
+    vy_prev = vy_new;
+    p0c = p0n;
+    rhoc = rhon;
+  }
+  if (own && j1 == Y) a.fgC[f.idx(ic, Y + 1)] = predict(Y + 1);
+  block_max_to(res, a.residual);
+}
+
+// Velocity ghost cells (VelocityBoundaryKernel, inc/bubble_CUDA_kernel.cuh:701-811,
+// the parts outside the faces the update computes).  Each value is written in
+// closed form from computed faces, in the section order of the reference.
+__global__ void vghost(const __grid_constant__ GridParams g, double* __restrict__ vx, double* __restrict__ vy) {
+  const Frame& f = g.f;
+  const int X = f.X, Y = f.Y;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  // vx after the x-face section (:702-721), for rows 1..Y.
+  auto vxA = [&](int i, int j) -> double {
+    if (i == -1) return g.pml_x0 ? 0.0 : vx[f.idx(1, j)];
+    if (i == X + 1) return g.pml_x1 ? 0.0 : -vx[f.idx(X - 1, j)];
+    return vx[f.idx(i, j)];
+  };
+  // vy after the y-face section (:734-798).
+  auto vyC = [&](int i, int j) -> double {
+    if (j == Y + 1) return g.pml_y1 ? 0.0 : vy[f.idx(i, Y - 1)];
+    return vy[f.idx(i, j)];
+  };
+  if (k >= 1 && k <= Y) {
+    if (!g.pml_x0) vx[f.idx(-1, k)] = vx[f.idx(1, k)];
+    if (!g.pml_x1) vx[f.idx(X + 1, k)] = -vx[f.idx(X - 1, k)];
+  }
+  if (k <= X + 2) {
+    int i = k - 1;
+    vx[f.idx(i, 0)] = vxA(i, 1);
+    vx[f.idx(i, Y + 1)] = vxA(i, Y);
+  }
+  if (k >= 1 && k <= X && !g.pml_y1) vy[f.idx(k, Y + 1)] = vy[f.idx(k, Y - 1)];
+  if (k <= Y + 2) {
+    int j = k - 1;
+    vy[f.idx(0, j)] = vyC(1, j);
+    // The X1 mirror reads row X+1 of the array, logical (X, X) (:808).
+    vy[f.idx(X + 1, j)] = (X <= Y + 1) ? vyC(X, X) : vyC(X, j);
+  }
+}
+
+struct BubbleArrays {
+  double *x, *y, *R_t, *R_p, *R_pn, *R_n, *R_nn, *d1_R_p, *d1_R_n, *PG_p, *PG_n, *PL_p, *PL_n, *PL_m, *Q_B, *n_B,
+      *dt, *dt_n, *re, *re_n, *vbx, *vby, *R0, *contrib;
+  int *ibmx, *ibmy, *ibnx, *ibny, *bin;
+  int n;
+};
+
+struct Bins {
+  int nbx, nby, nbins;
+  int* count;   // nbins, zero between steps
+  int* start;   // nbins + 1
+  int* idx;     // n
+  int* partial; // scan block sums
+};
+
+__device__ __forceinline__ int bin_of(const Frame& f, int bx, int by) {
+  if (bx < -1 || bx > f.X + 1 || by < -1 || by > f.Y + 1) return -1;
+  return (by + 1) * (f.X + 3) + (bx + 1);
+}
+
+// store_variables' bubble rotation (inc/bubble_CUDA_kernel.cuh:1241-1248),
+// BubbleInterpolationVelocityKernel (:398-448) and BubbleMotionKernel (:451-468),
+// plus the cell count for the bin sort.
+__global__ void bubble_move(const __grid_constant__ GridParams g, const __grid_constant__ BubbleParams bp,
+                            BubbleArrays b, const double* __restrict__ vx, const double* __restrict__ vy,
+                            int* __restrict__ bin_count) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= b.n) return;
+  const Frame& f = g.f;
+  b.R_pn[n] = b.R_p[n];
+  b.R_nn[n] = b.R_n[n];
+  b.d1_R_n[n] = b.d1_R_p[n];
+  b.PG_n[n] = b.PG_p[n];
+  b.PL_m[n] = b.PL_n[n];
+  b.PL_n[n] = b.PL_p[n];
+  b.dt_n[n] = b.dt[n];
+  b.re_n[n] = b.re[n];
+  double x = b.x[n], y = b.y[n];
+  int imx = b.ibmx[n], imy = b.ibmy[n], inx = b.ibnx[n], iny = b.ibny[n];
+  double vlx = 0.0, vly = 0.0;
+  for (int i = imx - 1; i <= imx; i++) {
+    double dxw = delta_x(bp, g, i, x);
+    for (int j = iny; j <= iny + 1; j++) {
+      double dyw = delta_y(bp, g, j, y);
+      if (i >= -1 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) vlx += vx[f.idx(i, j)] * dxw * dyw;
+    }
+  }
+  for (int i = inx; i <= inx + 1; i++) {
+    double dxw = delta_x(bp, g, i, x);
+    for (int j = imy - 1; j <= imy; j++) {
+      double dyw = delta_y(bp, g, j, y);
+      if (i >= 0 && i <= f.X + 1 && j >= -1 && j <= f.Y + 1) vly += vy[f.idx(i, j)] * dxw * dyw;
+    }
+  }
+  b.vbx[n] = vlx;
+  b.vby[n] = vly;
+  x = x + vlx * g.dt;
+  y = y + vly * g.dt;
+  b.x[n] = x;
+  b.y[n] = y;
+  b.ibmx[n] = (int)floor(x * g.rdx + 1.0);
+  b.ibmy[n] = (int)floor(y * g.rdy + 1.0);
+  inx = (int)floor(x * g.rdx + 0.5);
+  iny = (int)floor(y * g.rdy + 0.5);
+  b.ibnx[n] = inx;
+  b.ibny[n] = iny;
+  int c = bin_of(f, inx, iny);
+  b.bin[n] = c;
+  if (c >= 0) atomicAdd(&bin_count[c], 1);
+}
+
+// Cell indices of the initial positions (BubbleUpdateIndexKernel, :345-358) and bin counts.
+__global__ void bubble_index(const __grid_constant__ GridParams g, BubbleArrays b, int* __restrict__ bin_count) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= b.n) return;
+  double x = b.x[n], y = b.y[n];
+  b.ibmx[n] = (int)floor(x * g.rdx + 1.0);
+  b.ibmy[n] = (int)floor(y * g.rdy + 1.0);
+  int inx = (int)floor(x * g.rdx + 0.5);
+  int iny = (int)floor(y * g.rdy + 0.5);
+  b.ibnx[n] = inx;
+  b.ibny[n] = iny;
+  int c = bin_of(g.f, inx, iny);
+  b.bin[n] = c;
+  if (c >= 0) atomicAdd(&bin_count[c], 1);
+}
+
+// Exclusive scan of the bin counts: per-block scan, scan of block sums, add.
+constexpr int kScanThreads = 1024;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
+  __shared__ int s_w[32];
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_w[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int s = s_w[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    s_w[lane] = s;
+  }
+  __syncthreads();
+  int before = (w > 0 ? s_w[w - 1] : 0) + x - v;
+  if (total) *total = s_w[31];
+  return before;
+}
+
+__global__ void __launch_bounds__(kScanThreads) bin_scan_blocks(const int* __restrict__ count, int* __restrict__ start,
+                                                                int* __restrict__ partial, int nbins) {
+  int k = blockIdx.x * kScanThreads + threadIdx.x;
+  int v = k < nbins ? count[k] : 0;
+  int total;
+  int e = block_exclusive_scan(v, &total);
+  if (k < nbins) start[k] = e;
+  if (threadIdx.x == 0) partial[blockIdx.x] = total;
+}
+
+// partial[nparts] receives the grand total.
+__global__ void __launch_bounds__(kScanThreads) bin_scan_partials(int* __restrict__ partial, int nparts) {
+  int carry = 0;
+  for (int base = 0; base < nparts; base += kScanThreads) {
+    int k = base + threadIdx.x;
+    int v = k < nparts ? partial[k] : 0;
+    int total;
+    int e = block_exclusive_scan(v, &total);
+    __syncthreads();
+    if (k < nparts) partial[k] = e + carry;
+    carry += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[nparts] = carry;
+}
+
+__global__ void bin_scan_add(int* __restrict__ start, const int* __restrict__ partial, int nbins, int nparts) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nbins) start[k] += partial[k / kScanThreads];
+  if (k == nbins) start[nbins] = partial[nparts];
+}
+
+__global__ void bin_fill(const int* __restrict__ bin, int n, const int* __restrict__ start, int* __restrict__ count,
+                         int* __restrict__ idx) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  int c = bin[b];
+  if (c < 0) return;
+  int slot = start[c] + atomicSub(&count[c], 1) - 1;
+  idx[slot] = b;
+}
+
+// Bubbles of a cell in ascending index order, so every sum over a cell has a
+// fixed order run to run.
+__global__ void bin_sort(const int* __restrict__ start, int* __restrict__ idx, int nbins) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nbins) return;
+  int s = start[c], e = start[c + 1];
+  for (int k = s + 1; k < e; k++) {
+    int v = idx[k];
+    int m = k - 1;
+    while (m >= s && idx[m] > v) {
+      idx[m + 1] = idx[m];
+      m--;
+    }
+    idx[m + 1] = v;
+  }
+}
+
+// BubbleInterpolationScalarKernel (:361-395) and BubbleRadiusKernel (:471-554)
+// for one bubble, then the bubble's void-fraction contribution to the cells of
+// its stencil (VoidFractionReverseLookupKernel, :595-617) stored for the gather.
+__global__ void __launch_bounds__(128) bubble_rp(const __grid_constant__ GridParams g,
+                                                 const __grid_constant__ BubbleParams bp, BubbleArrays b,
+                                                 const double* __restrict__ px, const double* __restrict__ py,
+                                                 double t_cur, long long* __restrict__ substep_max,
+                                                 int* __restrict__ err) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= b.n) return;
+  const Frame& f = g.f;
+  const double x = b.x[n], y = b.y[n];
+  const int inx = b.ibnx[n], iny = b.ibny[n];
+  double dxw[2], dyw[2];
+  for (int q = 0; q < 2; q++) {
+    dxw[q] = delta_x(bp, g, inx + q, x);
+    dyw[q] = delta_y(bp, g, iny + q, y);
+  }
+  double PLp = 0.0;
+  for (int qi = 0; qi < 2; qi++) {
+    int i = inx + qi;
+    for (int qj = 0; qj < 2; qj++) {
+      int j = iny + qj;
+      if (i >= 0 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) PLp += p0_at(g, px, py, i, j, t_cur) * dxw[qi] * dyw[qj];
+    }
+  }
+  b.PL_p[n] = PLp;
+
+  const BubbleR0 r = bubble_r0(bp, b.R0[n]);
+  const double dt = g.dt;
+  double Rt = b.R_t[n];
+  double Rp = b.R_pn[n], Rn = b.R_nn[n], d1Rp = b.d1_R_n[n], PGp = b.PG_n[n], dtL = b.dt_n[n];
+  const double re_n = b.re_n[n];
+  double remain = re_n + dt;
+  double time = -re_n;
+  const double PLn = b.PL_n[n], PLm = b.PL_m[n];
+  const double PC0 = PLn + bp.PL0;
+  const double PC1 = 0.5 * (PLp - PLm) / dt;
+  const double PC2 = 0.5 * (PLp + PLm - 2.0 * PLn) / (dt * dt);
+  double heat = 0.0, vis = 0.0;
+  long long count = 0;
+  while (remain > 0.0) {
+    if (count >= bp.step_cap) {
+      atomicOr(err, 1);
+      break;
+    }
+    double PGn = PGp;
+    double PL = PC2 * time * time + PC1 * time + PC0;
+    rp_substep(Rt, Rp, Rn, d1Rp, PGn, PL, dtL, remain, bp);
+    time = time + dtL;
+    C64 alpha;
+    double omega = omega_n(alpha, PGn, Rn, bp, r);
+    C64 lp = lp_n(alpha, Rn);
+    PGp = gas_pressure(PGn, Rp, Rn, omega, dtL, lp, bp, r);
+    double s0 = 0.5 * (Rp + Rn);
+    double s1 = 1.0 / (lp.re * lp.re + lp.im * lp.im) * bp.T0 / (r.PG0 * r.R03);
+    double dTdr = lp.re * s1 * (r.PG0 * r.R03 - 0.5 * (PGp + PGn) * s0 * s0 * s0) +
+                  lp.im * s1 * (PGp * Rp * Rp * Rp - PGn * Rn * Rn * Rn) / (omega * dtL);
+    heat -= 4.0 * bp.pi * Rp * Rp * bp.K0 * dTdr * dtL;
+    vis += 4.0 * bp.pi * Rp * Rp * 4.0 * bp.mu * d1Rp / Rp * d1Rp * dtL;
+    count++;
+  }
+  b.R_t[n] = Rt;
+  b.R_p[n] = Rp;
+  b.R_n[n] = Rn;
+  b.d1_R_p[n] = d1Rp;
+  b.PG_p[n] = PGp;
+  b.dt[n] = dtL;
+  b.re[n] = remain;
+  b.Q_B[n] = (heat + vis) / (dt - remain + re_n);
+  atomicMax(substep_max, count);
+  const double vol = g.cyl ? bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy / x
+                           : bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy;
+  double* c = b.contrib + 4 * (long)n;
+  c[0] = vol * dxw[0] * dyw[0];
+  c[1] = vol * dxw[0] * dyw[1];
+  c[2] = vol * dxw[1] * dyw[0];
+  c[3] = vol * dxw[1] * dyw[1];
+}
+
+// Void fraction of one cell from the bubbles of the four bins whose stencils
+// cover it (bins (i-1..i) x (j-1..j), each in ascending bubble order).
+__device__ __forceinline__ double gather_fg(const Frame& f, const int* __restrict__ start, const int* __restrict__ idx,
+                                            const double* __restrict__ contrib, int i, int j) {
+  double s = 0.0;
+  for (int by = j - 1; by <= j; by++) {
+    for (int bx = i - 1; bx <= i; bx++) {
+      int c = (by + 1) * (f.X + 3) + (bx + 1);
+      int slot = (i - bx) * 2 + (j - by);
+      for (int k = start[c]; k < start[c + 1]; k++) s += contrib[4 * (long)idx[k] + slot];
+    }
+  }
+  return s;
+}
+
+struct CoupleArgs {
+  const double* vx;
+  const double* vy;
+  const double* pnx;
+  const double* pny;
+  double* px;
+  double* py;
+  double* fg;         // receives the gathered void fraction
+  const double* fgn;
+  const int* start;
+  const int* idx;
+  const double* contrib;
+  double t_cur;
+  unsigned long long* residual;
+};
+
+// calculate_void_fraction (memset, scatter, VoidFractionCylinderKernel fold:
+// :1198-1218, :559-573) as a gather, then MixturePressureKernel (:816-867) on
+// the new void fraction and the residual of calculate_pressure_field.
+__global__ void __launch_bounds__(256) couple_press(const __grid_constant__ GridParams g, const CoupleArgs a) {
+  const Frame& f = g.f;
+  const int X = f.X, Y = f.Y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;       // 0..X+1
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;       // 0..Y+1
+  double res = 0.0;
+  if (i <= X + 1 && j <= Y + 1) {
+    double fgv;
+    if (g.cyl && i <= 1)
+      fgv = gather_fg(f, a.start, a.idx, a.contrib, 0, j) + gather_fg(f, a.start, a.idx, a.contrib, 1, j);
+    else
+      fgv = gather_fg(f, a.start, a.idx, a.contrib, i, j);
+    long k = f.idx(i, j);
+    a.fg[k] = fgv;
+    if (i >= 1 && i <= X && j >= 1 && j <= Y) {
+      const double s3p = g.dt * g.rho_inf * g.c_inf * g.c_inf;
+      const double s4p = 0.5 * g.dt * g.c_inf;
+      double vxl = a.vx[f.idx(i - 1, j)], vxr = a.vx[k];
+      double s1x = g.cyl ? (-g.xu[i] * vxl + g.xu[i + 1] * vxr) * g.rdx * g.rxp[i] : (-vxl + vxr) * g.rdx;
+      double s1y = (-a.vy[f.idx(i, j - 1)] + a.vy[k]) * g.rdy;
+      double fgn = a.fgn[k];
+      double s5 = -(fgv - fgn) / g.dt / (1.0 - 0.5 * (fgv + fgn));
+      double s2x = s4p * g.mx[i], s2y = s4p * g.my[j];
+      double h = 0.5 * s5;
+      double qx = a.pnx[k] * (1.0 - s2x) - s3p * (s1x + h) / (1.0 + s2x);
+      double qy = a.pny[k] * (1.0 - s2y) - s3p * (s1y + h) / (1.0 + s2y);
+      bool forced = g.source_row > 0 && src_pressure(g) && j == g.source_row;
+      if (!forced) res = fabs((a.px[k] + a.py[k]) - (qx + qy));
+      a.px[k] = qx;
+      a.py[k] = qy;
+    }
+  }
+  block_max_to(res, a.residual);
+}
+
+// p0 with its boundary values into a dense (X+2) x (Y+2) array, for readback.
+__global__ void materialize_p0(const __grid_constant__ GridParams g, const double* __restrict__ px,
+                               const double* __restrict__ py, double t, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > g.f.X + 1 || j > g.f.Y + 1) return;
+  out[(long)j * (g.f.X + 2) + i] = p0_at(g, px, py, i, j, t);
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+#define CRP_CUDA(call)                                                      \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess) return fail(CRP_ERR_CUDA, #call, e_);            \
+  } while (0)
+
+// Kernel classes for launch counting and optional per-class device timing.
+enum KernelClass { kClassFdtd = 0, kClassRp = 1, kClassCouple = 2, kClassOther = 3 };
+
+struct Profiler {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;  // pairs
+  std::vector<int> cls;
+  size_t used = 0;
+  double ms[4] = {0, 0, 0, 0};
+  cudaError_t begin(cudaStream_t s, int c) {
+    if (!on) return cudaSuccess;
+    if (2 * used + 2 > ev.size()) {
+      for (int k = 0; k < 2; k++) {
+        cudaEvent_t e;
+        cudaError_t r = cudaEventCreate(&e);
+        if (r != cudaSuccess) return r;
+        ev.push_back(e);
+      }
+      cls.push_back(0);
+    }
+    cls[used] = c;
+    return cudaEventRecord(ev[2 * used], s);
+  }
+  cudaError_t end(cudaStream_t s) {
+    if (!on) return cudaSuccess;
+    cudaError_t r = cudaEventRecord(ev[2 * used + 1], s);
+    used++;
+    return r;
+  }
+  // After the stream has been synchronised.
+  void resolve() {
+    for (size_t k = 0; k < used; k++) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, ev[2 * k], ev[2 * k + 1]) == cudaSuccess) ms[cls[k]] += t;
+    }
+    used = 0;
+  }
+  ~Profiler() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  }
+};
+
+struct Sim {
+  crp_config cfg{};
+  Profiler prof;
+  int64_t launches[4] = {0, 0, 0, 0};
+  HostSetup hs;
+  GridParams gp{};
+  BubbleParams bp{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+
+  // Device memory: one allocation carved into aligned pieces.
+  char* pool = nullptr;
+  size_t pool_bytes = 0;
+  double* vx[2]{};
+  double* vy[2]{};
+  double* px[2]{};
+  double* py[2]{};
+  double* fg[3]{};
+  double* scratch = nullptr;  // dense (X+2) x (Y+2) doubles for readback
+  double* d_sigma = nullptr;
+  BubbleArrays bub{};
+  Bins bins{};
+  // Device scalars written by the kernels, read back once per pressure evaluation.
+  struct Scalars {
+    unsigned long long residual;  // max |dp0| as the bit pattern of a non-negative double
+    long long substep_max;        // largest RP sub-step count of one bubble
+    int err;                      // nonzero: a bubble hit the sub-step cap
+  };
+  Scalars* d_scalars = nullptr;
+  unsigned long long* d_residual = nullptr;
+  long long* d_substep_max = nullptr;
+  int* d_err = nullptr;
+  Scalars* h_scalars = nullptr;  // pinned
+
+  MinMax mm;       // running min/max of written rawdata values
+  int cur_v = 0;   // velocity buffer holding the latest velocities
+  int cur_p = 0;   // pressure buffer holding the latest pressure
+  int fg_a = 0, fg_b = 1, fg_c = 2;  // ring: f_g, f_gn, f_gm
+  double tstep = 0.0, tstepx = 0.0, t_prev = 0.0;
+  crp_stats stats{};
+
+  crp_status fail(crp_status s, const char* what, cudaError_t e = cudaSuccess) {
+    err = std::string(what);
+    if (e != cudaSuccess) err += std::string(": ") + cudaGetErrorString(e);
+    return s;
+  }
+
+  template <typename T>
+  T* carve(size_t count, size_t& off, bool dry) {
+    size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+    T* p = dry ? nullptr : reinterpret_cast<T*>(pool + off);
+    off += bytes;
+    return p;
+  }
+
+  size_t layout(bool dry) {
+    const Frame& f = gp.f;
+    size_t cells = (size_t)f.pitch * (f.Y + 4);
+    size_t off = 0;
+    for (int k = 0; k < 2; k++) {
+      vx[k] = carve<double>(cells, off, dry);
+      vy[k] = carve<double>(cells, off, dry);
+      px[k] = carve<double>(cells, off, dry);
+      py[k] = carve<double>(cells, off, dry);
+    }
+    for (int k = 0; k < 3; k++) fg[k] = carve<double>(cells, off, dry);
+    scratch = carve<double>((size_t)(f.X + 2) * (f.Y + 2), off, dry);
+    d_sigma = carve<double>(hs.sigma_block.size(), off, dry);
+    d_scalars = carve<Scalars>(1, off, dry);
+    if (!dry) {
+      d_residual = &d_scalars->residual;
+      d_substep_max = &d_scalars->substep_max;
+      d_err = &d_scalars->err;
+    }
+    const int n = hs.nb;
+    bub.n = n;
+    double** dp[] = {&bub.x, &bub.y, &bub.R_t, &bub.R_p, &bub.R_pn, &bub.R_n, &bub.R_nn, &bub.d1_R_p, &bub.d1_R_n,
+                     &bub.PG_p, &bub.PG_n, &bub.PL_p, &bub.PL_n, &bub.PL_m, &bub.Q_B, &bub.n_B, &bub.dt, &bub.dt_n,
+                     &bub.re, &bub.re_n, &bub.vbx, &bub.vby, &bub.R0};
+    for (double** p : dp) *p = carve<double>(std::max(n, 1), off, dry);
+    bub.contrib = carve<double>(4 * (size_t)std::max(n, 1), off, dry);
+    int** ip[] = {&bub.ibmx, &bub.ibmy, &bub.ibnx, &bub.ibny, &bub.bin};
+    for (int** p : ip) *p = carve<int>(std::max(n, 1), off, dry);
+    bins.nbx = f.X + 3;
+    bins.nby = f.Y + 3;
+    bins.nbins = bins.nbx * bins.nby;
+    bins.count = carve<int>(bins.nbins, off, dry);
+    bins.start = carve<int>(bins.nbins + 1, off, dry);
+    bins.idx = carve<int>(std::max(n, 1), off, dry);
+    bins.partial = carve<int>((bins.nbins + kScanThreads - 1) / kScanThreads + 1, off, dry);
+    return off;
+  }
+
+  // Launch one kernel (the callable enqueues it on `stream`), counted by class
+  // and bracketed by profiling events when profiling is on.
+  template <typename F>
+  cudaError_t launch(int cls, F&& enqueue) {
+    cudaError_t e = prof.begin(stream, cls);
+    if (e != cudaSuccess) return e;
+    enqueue();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    launches[cls]++;
+    return prof.end(stream);
+  }
+
+  crp_status create(const crp_config& c, const crp_bubbles_in* bin, void* user_stream) {
+    cfg = c;
+    crp_status st = host_setup(cfg, bin, &hs, &err);
+    if (st != CRP_OK) return st;
+    if (cfg.sim_order != 2 || cfg.sim_smooth_delta_band != 2)
+      return fail(CRP_ERR_UNSUPPORTED, "the CUDA path implements simulation.order = 2 and smooth_delta_band = 2");
+    if (cfg.ext_precision != CRP_PREC_FP64)
+      return fail(CRP_ERR_UNSUPPORTED, "ext.precision = mixed is not available in this build");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CRP_ERR_NO_DEVICE, "no CUDA device");
+    if (user_stream) {
+      stream = (cudaStream_t)user_stream;
+    } else {
+      CRP_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+      own_stream = true;
+    }
+    fill_params();
+    pool_bytes = layout(true);
+    CRP_CUDA(cudaMalloc(&pool, pool_bytes));
+    layout(false);
+    CRP_CUDA(cudaMemsetAsync(pool, 0, pool_bytes, stream));
+    CRP_CUDA(cudaMallocHost(&h_scalars, sizeof(Scalars)));
+    // PML profiles and metrics.
+    CRP_CUDA(cudaMemcpyAsync(d_sigma, hs.sigma_block.data(), sizeof(double) * hs.sigma_block.size(),
+                             cudaMemcpyHostToDevice, stream));
+    set_sigma_pointers();
+    // Bubbles: initial state of bubble_input (src/bubble_CUDA.cu:900-943).
+    if (hs.nb > 0) {
+      const int n = hs.nb;
+      std::vector<double> zeros(n, 0.0), dt0(n, bp.dt0), pg0(n);
+      for (int k = 0; k < n; k++) pg0[k] = cfg.bub_P0 + 2.0 * cfg.bub_sigma / hs.r0[k];
+      auto up = [&](double* d, const std::vector<double>& h) {
+        return cudaMemcpyAsync(d, h.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream);
+      };
+      CRP_CUDA(up(bub.x, hs.bx));
+      CRP_CUDA(up(bub.y, hs.by));
+      CRP_CUDA(up(bub.R0, hs.r0));
+      CRP_CUDA(up(bub.n_B, hs.nb_w));
+      for (double* d : {bub.R_t, bub.R_p, bub.R_pn, bub.R_n, bub.R_nn}) CRP_CUDA(up(d, hs.r0));
+      for (double* d : {bub.PG_p, bub.PG_n}) CRP_CUDA(up(d, pg0));
+      for (double* d : {bub.dt, bub.dt_n}) CRP_CUDA(up(d, dt0));
+      CRP_CUDA(cudaStreamSynchronize(stream));
+      // Init kernels (src/bubble_CUDA.cu:175-187): indices, void fraction, history.
+      int nb = (n + 255) / 256;
+      CRP_CUDA(launch(kClassOther, [&] { bubble_index<<<nb, 256, 0, stream>>>(gp, bub, bins.count); }));
+      CRP_CUDA(build_bins());
+      CRP_CUDA(launch_contrib_only());
+      CRP_CUDA(launch_couple(/*pressure=*/false));
+      size_t bytes = sizeof(double) * (size_t)gp.f.pitch * (gp.f.Y + 4);
+      CRP_CUDA(cudaMemcpyAsync(fg[fg_b], fg[fg_a], bytes, cudaMemcpyDeviceToDevice, stream));
+      CRP_CUDA(cudaMemcpyAsync(fg[fg_c], fg[fg_a], bytes, cudaMemcpyDeviceToDevice, stream));
+    }
+    CRP_CUDA(cudaStreamSynchronize(stream));
+    return CRP_OK;
+  }
+
+  void fill_params() {
+    const Derived& d = hs.d;
+    Frame f;
+    f.X = cfg.grid_x;
+    f.Y = cfg.grid_y;
+    f.pitch = ((f.X + 4) + 31) / 32 * 32;
+    gp.f = f;
+    gp.dx = d.dx;
+    gp.dy = d.dy;
+    gp.rdx = d.rdx;
+    gp.rdy = d.rdy;
+    gp.dt = d.dt;
+    gp.rho_inf = d.rho_inf;
+    gp.c_inf = d.c_inf;
+    gp.P_inf = d.P_inf;
+    gp.pml_x0 = cfg.pml_x0;
+    gp.pml_x1 = cfg.pml_x1;
+    gp.pml_y0 = cfg.pml_y0;
+    gp.pml_y1 = cfg.pml_y1;
+    gp.cyl = cfg.tr_cylindrical;
+    gp.plane_p = cfg.tr_plane_p;
+    gp.focused_p = cfg.tr_focused_p;
+    gp.plane_v = cfg.tr_plane_v;
+    gp.focused_v = cfg.tr_focused_v;
+    gp.source_row = cfg.ext_source_row;
+    gp.amp = cfg.tr_amp;
+    gp.pamp = d.rho_inf * d.c_inf * cfg.tr_amp;
+    gp.freq = cfg.tr_freq;
+    gp.omega = d.omega;
+    gp.on_time = (double)cfg.tr_on_wave / cfg.tr_freq;
+    gp.period = ((double)cfg.tr_on_wave + (double)cfg.tr_off_wave) / cfg.tr_freq;
+    gp.ramp_time = cfg.ext_ramp_cycles > 0.0 ? cfg.ext_ramp_cycles / cfg.tr_freq : 0.0;
+    gp.ctl_x = d.ctl_x;
+    gp.ctl_y = d.ctl_y;
+    gp.focal_dist = d.focal_dist;
+    bp.PL0 = cfg.bub_P0;
+    bp.T0 = cfg.bub_T0;
+    bp.gam = cfg.bub_gamma;
+    bp.sig = cfg.bub_sigma;
+    bp.mu = cfg.bub_mu;
+    bp.rho = cfg.bub_rho;
+    bp.K0 = cfg.bub_K0;
+    bp.dt0 = d.bub_dt0;
+    bp.pi = d.pi;
+    bp.pi4r3 = d.pi4r3;
+    bp.dcx = d.dcx;
+    bp.dcy = d.dcy;
+    bp.dcz = d.dcz;
+    bp.step_cap = cfg.ext_rp_step_cap;
+  }
+
+  void set_sigma_pointers() {
+    const double* b = d_sigma;
+    gp.mx = b + hs.off_mx;
+    gp.my = b + hs.off_my;
+    gp.nx = b + hs.off_nx;
+    gp.ny = b + hs.off_ny;
+    gp.xu = b + hs.off_xu;
+    gp.rxp = b + hs.off_rxp;
+  }
+
+  cudaError_t build_bins() {
+    const int nbins = bins.nbins;
+    const int nblk = (nbins + kScanThreads - 1) / kScanThreads;
+    cudaError_t e;
+    if ((e = launch(kClassOther, [&] {
+           bin_scan_blocks<<<nblk, kScanThreads, 0, stream>>>(bins.count, bins.start, bins.partial, nbins);
+         })) != cudaSuccess)
+      return e;
+    if ((e = launch(kClassOther, [&] { bin_scan_partials<<<1, kScanThreads, 0, stream>>>(bins.partial, nblk); })) !=
+        cudaSuccess)
+      return e;
+    if ((e = launch(kClassOther, [&] {
+           bin_scan_add<<<(nbins + 1 + 255) / 256, 256, 0, stream>>>(bins.start, bins.partial, nbins, nblk);
+         })) != cudaSuccess)
+      return e;
+    if ((e = launch(kClassOther, [&] {
+           bin_fill<<<(bub.n + 255) / 256, 256, 0, stream>>>(bub.bin, bub.n, bins.start, bins.count, bins.idx);
+         })) != cudaSuccess)
+      return e;
+    return launch(kClassOther, [&] { bin_sort<<<(nbins + 255) / 256, 256, 0, stream>>>(bins.start, bins.idx, nbins); });
+  }
+
+  // Void-fraction contributions of the initial radii (no RP step).
+  cudaError_t launch_contrib_only();
+
+  cudaError_t launch_couple(bool pressure);
+
+  crp_status read_scalars() {
+    CRP_CUDA(cudaMemcpyAsync(h_scalars, d_scalars, sizeof(Scalars), cudaMemcpyDeviceToHost, stream));
+    CRP_CUDA(cudaStreamSynchronize(stream));
+    prof.resolve();
+    return CRP_OK;
+  }
+
+  crp_status step_once() {
+    // Compensated time sum, src/bubble_CUDA.cu:208-212.
+    t_prev = tstep;
+    double s1 = tstep;
+    tstep = tstep + gp.dt + tstepx;
+    double s2 = tstep - s1;
+    tstepx = gp.dt + tstepx - s2;
+
+    const int nv = cur_v ^ 1, np = cur_p ^ 1;
+    // Ring rotation of store_variables: the predicted f_g goes to the f_gm buffer.
+    const int a = fg_a, b = fg_b, c = fg_c;
+    CRP_CUDA(cudaMemsetAsync(d_residual, 0, sizeof(unsigned long long), stream));
+    FdtdArgs fa;
+    fa.vx_old = vx[cur_v];
+    fa.vy_old = vy[cur_v];
+    fa.vx_new = vx[nv];
+    fa.vy_new = vy[nv];
+    fa.pnx = px[cur_p];
+    fa.pny = py[cur_p];
+    fa.px = px[np];
+    fa.py = py[np];
+    fa.fgA = fg[a];
+    fa.fgB = fg[b];
+    fa.fgC = fg[c];
+    fa.t_prev = t_prev;
+    fa.t_cur = tstep;
+    fa.rho_const = stats.steps == 0 ? 1 : 0;
+    fa.residual = d_residual;
+    dim3 grid((gp.f.X + (kFdtdThreads - 2) - 1) / (kFdtdThreads - 2), (gp.f.Y + kFdtdRows - 1) / kFdtdRows);
+    CRP_CUDA(launch(kClassFdtd, [&] { fdtd_step<<<grid, kFdtdThreads, 0, stream>>>(gp, fa); }));
+    int ng = std::max(gp.f.X, gp.f.Y) + 3;
+    double* vxn = vx[nv];
+    double* vyn = vy[nv];
+    CRP_CUDA(launch(kClassOther, [&] { vghost<<<(ng + 255) / 256, 256, 0, stream>>>(gp, vxn, vyn); }));
+    cur_v = nv;
+    cur_p = np;
+    fg_a = c;  // predicted f_g
+    fg_b = a;  // f_gn
+    fg_c = b;  // f_gm
+    if (hs.nb > 0) {
+      const double* vxc = vx[cur_v];
+      const double* vyc = vy[cur_v];
+      CRP_CUDA(launch(kClassOther, [&] {
+        bubble_move<<<(bub.n + 255) / 256, 256, 0, stream>>>(gp, bp, bub, vxc, vyc, bins.count);
+      }));
+      CRP_CUDA(build_bins());
+    }
+    crp_status st = read_scalars();
+    if (st != CRP_OK) return st;
+    double resimax = __longlong_as_double_host(h_scalars->residual) / gp.P_inf;
+    int loop = 0;
+    if (hs.nb > 0) {
+      while (resimax > 1.0e-7f) {
+        if (loop >= cfg.ext_picard_cap) return fail(CRP_ERR_PICARD, "Picard iteration cap reached");
+        loop++;
+        CRP_CUDA(cudaMemsetAsync(d_residual, 0, sizeof(unsigned long long), stream));
+        const double* pxc = px[cur_p];
+        const double* pyc = py[cur_p];
+        const double tc = tstep;
+        CRP_CUDA(launch(kClassRp, [&] {
+          bubble_rp<<<(bub.n + 127) / 128, 128, 0, stream>>>(gp, bp, bub, pxc, pyc, tc, d_substep_max, d_err);
+        }));
+        CRP_CUDA(launch_couple(true));
+        st = read_scalars();
+        if (st != CRP_OK) return st;
+        if (h_scalars->err) return fail(CRP_ERR_RP_STEPS, "Rayleigh-Plesset sub-step cap reached");
+        resimax = __longlong_as_double_host(h_scalars->residual) / gp.P_inf;
+      }
+    }
+    if (std::isnan(resimax)) return fail(CRP_ERR_NONFINITE, "non-finite pressure");
+    stats.steps++;
+    stats.time = tstep;
+    stats.picard_last = loop;
+    stats.picard_total += loop;
+    stats.picard_max = std::max(stats.picard_max, loop);
+    stats.residual_last = resimax;
+    stats.rp_substeps_max = h_scalars->substep_max;
+    fill_launch_stats();
+    return CRP_OK;
+  }
+
+  void fill_launch_stats() {
+    stats.kernel_launches = launches[0] + launches[1] + launches[2] + launches[3];
+    stats.fdtd_launches = launches[kClassFdtd];
+    stats.rp_launches = launches[kClassRp];
+    stats.couple_launches = launches[kClassCouple];
+    stats.ms_fdtd = prof.ms[kClassFdtd];
+    stats.ms_rp = prof.ms[kClassRp];
+    stats.ms_couple = prof.ms[kClassCouple];
+    stats.ms_other = prof.ms[kClassOther];
+  }
+
+  static double __longlong_as_double_host(unsigned long long b) {
+    double d;
+    std::memcpy(&d, &b, sizeof(d));
+    return d;
+  }
+
+  crp_status read_field(crp_field which, double* host) {
+    const Frame& f = gp.f;
+    auto copy_window = [&](const double* base, int ilo, int ihi, int jlo, int jhi) -> crp_status {
+      int w = ihi - ilo + 1, h = jhi - jlo + 1;
+      CRP_CUDA(cudaMemcpy2DAsync(host, sizeof(double) * w, base + f.idx(ilo, jlo), sizeof(double) * f.pitch,
+                                 sizeof(double) * w, h, cudaMemcpyDeviceToHost, stream));
+      CRP_CUDA(cudaStreamSynchronize(stream));
+      return CRP_OK;
+    };
+    const int X = f.X, Y = f.Y;
+    switch (which) {
+      case CRP_FIELD_P0: {
+        dim3 blk(32, 8), grd((X + 2 + 31) / 32, (Y + 2 + 7) / 8);
+        const double* pxc = px[cur_p];
+        const double* pyc = py[cur_p];
+        CRP_CUDA(launch(kClassOther, [&] { materialize_p0<<<grd, blk, 0, stream>>>(gp, pxc, pyc, tstep, scratch); }));
+        CRP_CUDA(cudaMemcpyAsync(host, scratch, sizeof(double) * (X + 2) * (Y + 2), cudaMemcpyDeviceToHost, stream));
+        CRP_CUDA(cudaStreamSynchronize(stream));
+        return CRP_OK;
+      }
+      case CRP_FIELD_PX: return copy_window(px[cur_p], 0, X + 1, 0, Y + 1);
+      case CRP_FIELD_PY: return copy_window(py[cur_p], 0, X + 1, 0, Y + 1);
+      case CRP_FIELD_PNX: return copy_window(px[cur_p ^ 1], 0, X + 1, 0, Y + 1);
+      case CRP_FIELD_PNY: return copy_window(py[cur_p ^ 1], 0, X + 1, 0, Y + 1);
+      case CRP_FIELD_VX: return copy_window(vx[cur_v], -1, X + 1, 0, Y + 1);
+      case CRP_FIELD_VY: return copy_window(vy[cur_v], 0, X + 1, -1, Y + 1);
+      case CRP_FIELD_FG: return copy_window(fg[fg_a], 0, X + 1, 0, Y + 1);
+      case CRP_FIELD_FGN: return copy_window(fg[fg_b], 0, X + 1, 0, Y + 1);
+      case CRP_FIELD_FGM: return copy_window(fg[fg_c], 0, X + 1, 0, Y + 1);
+      case CRP_FIELD_RHO_M: {
+        crp_status st = copy_window(fg[fg_a], 0, X + 1, 0, Y + 1);
+        if (st != CRP_OK) return st;
+        size_t n = (size_t)(X + 2) * (Y + 2);
+        for (size_t k = 0; k < n; k++) host[k] = stats.steps == 0 ? gp.rho_inf : (1.0 - host[k]) * gp.rho_inf;
+        return CRP_OK;
+      }
+    }
+    return fail(CRP_ERR_INVALID, "unknown field");
+  }
+
+  crp_status read_bubbles(crp_bubble_field w, double* host) {
+    const int n = bub.n;
+    if (n == 0) return CRP_OK;
+    const double* src = nullptr;
+    const int* isrc = nullptr;
+    switch (w) {
+      case CRP_BUB_X: src = bub.x; break;
+      case CRP_BUB_Y: src = bub.y; break;
+      case CRP_BUB_R_T: src = bub.R_t; break;
+      case CRP_BUB_R_P: src = bub.R_p; break;
+      case CRP_BUB_R_N: src = bub.R_n; break;
+      case CRP_BUB_D1R: src = bub.d1_R_p; break;
+      case CRP_BUB_PG: src = bub.PG_p; break;
+      case CRP_BUB_PL_P: src = bub.PL_p; break;
+      case CRP_BUB_PL_N: src = bub.PL_n; break;
+      case CRP_BUB_PL_M: src = bub.PL_m; break;
+      case CRP_BUB_DT: src = bub.dt; break;
+      case CRP_BUB_RE: src = bub.re; break;
+      case CRP_BUB_Q_B: src = bub.Q_B; break;
+      case CRP_BUB_N_B: src = bub.n_B; break;
+      case CRP_BUB_R0: src = bub.R0; break;
+      case CRP_BUB_VX: src = bub.vbx; break;
+      case CRP_BUB_VY: src = bub.vby; break;
+      case CRP_BUB_IBM_X: isrc = bub.ibmx; break;
+      case CRP_BUB_IBM_Y: isrc = bub.ibmy; break;
+      case CRP_BUB_IBN_X: isrc = bub.ibnx; break;
+      case CRP_BUB_IBN_Y: isrc = bub.ibny; break;
+      default: return fail(CRP_ERR_INVALID, "unknown bubble field");
+    }
+    if (src) {
+      CRP_CUDA(cudaMemcpyAsync(host, src, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+      CRP_CUDA(cudaStreamSynchronize(stream));
+    } else {
+      std::vector<int> tmp(n);
+      CRP_CUDA(cudaMemcpyAsync(tmp.data(), isrc, sizeof(int) * n, cudaMemcpyDeviceToHost, stream));
+      CRP_CUDA(cudaStreamSynchronize(stream));
+      for (int k = 0; k < n; k++) host[k] = tmp[k];
+    }
+    return CRP_OK;
+  }
+
+  ~Sim() {
+    if (pool) cudaFree(pool);
+    if (h_scalars) cudaFreeHost(h_scalars);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+  }
+};
+
+// Contributions for the initial radii: the RP kernel's tail without the solve.
+__global__ void bubble_contrib(const __grid_constant__ GridParams g, const __grid_constant__ BubbleParams bp,
+                               BubbleArrays b) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= b.n) return;
+  const double x = b.x[n], y = b.y[n];
+  const int inx = b.ibnx[n], iny = b.ibny[n];
+  double dxw[2], dyw[2];
+  for (int q = 0; q < 2; q++) {
+    dxw[q] = delta_x(bp, g, inx + q, x);
+    dyw[q] = delta_y(bp, g, iny + q, y);
+  }
+  const double Rt = b.R_t[n];
+  const double vol = g.cyl ? bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy / x
+                           : bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy;
+  double* c = b.contrib + 4 * (long)n;
+  c[0] = vol * dxw[0] * dyw[0];
+  c[1] = vol * dxw[0] * dyw[1];
+  c[2] = vol * dxw[1] * dyw[0];
+  c[3] = vol * dxw[1] * dyw[1];
+}
+
+// Gather-only variant of couple_press for the initial void fraction.
+__global__ void __launch_bounds__(256) couple_fg_only(const __grid_constant__ GridParams g, const CoupleArgs a) {
+  const Frame& f = g.f;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > f.X + 1 || j > f.Y + 1) return;
+  double fgv;
+  if (g.cyl && i <= 1)
+    fgv = gather_fg(f, a.start, a.idx, a.contrib, 0, j) + gather_fg(f, a.start, a.idx, a.contrib, 1, j);
+  else
+    fgv = gather_fg(f, a.start, a.idx, a.contrib, i, j);
+  a.fg[f.idx(i, j)] = fgv;
+}
+
+cudaError_t Sim::launch_contrib_only() {
+  return launch(kClassOther, [&] { bubble_contrib<<<(bub.n + 255) / 256, 256, 0, stream>>>(gp, bp, bub); });
+}
+
+cudaError_t Sim::launch_couple(bool pressure) {
+  CoupleArgs ca;
+  ca.vx = vx[cur_v];
+  ca.vy = vy[cur_v];
+  ca.pnx = px[cur_p ^ 1];
+  ca.pny = py[cur_p ^ 1];
+  ca.px = px[cur_p];
+  ca.py = py[cur_p];
+  ca.fg = fg[fg_a];
+  ca.fgn = fg[fg_b];
+  ca.start = bins.start;
+  ca.idx = bins.idx;
+  ca.contrib = bub.contrib;
+  ca.t_cur = tstep;
+  ca.residual = d_residual;
+  dim3 blk(32, 8), grd((gp.f.X + 2 + 31) / 32, (gp.f.Y + 2 + 7) / 8);
+  if (pressure) return launch(kClassCouple, [&] { couple_press<<<grd, blk, 0, stream>>>(gp, ca); });
+  return launch(kClassOther, [&] { couple_fg_only<<<grd, blk, 0, stream>>>(gp, ca); });
+}
+
+}  // namespace crp
+
+// ---------------------------------------------------------------------------
+struct crp_sim {
+  crp::Sim s;
+};
+
+extern "C" {
+
+crp_status crp_create(const crp_config* cfg, const crp_bubbles_in* bubbles, void* stream, crp_sim** out) {
+  if (!cfg || !out) return CRP_ERR_INVALID;
+  *out = nullptr;
+  crp_sim* h = new (std::nothrow) crp_sim();
+  if (!h) return CRP_ERR_ALLOC;
+  crp_status st = h->s.create(*cfg, bubbles, stream);
+  if (st != CRP_OK) {
+    fprintf(stderr, "crp_create: %s\n", h->s.err.c_str());
+    delete h;
+    return st;
+  }
+  *out = h;
+  return CRP_OK;
+}
+
+crp_status crp_step(crp_sim* h, int32_t n) {
+  if (!h || n < 0) return CRP_ERR_INVALID;
+  for (int k = 0; k < n; k++) {
+    crp_status st = h->s.step_once();
+    if (st != CRP_OK) return st;
+  }
+  return CRP_OK;
+}
+
+crp_status crp_get_dims(const crp_sim* h, crp_dims* d) {
+  if (!h || !d) return CRP_ERR_INVALID;
+  const crp::Frame& f = h->s.gp.f;
+  d->i1m = f.X + 2;
+  d->j1m = f.Y + 2;
+  d->i2m = f.X + 2;
+  d->j2m = f.Y + 2;
+  d->i2n = f.X + 3;
+  d->j2n = f.Y + 3;
+  d->num_bubbles = h->s.bub.n;
+  d->dx = h->s.gp.dx;
+  d->dy = h->s.gp.dy;
+  d->dt = h->s.gp.dt;
+  return CRP_OK;
+}
+
+crp_status crp_get_stats(const crp_sim* h, crp_stats* st) {
+  if (!h || !st) return CRP_ERR_INVALID;
+  *st = h->s.stats;
+  return CRP_OK;
+}
+
+crp_status crp_set_profiling(crp_sim* h, int32_t enable) {
+  if (!h) return CRP_ERR_INVALID;
+  if (cudaStreamSynchronize(h->s.stream) != cudaSuccess) return CRP_ERR_CUDA;
+  h->s.prof.resolve();
+  h->s.prof.on = enable != 0;
+  h->s.fill_launch_stats();
+  return CRP_OK;
+}
+
+crp_status crp_read_field(crp_sim* h, crp_field f, double* host) {
+  if (!h || !host) return CRP_ERR_INVALID;
+  return h->s.read_field(f, host);
+}
+
+crp_status crp_read_bubbles(crp_sim* h, crp_bubble_field w, double* host) {
+  if (!h || !host) return CRP_ERR_INVALID;
+  return h->s.read_bubbles(w, host);
+}
+
+crp_status crp_minmax(const crp_sim* h, double* fg_min, double* fg_max, double* p0_min, double* p0_max) {
+  if (!h || !fg_min || !fg_max || !p0_min || !p0_max) return CRP_ERR_INVALID;
+  *fg_min = h->s.mm.fg_min;
+  *fg_max = h->s.mm.fg_max;
+  *p0_min = h->s.mm.p0_min;
+  *p0_max = h->s.mm.p0_max;
+  return CRP_OK;
+}
+
+void* crp_stream(crp_sim* h) { return h ? (void*)h->s.stream : nullptr; }
+
+const char* crp_last_error(const crp_sim* h) { return h ? h->s.err.c_str() : "null handle"; }
+
+void crp_destroy(crp_sim* h) { delete h; }
+
+crp_status crp_write_rawdata(crp_sim* h, const char* dir) {
+  if (!h || !dir) return CRP_ERR_INVALID;
+  return crp::write_rawdata(h, dir);
+}
+
+}  // extern "C"
+
+namespace crp {
+// Accessors used by the rawdata writer (rawdata.cpp).
+crp_status sim_read_field(crp_sim* h, crp_field f, double* host) { return h->s.read_field(f, host); }
+crp_status sim_read_bubbles(crp_sim* h, crp_bubble_field w, double* host) { return h->s.read_bubbles(w, host); }
+const crp_config& sim_config(const crp_sim* h) { return h->s.cfg; }
+int64_t sim_step_count(const crp_sim* h) { return h->s.stats.steps; }
+MinMax& sim_minmax(crp_sim* h) { return h->s.mm; }
+}  // namespace crp

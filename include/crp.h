@@ -1,0 +1,229 @@
+/* crp.h — C ABI of the B200 implementation of CUDA-RP's simulation path:
+ * staggered-grid FDTD of the bubbly mixture (velocity, split-field pressure,
+ * mixture density, PML), per-bubble Rayleigh–Plesset integration, and the
+ * two-way bubble/grid coupling with its Picard sub-loop.
+ *
+ * Plain C types only.  Every function returns a crp_status; nothing exits the
+ * process or throws across this boundary.  A crp_sim owns all of its device
+ * memory and its CUDA stream; host buffers passed in are owned by the caller.
+ * One crp_sim per host thread at a time (handles are independent of each
+ * other; there is no process-global state).
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   crp_config / crp_config_parse_file  <- Boost program_options keys and
+ *                                           config-file parsing, src/bubbles.cpp:61-195
+ *   crp_create                          <- initialize_variables + initialize_CUDA_variables
+ *                                           + the init kernels, src/bubble_CUDA.cu:93-188,
+ *                                           479-521, 1231-1520
+ *   crp_step                            <- one pass of the main loop of solve_bubbles,
+ *                                           src/bubble_CUDA.cu:203-285
+ *   crp_read_field / crp_read_bubbles   <- the device-to-host copies before a save,
+ *                                           src/bubble_CUDA.cu:360-392
+ *   crp_write_rawdata                   <- save_ascii, src/output_styles.cpp:139-341
+ *   crp_destroy                         <- destroy_CUDA_variables, src/bubble_CUDA.cu:1523-1623
+ *   solve_bubbles (inc/bubble_CUDA.h:235) as a whole is crp_create + crp_step
+ *   loop + crp_read_* + crp_destroy, driven by the `bubbles` program.
+ */
+#ifndef CRP_H_
+#define CRP_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum crp_status {
+  CRP_OK = 0,
+  CRP_ERR_INVALID = 1,      /* bad argument or configuration value */
+  CRP_ERR_UNSUPPORTED = 2,  /* configuration outside what this build implements */
+  CRP_ERR_CUDA = 3,         /* a CUDA runtime call failed; see crp_last_error */
+  CRP_ERR_ALLOC = 4,        /* device or host allocation failed */
+  CRP_ERR_RP_STEPS = 5,     /* a bubble exceeded the Rayleigh–Plesset sub-step cap */
+  CRP_ERR_PICARD = 6,       /* the Picard sub-loop exceeded its iteration cap */
+  CRP_ERR_NONFINITE = 7,    /* a NaN/Inf was found in the state */
+  CRP_ERR_IO = 8,           /* file could not be read or written */
+  CRP_ERR_PARSE = 9,        /* configuration file syntax or value error */
+  CRP_ERR_NO_DEVICE = 10    /* no usable CUDA device */
+} crp_status;
+
+/* Arithmetic of the grid fields. */
+typedef enum crp_precision {
+  CRP_PREC_FP64 = 0,   /* all state and arithmetic in FP64 (the reference's precision) */
+  CRP_PREC_MIXED = 1   /* FP32 fields with compensated (Kahan) accumulation; FP64 void
+                          fraction and FP64 bubble dynamics in the stiff phase */
+} crp_precision;
+
+/* Every key of the reference configuration (src/bubbles.cpp:76-132) plus the
+ * extension keys of the [ext] section.  crp_config_defaults fills the
+ * reference's defaults (zero where the reference has none). */
+typedef struct crp_config {
+  /* [grid] */
+  int32_t grid_x, grid_y;            /* cells */
+  double grid_lx, grid_ly;           /* m */
+  /* [pml] */
+  int32_t pml_x0, pml_x1, pml_y0, pml_y1;
+  int32_t pml_grid_number;
+  double pml_sigma;
+  int32_t pml_order;
+  /* [simulation] */
+  double sim_cfl;
+  double sim_dt0;
+  int32_t sim_n_step_max;
+  double sim_t_step_max;
+  int32_t sim_save_interval;
+  int32_t sim_order;                 /* FDTD order (2 is the only order the kernels use) */
+  int32_t sim_smooth_delta_band;
+  /* [transducer] */
+  double tr_amp, tr_freq, tr_focal_dist;
+  int32_t tr_pid, tr_pid_start_step;
+  double tr_init_control;
+  int32_t tr_pid_iterate;
+  double tr_box_size;
+  int32_t tr_cylindrical;
+  int32_t tr_on_wave, tr_off_wave;
+  int32_t tr_plane_v, tr_plane_p;    /* keys transducer.transducer_v / transducer_p */
+  int32_t tr_focused_v, tr_focused_p;
+  /* [bubbles] */
+  int32_t bub_enable;
+  double bub_fg0, bub_R0, bub_P0, bub_T0, bub_gamma;
+  double bub_sigma, bub_mu, bub_rho, bub_K0;
+  /* [debug] (also selects which rawdata files are written) */
+  int32_t dbg_display;
+  int32_t dbg_fg, dbg_T, dbg_p, dbg_v, dbg_bubbles;
+  /* generic options that may also appear in the file */
+  int32_t opt_ascii, opt_sph;
+  /* [ext] — extensions, all off by default so reference configs behave as before */
+  double ext_rho_inf;        /* liquid density, default 1000 (hard-coded in the reference) */
+  double ext_c_inf;          /* sound speed, default 1500 (hard-coded in the reference) */
+  double ext_p_inf;          /* mixture reference pressure for the Picard residual, default 1e5 */
+  int32_t ext_source_row;    /* 0: source on the y=0 ghost row only without a y0 PML (reference);
+                                j>0: source forced on row j (p0 for *_p sources, vy for *_v) */
+  double ext_ramp_cycles;    /* cosine ramp-up/down length of each burst in cycles (0 = off) */
+  int32_t ext_precision;     /* crp_precision */
+  int32_t ext_picard_cap;    /* Picard iteration cap per step (reference: none), default 1000 */
+  int32_t ext_rp_step_cap;   /* RP sub-step cap per bubble per call, default 1000000 */
+  int32_t ext_bubble_count;  /* >0: seed this many bubbles instead of the per-cell lattice */
+  uint64_t ext_bubble_seed;
+  double ext_r0_sigma_ln;    /* lognormal sigma of seeded R0 (median bubbles.R0) */
+  int32_t ext_cloud_shape;   /* 0 cylinder (r <= cloud_r, |z - focus| <= cloud_h/2), 1 sphere, 2 gaussian */
+  double ext_cloud_r, ext_cloud_h;
+  double ext_n_b;            /* weight n_B of each seeded bubble, default 1 */
+} crp_config;
+
+/* Dense host layouts of the readable fields, in the reference's index order:
+ * row-major, x fastest, widths and heights from crp_dims. */
+typedef enum crp_field {
+  CRP_FIELD_P0 = 0,    /* i1m x j1m, pressure p0 = px + py with boundary values */
+  CRP_FIELD_PX = 1,    /* i1m x j1m, split pressure components */
+  CRP_FIELD_PY = 2,
+  CRP_FIELD_PNX = 3,   /* i1m x j1m, previous-step split pressure */
+  CRP_FIELD_PNY = 4,
+  CRP_FIELD_VX = 5,    /* i2n x j2m */
+  CRP_FIELD_VY = 6,    /* i2m x j2n */
+  CRP_FIELD_FG = 7,    /* i2m x j2m, void fraction */
+  CRP_FIELD_FGN = 8,   /* i2m x j2m, previous step */
+  CRP_FIELD_FGM = 9,   /* i2m x j2m, two steps back */
+  CRP_FIELD_RHO_M = 10 /* i1m x j1m, mixture density as the next velocity update sees it */
+} crp_field;
+
+typedef enum crp_bubble_field {
+  CRP_BUB_X = 0, CRP_BUB_Y = 1, CRP_BUB_R_T = 2, CRP_BUB_R_P = 3, CRP_BUB_R_N = 4,
+  CRP_BUB_D1R = 5, CRP_BUB_PG = 6, CRP_BUB_PL_P = 7, CRP_BUB_PL_N = 8, CRP_BUB_PL_M = 9,
+  CRP_BUB_DT = 10, CRP_BUB_RE = 11, CRP_BUB_Q_B = 12, CRP_BUB_N_B = 13, CRP_BUB_R0 = 14,
+  CRP_BUB_VX = 15, CRP_BUB_VY = 16,
+  CRP_BUB_IBM_X = 17, CRP_BUB_IBM_Y = 18, CRP_BUB_IBN_X = 19, CRP_BUB_IBN_Y = 20
+} crp_bubble_field;
+
+typedef struct crp_dims {
+  int32_t i1m, j1m, i2m, j2m, i2n, j2n;
+  int32_t num_bubbles;
+  double dx, dy, dt;
+} crp_dims;
+
+typedef struct crp_stats {
+  int64_t steps;               /* mixture steps taken */
+  double time;                 /* simulated time (compensated sum) */
+  int64_t picard_total;        /* Picard sub-iterations summed over all steps */
+  int32_t picard_last;         /* sub-iterations of the last step */
+  int32_t picard_max;
+  int64_t rp_substeps_max;     /* largest RP sub-step count of one bubble in one call */
+  double residual_last;        /* last max|dp0| / P_inf */
+  int64_t kernel_launches;     /* CUDA kernels launched by this handle */
+  int64_t fdtd_launches, rp_launches, couple_launches;
+  /* Device time per kernel class, accumulated while profiling is on
+   * (crp_set_profiling): the fused FDTD kernel, the RP kernel, the coupling
+   * gather + pressure kernel, and everything else (ghosts, motion, binning). */
+  double ms_fdtd, ms_rp, ms_couple, ms_other;
+} crp_stats;
+
+/* Explicit bubble population: n bubbles with position (x, y), equilibrium
+ * radius R0 and weight n_B.  Replaces the per-cell lattice of the reference
+ * (src/bubble_CUDA.cu:811-839) when passed to crp_create. */
+typedef struct crp_bubbles_in {
+  int32_t n;
+  const double* x;
+  const double* y;
+  const double* r0;
+  const double* n_b;
+} crp_bubbles_in;
+
+typedef struct crp_sim crp_sim;
+
+/* Reference defaults for every key (src/bubbles.cpp:97-132); [ext] defaults. */
+crp_status crp_config_defaults(crp_config* cfg);
+
+/* Parse a reference configuration file (INI: `[section]`, `key = value`, `#`
+ * comments; unknown keys ignored as the reference does) on top of *cfg. */
+crp_status crp_config_parse_file(const char* path, crp_config* cfg, char* err, size_t err_len);
+crp_status crp_config_parse_string(const char* text, crp_config* cfg, char* err, size_t err_len);
+
+/* Seeded bubble population of the [ext] keys (ext_bubble_count > 0): positions
+ * uniform in the cloud around the focal point, R0 lognormal with median
+ * bubbles.R0 and sigma ext_r0_sigma_ln, weight ext_n_b.  Host only; fills
+ * caller arrays of length ext_bubble_count from a Philox-4x32-10 stream keyed
+ * by ext_bubble_seed. */
+crp_status crp_seed_bubbles(const crp_config* cfg, double* x, double* y, double* r0, double* n_b);
+
+/* Build the simulation on the current CUDA device.  bubbles may be NULL (the
+ * reference's lattice seeding, or ext seeding when ext_bubble_count > 0).
+ * stream may be NULL (a stream is created) or a cudaStream_t to run on. */
+crp_status crp_create(const crp_config* cfg, const crp_bubbles_in* bubbles, void* stream, crp_sim** out);
+
+/* Advance n mixture time steps.  Blocks until they are done. */
+crp_status crp_step(crp_sim* sim, int32_t n);
+
+crp_status crp_get_dims(const crp_sim* sim, crp_dims* dims);
+crp_status crp_get_stats(const crp_sim* sim, crp_stats* stats);
+
+/* Copy one field into a dense host array (layout above). */
+crp_status crp_read_field(crp_sim* sim, crp_field field, double* host);
+
+/* Copy one per-bubble quantity into host[num_bubbles]. */
+crp_status crp_read_bubbles(crp_sim* sim, crp_bubble_field what, double* host);
+
+/* Write the reference's plain-text rawdata files for the current step into
+ * dir (created if missing, never cleared): fg/p0/vx/vy_step_%05d.txt and
+ * bubble_radii_/bubble_PG_%05d.txt as selected by the debug keys. */
+crp_status crp_write_rawdata(crp_sim* sim, const char* dir);
+
+/* Running min/max of the f_g and p0 values written by crp_write_rawdata so far
+ * (what save_ascii accumulates for *_minmax.txt, src/output_styles.cpp:200-224). */
+crp_status crp_minmax(const crp_sim* sim, double* fg_min, double* fg_max, double* p0_min, double* p0_max);
+
+/* Record CUDA events around every kernel launch (on the simulation's stream)
+ * and accumulate device time per kernel class into crp_stats. */
+crp_status crp_set_profiling(crp_sim* sim, int32_t enable);
+
+/* Device stream the simulation runs on (a cudaStream_t). */
+void* crp_stream(crp_sim* sim);
+
+const char* crp_last_error(const crp_sim* sim);
+const char* crp_status_string(crp_status s);
+void crp_destroy(crp_sim* sim);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CRP_H_ */

@@ -1,0 +1,56 @@
+/* CPU oracle for the CUDA-RP simulation path — TEST INFRASTRUCTURE ONLY.
+ *
+ * An FP64 host restatement of the reference's initialisers, kernels and main
+ * loop (src/bubble_CUDA.cu, inc/bubble_CUDA_kernel.cuh, inc/complex.cuh,
+ * inc/double_vector_math.cuh), used by the tests as the checker and by
+ * bench.py as the timed CPU baseline.  The product never links or calls it.
+ *
+ * Parity pin: the initialisers and bubble-physics functions are compared
+ * bit-for-bit with the reference's own code compiled on the host
+ * (oracle/_ref/libcrp_ref.so), and whole runs are compared with the reference's
+ * own kernels run on the GPU (golden fixtures under tests/golden/).
+ *
+ * Layout: the reference's dense arrays, row-major with x fastest, widths
+ * i1m/i2m/i2n and heights j1m/j2m/j2n (crp_dims), indexed by the reference's
+ * logical (i, j) ranges.
+ */
+#ifndef CRP_ORACLE_H_
+#define CRP_ORACLE_H_
+#include "crp.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct crpo_sim crpo_sim;
+
+/* Same meaning as crp_create; bubbles == NULL selects the reference lattice. */
+crp_status crpo_create(const crp_config* cfg, const crp_bubbles_in* bubbles, crpo_sim** out);
+crp_status crpo_step(crpo_sim* sim, int32_t n);
+crp_status crpo_get_dims(const crpo_sim* sim, crp_dims* dims);
+crp_status crpo_get_stats(const crpo_sim* sim, crp_stats* stats);
+crp_status crpo_read_field(crpo_sim* sim, crp_field field, double* host);
+crp_status crpo_read_bubbles(crpo_sim* sim, crp_bubble_field what, double* host);
+/* Number of OpenMP threads the oracle uses (0 = library default). */
+void crpo_set_threads(int32_t n);
+int32_t crpo_get_threads(void);
+void crpo_destroy(crpo_sim* sim);
+
+/* Bubble physics on single inputs, for comparison with the reference's
+ * functions (inc/bubble_CUDA_kernel.cuh:227-340).  bp = (R0, PG0, PL0, T0, gam,
+ * sig, mu, rho, K0, dt0). */
+void crpo_rp_step(const double* bp, double* state /* Rt,Rp,Rn,d1R,dt,remain */, double PG, double PL);
+double crpo_omega_n(const double* bp, double PG, double R, double* alpha /* re, im */);
+void crpo_upsilon_lp(double are, double aim, double gam, double R, double* out /* U re,im, Lp re,im */);
+double crpo_solve_pg(const double* bp, double PGn, double Rp, double Rn, double omega_N, double dt,
+                     double lp_re, double lp_im);
+/* Derived scalars in the order of crp_ref_host_scalars (oracle/ref_harness.inc). */
+void crpo_host_scalars(const crp_config* cfg, double* out);
+/* PML profiles and cylindrical metrics: mx[i1m], my[j1m], nx[i2n], ny[j2n], xu[i2n], rxp[i2m]. */
+crp_status crpo_host_sigma(const crp_config* cfg, double* mx, double* my, double* nx, double* ny,
+                           double* xu, double* rxp);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,110 @@
+"""CUDA path against the CPU oracle (same seeded inputs), run through the C ABI.
+
+FP64 fields: every field after N steps within a relative max error of
+TOL_FP64 of the oracle (the GPU differs from the host only in the last bits of
+cos/sin/tanh/tan and in FMA contraction).  Bubble radii likewise.
+"""
+import numpy as np
+import pytest
+
+import _bind as B
+import crp
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-9  # max |gpu - oracle| / max |oracle| per field
+
+FIELDS = ["p0", "px", "py", "pnx", "pny", "vx", "vy", "f_g", "f_gn", "f_gm", "rho_m"]
+BUBBLE = ["x", "y", "R_t", "R_p", "R_n", "d1_R_p", "PG_p", "PL_p", "PL_n", "dt", "Q_B", "v_x", "v_y"]
+
+CASES = {
+    "focus_p": (dict(), 300),
+    "plane_p_all_cells": (dict(grid_x=32, grid_y=64, grid_lx=3.2e-3, grid_ly=6.4e-3, tr_cylindrical=0,
+                               tr_focused_p=0, tr_plane_p=1, tr_box_size=0.0, bub_fg0=2.0e-6, tr_amp=0.05), 80),
+    "focus_v_wall_burst": (dict(pml_x1=0, tr_focused_p=0, tr_focused_v=1, tr_on_wave=1, tr_off_wave=1,
+                                tr_amp=0.1), 300),
+    "plane_v_pml_x0_nobub": (dict(pml_x0=1, tr_focused_p=0, tr_plane_v=1, bub_enable=0), 100),
+    "ext_source_row_ramp": (dict(pml_y0=1, ext_source_row=9, ext_ramp_cycles=0.5, ext_rho_inf=998.0,
+                                 ext_c_inf=1482.0), 300),
+    "rigid_y1_mirror": (dict(pml_y1=0, grid_y=60, grid_ly=6.0e-3, tr_focal_dist=5.0e-3), 250),
+    "wide_planar": (dict(grid_x=70, grid_y=40, grid_lx=7.0e-3, grid_ly=4.0e-3, tr_cylindrical=0,
+                         tr_focal_dist=3.0e-3, tr_box_size=1.0e-3), 150),
+    "strong_drive": (dict(grid_x=24, grid_y=48, grid_lx=2.4e-3, grid_ly=4.8e-3, tr_cylindrical=0, tr_focused_p=0,
+                          tr_plane_p=1, tr_box_size=0.0, tr_amp=0.6, bub_fg0=1e-6), 120),
+}
+
+
+def _compare(gpu, cpu, tol):
+    worst = {}
+    for k in FIELDS:
+        a, b = gpu.field(k), cpu.field(k)
+        assert a.shape == b.shape, k
+        scale = max(np.abs(b).max(), 1e-300)
+        worst[k] = np.abs(a - b).max() / scale if np.abs(b).max() > 0 else np.abs(a).max()
+    if gpu.dims.num_bubbles:
+        assert gpu.dims.num_bubbles == cpu.dims.num_bubbles
+        for k in BUBBLE:
+            a, b = gpu.bubbles(k), cpu.bubbles(k)
+            scale = max(np.abs(b).max(), 1e-300)
+            worst["bub_" + k] = np.abs(a - b).max() / scale if np.abs(b).max() > 0 else np.abs(a).max()
+        for k in ("ibn_x", "ibn_y", "ibm_x", "ibm_y"):
+            assert np.array_equal(gpu.bubbles(k), cpu.bubbles(k)), k
+    print({k: f"{v:.2e}" for k, v in worst.items()})
+    bad = {k: v for k, v in worst.items() if not v <= tol}
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_fp64_matches_oracle(name):
+    over, steps = CASES[name]
+    cfg = B.small_config(**over)
+    cpu = B.OracleSim(cfg)
+    with crp.Sim(cfg) as gpu:
+        _compare(gpu, cpu, TOL_FP64)  # initial state
+        for chunk in (steps // 2, steps - steps // 2):
+            gpu.step(chunk)
+            cpu.step(chunk)
+        gs, cs = gpu.stats(), cpu.stats()
+        assert gs.steps == cs.steps == steps
+        assert abs(gs.time - cs.time) <= 1e-15 * cs.time
+        print(name, "picard gpu", gs.picard_total, "oracle", cs.picard_total)
+        assert abs(gs.picard_total - cs.picard_total) <= max(2, cs.picard_total // 50)
+        _compare(gpu, cpu, TOL_FP64)
+
+
+def test_explicit_lognormal_bubbles():
+    """Seeded population with per-bubble R0 ([ext] keys), passed to both sides."""
+    cfg = B.small_config(ext_bubble_count=300, ext_bubble_seed=7, ext_r0_sigma_ln=0.3, ext_cloud_r=1.0e-3,
+                         ext_cloud_h=2.0e-3, ext_n_b=40.0, bub_R0=3.0e-6)
+    bub = crp.seed_bubbles(cfg)
+    cpu = B.OracleSim(cfg, bub)
+    with crp.Sim(cfg, bub) as gpu:
+        gpu.step(100)
+        cpu.step(100)
+        assert np.array_equal(gpu.bubbles("R0"), bub.r0)
+        _compare(gpu, cpu, TOL_FP64)
+
+
+def test_scatter_is_deterministic():
+    """Two runs give bitwise identical fields (no atomics in the void-fraction sum)."""
+    cfg = B.small_config(grid_x=32, grid_y=64, grid_lx=3.2e-3, grid_ly=6.4e-3, tr_box_size=0.0, bub_fg0=2e-6)
+    out = []
+    for _ in range(2):
+        with crp.Sim(cfg) as gpu:
+            gpu.step(60)
+            out.append([gpu.field(k) for k in ("p0", "f_g", "vx")] + [gpu.bubbles("R_t")])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
+def test_void_fraction_conservation_gpu():
+    """Planar: sum f_g * dx * dy equals sum (4/3) pi n_B R^3 (partition of unity of the delta)."""
+    cfg = B.small_config(tr_cylindrical=0, tr_box_size=1.6e-3)
+    with crp.Sim(cfg) as gpu:
+        gpu.step(40)
+        fg = gpu.field("f_g")
+        R, nb = gpu.bubbles("R_t"), gpu.bubbles("n_B")
+        d = gpu.dims
+        lhs = fg.sum() * d.dx * d.dy
+        rhs = (4.0 / 3.0 * np.pi * nb * R ** 3).sum()
+        assert abs(lhs - rhs) <= 1e-12 * rhs
