@@ -50,8 +50,12 @@ WORKLOADS = {
 }
 # Mixture steps before the burst's leading edge reaches the bubble cloud
 # (about (focus depth - cloud half length - source row depth) / c / dt).
-PREROLL = {"axisym_1024x2048": 1200, "axisym_256x512": 250}
-BYTES_PER_CELL_FP64 = 96  # compulsory traffic of the fused FDTD pass
+PREROLL = {"axisym_1024x2048": 1300, "axisym_256x512": 700}
+# Compulsory HBM traffic of the fused FDTD pass per cell: FP64
+# reads px, py, vx, vy, f_g, f_gn, f_gm and writes px, py, vx, vy, predicted f_g;
+# mixed stores each velocity/pressure value as two FP32 words and f_g as FP32.
+BYTES_PER_CELL = {"fp64": 96, "mixed": 80}
+DTYPE = {"fp64": "f64", "mixed": "f32 fields + f32 compensation (f64 arithmetic), f32 thermal model, f64 RP"}
 
 
 def parse():
@@ -66,6 +70,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
+    ap.add_argument("--primary", default="mixed", choices=["fp64", "mixed"])
     return ap.parse_args()
 
 
@@ -201,6 +207,50 @@ def run_reference(args, rank, world):
     }
 
 
+def timed_run(cfg, bub, args, preroll, dist, dev):
+    """Pre-roll, warm up, then time args.steps bench steps on the simulation's
+    stream (CUDA events, max over ranks).  Returns (ms, stats0, stats1, sim)."""
+    import torch
+
+    import crp
+
+    sim = crp.Sim(cfg, bub)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    sim.step(preroll)
+    for _ in range(args.warmup):
+        sim.step(args.chunk)
+    s0 = sim.stats()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(dev) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            sim.step(args.chunk)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, s0, sim.stats(), sim, clk.summary()
+
+
+def focal_mask(sim, cfg, radius=2e-3):
+    d = sim.dims
+    fy = cfg.tr_focal_dist * 0.5 * np.sqrt(3.0)
+    ii, jj = np.meshgrid(np.arange(d.i1m), np.arange(d.j1m))
+    return np.hypot((ii - 0.5) * d.dx, (jj - 0.5) * d.dy - fy) <= radius
+
+
+def rel_l2(a, b):
+    n = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / n) if n > 0 else float(np.linalg.norm(a))
+
+
 def run_ours(args, rank, world, dist):
     import torch
 
@@ -212,66 +262,75 @@ def run_ours(args, rank, world, dist):
     cells = cfg.grid_x * cfg.grid_y
     preroll = PREROLL[args.workload] if args.preroll is None else args.preroll
     S = args.chunk
-
-    sim = crp.Sim(cfg, bub)
-    nb = sim.dims.num_bubbles
-    stream = torch.cuda.ExternalStream(sim.stream)
-    sim.step(preroll)
-    for _ in range(args.warmup):
-        sim.step(S)
-    s0 = sim.stats()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(dev) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            sim.step(S)
-        e1.record(stream)
-        e1.synchronize()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    s1 = sim.stats()
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     mix_steps = args.steps * S
+
+    # Both forms of the workload: the plain FP64 path and the mixed form.
+    runs = {}
+    for prec in (["mixed", "fp64"] if args.precision == "both" else [args.precision]):
+        cfg.ext_precision = 1 if prec == "mixed" else 0
+        ms, s0, s1, sim, clocks = timed_run(cfg, bub, args, preroll, dist, dev)
+        runs[prec] = {"ms": ms, "s0": s0, "s1": s1, "clocks": clocks,
+                      "p0": sim.field("p0"), "R_t": sim.bubbles("R_t"), "sim": sim}
+        if prec != args.primary and len(runs) > 1:
+            sim.close()
+    primary = args.primary if args.primary in runs else next(iter(runs))
+    run = runs[primary]
+    sim = run["sim"]
+    cfg.ext_precision = 1 if primary == "mixed" else 0
+    nb = sim.dims.num_bubbles
+    ms, s0, s1 = run["ms"], run["s0"], run["s1"]
     value = cells * mix_steps * world / (ms * 1e-3) / 1e6
     launches = s1.kernel_launches - s0.kernel_launches
     picard = s1.picard_total - s0.picard_total
 
     # Roofline of the fused FDTD kernel: device time per launch from profiling events.
     sim.set_profiling(True)
-    p0 = sim.stats()
+    p0s = sim.stats()
     sim.step(S)
-    p1 = sim.stats()
+    p1s = sim.stats()
     sim.set_profiling(False)
-    n_fdtd = p1.fdtd_launches - p0.fdtd_launches
-    fdtd_ms = (p1.ms_fdtd - p0.ms_fdtd) / max(n_fdtd, 1)
-    prof = {k: (getattr(p1, k) - getattr(p0, k)) for k in ("ms_fdtd", "ms_rp", "ms_couple", "ms_other")}
+    n_fdtd = p1s.fdtd_launches - p0s.fdtd_launches
+    fdtd_ms = (p1s.ms_fdtd - p0s.ms_fdtd) / max(n_fdtd, 1)
+    prof = {k: (getattr(p1s, k) - getattr(p0s, k)) for k in ("ms_fdtd", "ms_rp", "ms_couple", "ms_other")}
     hbm, kind = peaks()
-    achieved = BYTES_PER_CELL_FP64 * cells / (fdtd_ms * 1e-3) / 1e9
+    bpc = BYTES_PER_CELL[primary]
+    achieved = bpc * cells / (fdtd_ms * 1e-3) / 1e9
     result = None
     if rank == 0:
         result = {
             "metric": "Mcell-upd/s", "value": value, "unit": "Mcell-upd/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bubbles, Philox-4x32-10)",
+            "vs_baseline": None, "dtype": DTYPE[primary], "data": "synthetic (seeded bubbles, Philox-4x32-10)",
             "config": {"workload": args.workload, "grid": [cfg.grid_x, cfg.grid_y], "bubbles": nb,
-                       "mixture_steps_per_step": S, "preroll_steps": preroll, "precision": "fp64",
+                       "mixture_steps_per_step": S, "preroll_steps": preroll, "precision": primary,
                        "parallelism": f"replicas x{world}", "l2": "state > L2 (no flush needed)"},
             "bubble_steps_per_s": nb * mix_steps * world / (ms * 1e-3),
             "picard_iterations_per_step": picard / mix_steps,
             "gpu_launches": int(launches),
             "roofline": {"kernel": "fdtd_step", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "peak_kind": kind, "traffic": None,
-                         "bytes_per_cell": BYTES_PER_CELL_FP64, "ms_per_launch": fdtd_ms},
+                         "frac": achieved / hbm, "peak_kind": kind, "traffic": None, "bytes_per_cell": bpc,
+                         "ms_per_launch": fdtd_ms},
             "kernel_ms_per_chunk": prof,
-            "clocks": clk.summary(),
+            "clocks": run["clocks"],
         }
-    sim.close()
+        for prec, r in runs.items():
+            result[f"{prec}_path"] = {"value": cells * mix_steps * world / (r["ms"] * 1e-3) / 1e6,
+                                      "ms_per_step": r["ms"] / args.steps,
+                                      "picard_iterations_per_step": (r["s1"].picard_total - r["s0"].picard_total)
+                                      / mix_steps,
+                                      "rp_substeps_max": int(r["s1"].rp_substeps_max)}
+        if "fp64" in runs and "mixed" in runs:
+            a, b = runs["mixed"], runs["fp64"]
+            m = focal_mask(sim, cfg)
+            result["mixed_vs_fp64"] = {
+                "speedup": b["ms"] / a["ms"],
+                "p0_rel_l2": rel_l2(a["p0"], b["p0"]),
+                "p0_focal_rel_l2": rel_l2(a["p0"][m], b["p0"][m]),
+                "R_t_rel_l2": rel_l2(a["R_t"], b["R_t"]),
+                "at_step": int(preroll + (args.warmup + args.steps) * S),
+                "note": "the FP64 GPU path matches the FP64 oracle to ~1e-12 (tests/test_parity_gpu.py)"}
+    for r in runs.values():
+        r["sim"].close()
 
     # End to end through the C ABI: host inputs in, host rawdata arrays out.
     if rank == 0 and not args.no_e2e:
@@ -294,7 +353,8 @@ def run_ours(args, rank, world, dist):
 
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        rate, n, wall, oracle = cpu_baseline(cfg, bub, args.cpu_seconds, threads)
+        cfg64 = crp.parse_file(WORKLOADS[args.workload])
+        rate, n, wall, oracle = cpu_baseline(cfg64, bub, args.cpu_seconds, threads)
         result["cpu_baseline"] = {"value": rate / 1e6, "unit": "Mcell-upd/s", "cores": threads, "kind": "port",
                                   "sample": f"{n} mixture steps of {args.workload} from t=0 "
                                             f"({wall:.1f} s, OpenMP)"}

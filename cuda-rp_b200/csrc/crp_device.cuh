@@ -96,15 +96,40 @@ __device__ __forceinline__ bool source_value(const GridParams& g, bool pressure,
   return set;
 }
 
+// Field storage.  FP64 path: one double per value.  Mixed path: an FP32 value
+// plus an FP32 compensation term holding its rounding error (hi + lo carries
+// about 48 significant bits); arithmetic is done in FP64 registers and each
+// store re-splits the result, so no rounding error accumulates step to step.
+struct F64 {
+  double* p;
+  __device__ __forceinline__ double get(long k) const { return p[k]; }
+  __device__ __forceinline__ void put(long k, double v) const { p[k] = v; }
+};
+struct F32c {
+  float* hi;
+  float* lo;
+  __device__ __forceinline__ double get(long k) const { return (double)hi[k] + (double)lo[k]; }
+  __device__ __forceinline__ void put(long k, double v) const {
+    const float h = (float)v;
+    hi[k] = h;
+    lo[k] = (float)(v - (double)h);
+  }
+};
+// Void-fraction history of the mixed path: FP32 storage (sums are FP64).
+struct F32 {
+  float* p;
+  __device__ __forceinline__ double get(long k) const { return (double)p[k]; }
+  __device__ __forceinline__ void put(long k, double v) const { p[k] = (float)v; }
+};
+
 // Mixture pressure p0 at logical (i, j), i in [0, X+1], j in [0, Y+1], from the
 // split components of one pressure buffer, with the boundary values that
 // MixtureBoundaryPressureKernel (inc/bubble_CUDA_kernel.cuh:870-952) leaves in
 // p0: its y-face section is applied before its x-face section, PML faces keep
 // p0 = 0, and the y1 mirror is p0(Y+1) = p0(Y).  t is the time of the pressure
 // evaluation that produced the buffer (the source value on the forced row).
-template <typename T>
-__device__ __forceinline__ double p0_at(const GridParams& g, const T* __restrict__ px, const T* __restrict__ py,
-                                        int i, int j, double t) {
+template <typename S>
+__device__ __forceinline__ double p0_at(const GridParams& g, const S& px, const S& py, int i, int j, double t) {
   const int X = g.f.X, Y = g.f.Y;
   if (i == 0 || i == X + 1) {
     if (i == 0 ? g.pml_x0 : g.pml_x1) return 0.0;
@@ -123,30 +148,47 @@ __device__ __forceinline__ double p0_at(const GridParams& g, const T* __restrict
     double v;
     if (source_value(g, true, ((double)i - 0.5) * g.dx, ((double)g.source_row - 0.5) * g.dy, t, v)) return v;
   }
-  long k = g.f.idx(i, j);
-  return (double)px[k] + (double)py[k];
+  const long k = g.f.idx(i, j);
+  return px.get(k) + py.get(k);
 }
 
 // ---------------------------------------------------------------------------
-// Bubble physics (inc/bubble_CUDA_kernel.cuh:227-340, inc/complex.cuh) in FP64.
-struct C64 {
-  double re, im;
+// Bubble physics (inc/bubble_CUDA_kernel.cuh:227-340, inc/complex.cuh).  The
+// thermal model (alpha_N, Upsilon, omega_N, Lp_N) is a template on the real
+// type: FP64 for the FP64 path, FP32 for the mixed path.  The radius update,
+// its step-size control and the gas-pressure update stay FP64 in both.
+template <typename R>
+struct Cx {
+  R re, im;
 };
-__device__ __forceinline__ C64 cmul(C64 a, C64 b) { return {a.re * b.re - a.im * b.im, a.im * b.re + a.re * b.im}; }
-__device__ __forceinline__ C64 cdiv(C64 a, C64 b) {
-  double c = b.re * b.re + b.im * b.im;
+template <typename R>
+__device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
+  return {a.re * b.re - a.im * b.im, a.im * b.re + a.re * b.im};
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> cdiv(Cx<R> a, Cx<R> b) {
+  R c = b.re * b.re + b.im * b.im;
   return {(a.re * b.re + a.im * b.im) / c, (a.im * b.re - a.re * b.im) / c};
 }
-__device__ __forceinline__ C64 rdiv(double a, C64 b) {
-  double c = b.re * b.re + b.im * b.im;
+template <typename R>
+__device__ __forceinline__ Cx<R> rdiv(R a, Cx<R> b) {
+  R c = b.re * b.re + b.im * b.im;
   return {a * b.re / c, -a * b.im / c};
 }
-__device__ __forceinline__ C64 cscl(C64 a, double s) { return {a.re * s, a.im * s}; }
-__device__ __forceinline__ double cabs64(C64 a) { return sqrt(a.re * a.re + a.im * a.im); }
-__device__ __forceinline__ C64 ccoth(C64 a) {
-  double x = tanh(a.re), y = tan(a.im);
-  return cdiv(C64{1.0, x * y}, C64{x, y});
+template <typename R>
+__device__ __forceinline__ Cx<R> cscl(Cx<R> a, R s) {
+  return {a.re * s, a.im * s};
 }
+template <typename R>
+__device__ __forceinline__ R cabsx(Cx<R> a) {
+  return sqrt(a.re * a.re + a.im * a.im);
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> ccoth(Cx<R> a) {
+  R x = tanh(a.re), y = tan(a.im);
+  return cdiv(Cx<R>{R(1), x * y}, Cx<R>{x, y});
+}
+using C64 = Cx<double>;
 
 // Per-bubble constants derived from its R0 (init_bub_params, src/bubble_CUDA.cu:666-670).
 struct BubbleR0 {
@@ -162,60 +204,63 @@ __device__ __forceinline__ BubbleR0 bubble_r0(const BubbleParams& b, double R0) 
 }
 
 // Upsilon (:297-307).
-__device__ __forceinline__ C64 upsilon(C64 a, double gam) {
-  C64 aa = cmul(a, a);
-  C64 t;
-  if (cabs64(a) > 1.0e-1) {
-    C64 ac = cmul(a, ccoth(a));
-    t = cdiv(C64{ac.re - 1.0, ac.im}, aa);
+template <typename R>
+__device__ __forceinline__ Cx<R> upsilon(Cx<R> a, R gam) {
+  Cx<R> aa = cmul(a, a);
+  Cx<R> t;
+  if (cabsx(a) > R(1.0e-1)) {
+    Cx<R> ac = cmul(a, ccoth(a));
+    t = cdiv(Cx<R>{ac.re - R(1), ac.im}, aa);
   } else {
-    C64 q = cmul(aa, C64{2.0 / 945.0 - aa.re / 4725.0, -aa.im / 4725.0});
-    C64 m = cmul(aa, C64{-1.0 / 45.0 + q.re, q.im});
-    t = C64{1.0 / 3.0 + m.re, m.im};
+    Cx<R> q = cmul(aa, Cx<R>{R(2.0 / 945.0) - aa.re / R(4725.0), -aa.im / R(4725.0)});
+    Cx<R> m = cmul(aa, Cx<R>{R(-1.0 / 45.0) + q.re, q.im});
+    t = Cx<R>{R(1.0 / 3.0) + m.re, m.im};
   }
-  C64 d = cscl(cscl(t, gam - 1.0), 3.0);
-  return rdiv(3.0 * gam, C64{1.0 + d.re, d.im});
+  Cx<R> d = cscl(cscl(t, gam - R(1)), R(3));
+  return rdiv(R(3) * gam, Cx<R>{R(1) + d.re, d.im});
 }
 
 // solveLp (:310-323).
-__device__ __forceinline__ C64 lp_n(C64 a, double R) {
-  C64 aa = cmul(a, a);
-  C64 c;
-  if (cabs64(a) > 1.0e-1) {
-    C64 ac = cmul(a, ccoth(a));
-    c = C64{ac.re - 1.0, ac.im};
-    c = cdiv(C64{aa.re - 3.0 * c.re, aa.im - 3.0 * c.im}, cmul(aa, c));
+template <typename R>
+__device__ __forceinline__ Cx<R> lp_n(Cx<R> a, R Rb) {
+  Cx<R> aa = cmul(a, a);
+  Cx<R> c;
+  if (cabsx(a) > R(1.0e-1)) {
+    Cx<R> ac = cmul(a, ccoth(a));
+    c = Cx<R>{ac.re - R(1), ac.im};
+    c = cdiv(Cx<R>{aa.re - R(3) * c.re, aa.im - R(3) * c.im}, cmul(aa, c));
   } else {
-    C64 a37 = cscl(aa, 37.0);
-    C64 q = cmul(aa, C64{2.0 / 7875.0 - a37.re / 3031875.0, -a37.im / 3031875.0});
-    C64 m = cmul(aa, C64{-1.0 / 175.0 + q.re, q.im});
-    c = C64{1.0 / 5.0 + m.re, m.im};
+    Cx<R> a37 = cscl(aa, R(37));
+    Cx<R> q = cmul(aa, Cx<R>{R(2.0 / 7875.0) - a37.re / R(3031875.0), -a37.im / R(3031875.0)});
+    Cx<R> m = cmul(aa, Cx<R>{R(-1.0 / 175.0) + q.re, q.im});
+    c = Cx<R>{R(1.0 / 5.0) + m.re, m.im};
   }
-  return cscl(c, R);
+  return cscl(c, Rb);
 }
 
-// solveOmegaN (:263-288).
-__device__ __forceinline__ double omega_n(C64& alpha, double PG, double R, const BubbleParams& b,
-                                          const BubbleR0& r) {
-  const double eps = 2.22044604925031308e-016;
-  double Rx = R / r.R0;
-  double coef1 = r.PG0 / (PG * Rx * Rx * Rx);
-  double coef2 = PG * b.rho;
-  double coef3 = 4.0 / (R * R);
-  double value1 = -2.0 * b.sig * b.rho / R;
-  double ups_re = 3.0 * b.gam * coef1;
-  double mu_eff = b.mu;
-  double eta = ups_re * coef2 + value1 - mu_eff * mu_eff * coef3;
-  double omega = sqrt(fmax(eta, 1.0e-6 * eps)) / (b.rho * R);
+// solveOmegaN (:263-288): omega_N and alpha_N for gas pressure PG at radius Rb.
+template <typename R>
+__device__ __forceinline__ R omega_n(Cx<R>& alpha, R PG, R Rb, const BubbleParams& b, const BubbleR0& r) {
+  const R eps = R(2.22044604925031308e-016);
+  const R rho = R(b.rho), sig = R(b.sig), mu = R(b.mu), gam = R(b.gam), ca = R(r.coeff_alpha);
+  R Rx = Rb / R(r.R0);
+  R coef1 = R(r.PG0) / (PG * Rx * Rx * Rx);
+  R coef2 = PG * rho;
+  R coef3 = R(4) / (Rb * Rb);
+  R value1 = R(-2) * sig * rho / Rb;
+  R ups_re = R(3) * gam * coef1;
+  R mu_eff = mu;
+  R eta = ups_re * coef2 + value1 - mu_eff * mu_eff * coef3;
+  R omega = sqrt(fmax(eta, R(1.0e-6) * eps)) / (rho * Rb);
   for (int k = 0; k < 3; k++) {
-    double s = sqrt(r.coeff_alpha / R * omega);
-    C64 u = cscl(upsilon(C64{s, s}, b.gam), coef1);
-    mu_eff = b.mu + u.im * PG / (4.0 * omega);
+    R s = sqrt(ca / Rb * omega);
+    Cx<R> u = cscl(upsilon(Cx<R>{s, s}, gam), coef1);
+    mu_eff = mu + u.im * PG / (R(4) * omega);
     eta = u.re * coef2 + value1 - mu_eff * mu_eff * coef3;
-    omega = sqrt(fmax(eta, 1.0e-6 * eps)) / (b.rho * R);
+    omega = sqrt(fmax(eta, R(1.0e-6) * eps)) / (rho * Rb);
   }
-  double s = sqrt(r.coeff_alpha / R * omega);
-  alpha = C64{s, s};
+  R s = sqrt(ca / Rb * omega);
+  alpha = Cx<R>{s, s};
   return omega;
 }
 

@@ -35,23 +35,31 @@ namespace crp {
 // ---------------------------------------------------------------------------
 // Kernels, FP64 fields.
 
-constexpr int kFdtdThreads = 128;  // columns per CTA incl. one halo column each side
-constexpr int kFdtdRows = 32;      // rows per CTA
 
+// Storage of each field class and the real type of the bubble thermal model.
+struct PrecFP64 {
+  using V = F64;  // velocity
+  using S = F64;  // split pressure
+  using G = F64;  // void fraction
+  using T = double;
+};
+struct PrecMixed {
+  using V = F32c;
+  using S = F32c;
+  using G = F32;
+  using T = float;
+};
+
+template <typename P>
 struct FdtdArgs {
-  const double* vx_old;
-  const double* vy_old;
-  double* vx_new;
-  double* vy_new;
-  const double* pnx;  // pressure of the previous step
-  const double* pny;
-  double* px;         // pressure of this step
-  double* py;
-  const double* fgA;  // f_g of the previous step (becomes f_gn)
-  const double* fgB;  // f_gn of the previous step
-  double* fgC;        // f_gm of the previous step; receives the predicted f_g
+  typename P::V vx_old, vy_old, vx_new, vy_new;
+  typename P::S pnx, pny;  // pressure of the previous step
+  typename P::S px, py;    // pressure of this step
+  typename P::G fgA;       // f_g of the previous step (becomes f_gn)
+  typename P::G fgB;       // f_gn of the previous step
+  typename P::G fgC;       // f_gm of the previous step; receives the predicted f_g
   double t_prev, t_cur;
-  int rho_const;      // first step: the mixture density is still rho_inf everywhere
+  int rho_const;           // first step: the mixture density is still rho_inf everywhere
   unsigned long long* residual;
 };
 
@@ -83,168 +91,138 @@ __device__ __forceinline__ double velocity_face(const GridParams& g, double v_ol
   return (v_old * (1.0 - s3) - g.dt / s1 * s2) / (1.0 + s3);
 }
 
-__global__ void __launch_bounds__(kFdtdThreads) fdtd_step(const __grid_constant__ GridParams g, const FdtdArgs a) {
-  __shared__ double s_p0[kFdtdThreads];
-  __shared__ double s_rho[kFdtdThreads];
-  __shared__ double s_vx[kFdtdThreads];
+// One thread per cell (i, j) of the f_g window [0, X+1] x [0, Y+1].  Interior
+// threads compute the four velocity faces around their cell (the west and
+// south faces duplicate a neighbour's east/north face; those values are
+// identical, and only the owner writes them), then the pressure of the cell.
+// Neighbour loads hit L1/L2, so HBM sees each array about once per step.
+constexpr int kFdtdBX = 32, kFdtdBY = 8;
+
+template <typename P>
+__global__ void __launch_bounds__(kFdtdBX * kFdtdBY) fdtd_step(const __grid_constant__ GridParams g,
+                                                               const FdtdArgs<P> a) {
   const Frame& f = g.f;
   const int X = f.X, Y = f.Y;
-  constexpr int W = kFdtdThreads - 2;
-  const int t = threadIdx.x;
-  const int i0 = 1 + blockIdx.x * W;
-  const int ic = i0 - 1 + t;
-  const int j0 = 1 + blockIdx.y * kFdtdRows;
-  const int j1 = min(j0 + kFdtdRows - 1, Y);
-  const bool col_ok = ic <= X + 1;
-  const bool own = col_ok && ((ic >= i0 && ic <= i0 + W - 1) || ic == 0 || ic == X + 1);
-  const bool interior_col = ic >= 1 && ic <= X;
-  const bool forced_p = g.source_row > 0 && src_pressure(g);
-  const double s3p = g.dt * g.rho_inf * g.c_inf * g.c_inf;
-  const double s4p = 0.5 * g.dt * g.c_inf;
-  const double xm = ((double)ic - 0.5) * g.dx;
-  const double mxi = interior_col ? g.mx[ic] : 0.0;
-  const double nxi = (col_ok && ic <= X) ? g.nx[ic + 1] : 0.0;
-
-  auto rho_at = [&](int j) -> double {
-    if (!col_ok) return g.rho_inf;
-    return a.rho_const ? g.rho_inf : (1.0 - a.fgA[f.idx(ic, j)]) * g.rho_inf;
-  };
-  auto p0_old = [&](int j) -> double { return col_ok ? p0_at(g, a.pnx, a.pny, ic, j, a.t_prev) : 0.0; };
-  // vy at face (ic, j) with the overrides of VelocityBoundaryKernel's vy
-  // section (:734-798): y0 wall/source, [ext] source row, y1 wall.  pre is the
-  // value the y0 ghost mirror copies (before a velocity source is applied).
-  auto vy_face = [&](int j, double p0a, double p0b, double rhoa, double rhob, double& pre) -> double {
-    double v = velocity_face(g, a.vy_old[f.idx(ic, j)], p0a, p0b, rhoa, rhob, g.ny[j + 1]);
-    pre = v;
-    if (j == 0 && !g.pml_y0) {
-      if (!src_pressure(g)) v = 0.0;
-      pre = v;
-      double s;
-      if (g.source_row == 0 && source_value(g, false, xm, 0.0, a.t_cur, s)) v = s;
-    }
-    if (g.source_row > 0 && j == g.source_row) {
-      double s;
-      if (source_value(g, false, xm, (double)g.source_row * g.dy, a.t_cur, s)) v = s;
-    }
-    if (j == Y && !g.pml_y1) v = 0.0;
-    return v;
-  };
-  auto predict = [&](int j) -> double {
-    long k = f.idx(ic, j);
-    return 3.0 * a.fgA[k] - 3.0 * a.fgB[k] + a.fgC[k];
-  };
-
+  const int i = blockIdx.x * kFdtdBX + threadIdx.x;
+  const int j = blockIdx.y * kFdtdBY + threadIdx.y;
   double res = 0.0;
-  // Row j0-1: the vy face below the first row of this block.
-  double p0c = p0_old(j0 - 1), rhoc = rho_at(j0 - 1);
-  double p0n = p0_old(j0), rhon = rho_at(j0);
-  double vy_prev = 0.0;
-  if (own && interior_col) {
-    double pre;
-    vy_prev = vy_face(j0 - 1, p0c, p0n, rhoc, rhon, pre);
-    if (j0 == 1) {
-      a.vy_new[f.idx(ic, 0)] = vy_prev;
-      if (!g.pml_y0) a.vy_new[f.idx(ic, -1)] = pre;
-    }
-  }
-  if (own && j0 == 1) a.fgC[f.idx(ic, 0)] = predict(0);
-  p0c = p0n;
-  rhoc = rhon;
-
-  for (int j = j0; j <= j1; j++) {
-    p0n = p0_old(j + 1);
-    rhon = rho_at(j + 1);
-    s_p0[t] = p0c;
-    s_rho[t] = rhoc;
-    __syncthreads();
-    double vx_new = 0.0;
-    if (col_ok && ic <= X && t < kFdtdThreads - 1) {
-      vx_new = velocity_face(g, a.vx_old[f.idx(ic, j)], p0c, s_p0[t + 1], rhoc, s_rho[t + 1], nxi);
-      if ((ic == 0 && !g.pml_x0) || (ic == X && !g.pml_x1)) vx_new = 0.0;
-    }
-    double vy_new = 0.0;
-    if (own && interior_col) {
-      double pre;
-      vy_new = vy_face(j, p0c, p0n, rhoc, rhon, pre);
-    }
-    s_vx[t] = vx_new;
-    __syncthreads();
-    if (own) {
-      long k = f.idx(ic, j);
-      double fgp = predict(j);
-      if (interior_col) {
-        double vxl = s_vx[t - 1];
-        double s1x = g.cyl ? (-g.xu[ic] * vxl + g.xu[ic + 1] * vx_new) * g.rdx * g.rxp[ic]
-                           : (-vxl + vx_new) * g.rdx;
-        double s1y = (-vy_prev + vy_new) * g.rdy;
-        double fgn = a.fgA[k];
-        double s5 = -(fgp - fgn) / g.dt / (1.0 - 0.5 * (fgp + fgn));
-        double s2x = s4p * mxi, s2y = s4p * g.my[j];
-        double h = 0.5 * s5;
-        double qx = a.pnx[k] * (1.0 - s2x) - s3p * (s1x + h) / (1.0 + s2x);
-        double qy = a.pny[k] * (1.0 - s2y) - s3p * (s1y + h) / (1.0 + s2y);
-        a.px[k] = qx;
-        a.py[k] = qy;
-        double p0new = qx + qy;
-        if (forced_p && j == g.source_row) {
+  if (i <= X + 1 && j <= Y + 1) {
+    const long k = f.idx(i, j);
+    const double fgA = a.fgA.get(k);
+    // Predicted f_g, rounded to its storage precision before use.
+    a.fgC.put(k, 3.0 * fgA - 3.0 * a.fgB.get(k) + a.fgC.get(k));
+    const double fgp = a.fgC.get(k);
+    if (i >= 1 && i <= X && j >= 1 && j <= Y) {
+      const double xm = ((double)i - 0.5) * g.dx;
+      auto rho_at = [&](long kk) -> double { return a.rho_const ? g.rho_inf : (1.0 - a.fgA.get(kk)) * g.rho_inf; };
+      // p0 of the previous step (interior: px + py; boundary values by p0_at).
+      const double pnx = a.pnx.get(k), pny = a.pny.get(k);
+      const bool forced_here = g.source_row > 0 && j == g.source_row && src_pressure(g);
+      const double p0c = forced_here ? p0_at(g, a.pnx, a.pny, i, j, a.t_prev) : pnx + pny;
+      const double p0l = p0_at(g, a.pnx, a.pny, i - 1, j, a.t_prev);
+      const double p0r = p0_at(g, a.pnx, a.pny, i + 1, j, a.t_prev);
+      const double p0d = p0_at(g, a.pnx, a.pny, i, j - 1, a.t_prev);
+      const double p0u = p0_at(g, a.pnx, a.pny, i, j + 1, a.t_prev);
+      const double rc = a.rho_const ? g.rho_inf : (1.0 - fgA) * g.rho_inf;
+      const double rl = rho_at(f.idx(i - 1, j)), rr = rho_at(f.idx(i + 1, j));
+      const double rd = rho_at(f.idx(i, j - 1)), ru = rho_at(f.idx(i, j + 1));
+      // x faces (VelocityKernel :658-666, VelocityBoundaryKernel :704-720).
+      double vxl = velocity_face(g, a.vx_old.get(f.idx(i - 1, j)), p0l, p0c, rl, rc, g.nx[i]);
+      if (i - 1 == 0 && !g.pml_x0) vxl = 0.0;
+      double vxr = velocity_face(g, a.vx_old.get(k), p0c, p0r, rc, rr, g.nx[i + 1]);
+      if (i == X && !g.pml_x1) vxr = 0.0;
+      // y faces (:668-676, :734-798): y0 wall/source, [ext] source row, y1 wall.
+      auto vy_face = [&](int jf, double v_old, double p0a, double p0b, double ra, double rb, double& pre) -> double {
+        double v = velocity_face(g, v_old, p0a, p0b, ra, rb, g.ny[jf + 1]);
+        pre = v;
+        if (jf == 0 && !g.pml_y0) {
+          if (!src_pressure(g)) v = 0.0;
+          pre = v;
           double s;
-          source_value(g, true, xm, ((double)g.source_row - 0.5) * g.dy, a.t_cur, s);
-          p0new = s;
+          if (g.source_row == 0 && source_value(g, false, xm, 0.0, a.t_cur, s)) v = s;
         }
-        res = fmax(res, fabs(p0c - p0new));
-        a.vy_new[k] = vy_new;
+        if (g.source_row > 0 && jf == g.source_row) {
+          double s;
+          if (source_value(g, false, xm, (double)g.source_row * g.dy, a.t_cur, s)) v = s;
+        }
+        if (jf == Y && !g.pml_y1) v = 0.0;
+        return v;
+      };
+      double pre_d, pre_u;
+      const double vyd = vy_face(j - 1, a.vy_old.get(f.idx(i, j - 1)), p0d, p0c, rd, rc, pre_d);
+      const double vyu = vy_face(j, a.vy_old.get(k), p0c, p0u, rc, ru, pre_u);
+      a.vx_new.put(k, vxr);
+      a.vy_new.put(k, vyu);
+      if (i == 1) a.vx_new.put(f.idx(0, j), vxl);
+      if (j == 1) {
+        a.vy_new.put(f.idx(i, 0), vyd);
+        if (!g.pml_y0) a.vy_new.put(f.idx(i, -1), pre_d);
       }
-      if (ic <= X) a.vx_new[k] = vx_new;
-      a.fgC[k] = fgp;
+      // Pressure (MixturePressureKernel :840-864) with the predicted f_g.
+      const double s3p = g.dt * g.rho_inf * g.c_inf * g.c_inf;
+      const double s4p = 0.5 * g.dt * g.c_inf;
+      const double s1x = g.cyl ? (-g.xu[i] * vxl + g.xu[i + 1] * vxr) * g.rdx * g.rxp[i] : (-vxl + vxr) * g.rdx;
+      const double s1y = (-vyd + vyu) * g.rdy;
+      const double s5 = -(fgp - fgA) / g.dt / (1.0 - 0.5 * (fgp + fgA));
+      const double s2x = s4p * g.mx[i], s2y = s4p * g.my[j];
+      const double h = 0.5 * s5;
+      const double qx = pnx * (1.0 - s2x) - s3p * (s1x + h) / (1.0 + s2x);
+      const double qy = pny * (1.0 - s2y) - s3p * (s1y + h) / (1.0 + s2y);
+      a.px.put(k, qx);
+      a.py.put(k, qy);
+      double p0new = qx + qy;
+      if (forced_here) {
+        double s;
+        source_value(g, true, xm, ((double)g.source_row - 0.5) * g.dy, a.t_cur, s);
+        p0new = s;
+      }
+      res = fabs(p0c - p0new);
     }
-    vy_prev = vy_new;
-    p0c = p0n;
-    rhoc = rhon;
   }
-  if (own && j1 == Y) a.fgC[f.idx(ic, Y + 1)] = predict(Y + 1);
   block_max_to(res, a.residual);
 }
 
 // Velocity ghost cells (VelocityBoundaryKernel, inc/bubble_CUDA_kernel.cuh:701-811,
 // the parts outside the faces the update computes).  Each value is written in
 // closed form from computed faces, in the section order of the reference.
-__global__ void vghost(const __grid_constant__ GridParams g, double* __restrict__ vx, double* __restrict__ vy) {
+template <typename V>
+__global__ void vghost(const __grid_constant__ GridParams g, const V vx, const V vy) {
   const Frame& f = g.f;
   const int X = f.X, Y = f.Y;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   // vx after the x-face section (:702-721), for rows 1..Y.
   auto vxA = [&](int i, int j) -> double {
-    if (i == -1) return g.pml_x0 ? 0.0 : vx[f.idx(1, j)];
-    if (i == X + 1) return g.pml_x1 ? 0.0 : -vx[f.idx(X - 1, j)];
-    return vx[f.idx(i, j)];
+    if (i == -1) return g.pml_x0 ? 0.0 : vx.get(f.idx(1, j));
+    if (i == X + 1) return g.pml_x1 ? 0.0 : -vx.get(f.idx(X - 1, j));
+    return vx.get(f.idx(i, j));
   };
   // vy after the y-face section (:734-798).
   auto vyC = [&](int i, int j) -> double {
-    if (j == Y + 1) return g.pml_y1 ? 0.0 : vy[f.idx(i, Y - 1)];
-    return vy[f.idx(i, j)];
+    if (j == Y + 1) return g.pml_y1 ? 0.0 : vy.get(f.idx(i, Y - 1));
+    return vy.get(f.idx(i, j));
   };
   if (k >= 1 && k <= Y) {
-    if (!g.pml_x0) vx[f.idx(-1, k)] = vx[f.idx(1, k)];
-    if (!g.pml_x1) vx[f.idx(X + 1, k)] = -vx[f.idx(X - 1, k)];
+    if (!g.pml_x0) vx.put(f.idx(-1, k), vx.get(f.idx(1, k)));
+    if (!g.pml_x1) vx.put(f.idx(X + 1, k), -vx.get(f.idx(X - 1, k)));
   }
   if (k <= X + 2) {
     int i = k - 1;
-    vx[f.idx(i, 0)] = vxA(i, 1);
-    vx[f.idx(i, Y + 1)] = vxA(i, Y);
+    vx.put(f.idx(i, 0), vxA(i, 1));
+    vx.put(f.idx(i, Y + 1), vxA(i, Y));
   }
-  if (k >= 1 && k <= X && !g.pml_y1) vy[f.idx(k, Y + 1)] = vy[f.idx(k, Y - 1)];
+  if (k >= 1 && k <= X && !g.pml_y1) vy.put(f.idx(k, Y + 1), vy.get(f.idx(k, Y - 1)));
   if (k <= Y + 2) {
     int j = k - 1;
-    vy[f.idx(0, j)] = vyC(1, j);
+    vy.put(f.idx(0, j), vyC(1, j));
     // The X1 mirror reads row X+1 of the array, logical (X, X) (:808).
-    vy[f.idx(X + 1, j)] = (X <= Y + 1) ? vyC(X, X) : vyC(X, j);
+    vy.put(f.idx(X + 1, j), (X <= Y + 1) ? vyC(X, X) : vyC(X, j));
   }
 }
 
 struct BubbleArrays {
   double *x, *y, *R_t, *R_p, *R_pn, *R_n, *R_nn, *d1_R_p, *d1_R_n, *PG_p, *PG_n, *PL_p, *PL_n, *PL_m, *Q_B, *n_B,
       *dt, *dt_n, *re, *re_n, *vbx, *vby, *R0, *contrib;
-  int *ibmx, *ibmy, *ibnx, *ibny, *bin;
+  int *ibmx, *ibmy, *ibnx, *ibny, *bin, *nsub;
   int n;
 };
 
@@ -264,9 +242,9 @@ __device__ __forceinline__ int bin_of(const Frame& f, int bx, int by) {
 // store_variables' bubble rotation (inc/bubble_CUDA_kernel.cuh:1241-1248),
 // BubbleInterpolationVelocityKernel (:398-448) and BubbleMotionKernel (:451-468),
 // plus the cell count for the bin sort.
+template <typename V>
 __global__ void bubble_move(const __grid_constant__ GridParams g, const __grid_constant__ BubbleParams bp,
-                            BubbleArrays b, const double* __restrict__ vx, const double* __restrict__ vy,
-                            int* __restrict__ bin_count) {
+                            BubbleArrays b, const V vx, const V vy, int* __restrict__ bin_count) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= b.n) return;
   const Frame& f = g.f;
@@ -285,14 +263,14 @@ __global__ void bubble_move(const __grid_constant__ GridParams g, const __grid_c
     double dxw = delta_x(bp, g, i, x);
     for (int j = iny; j <= iny + 1; j++) {
       double dyw = delta_y(bp, g, j, y);
-      if (i >= -1 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) vlx += vx[f.idx(i, j)] * dxw * dyw;
+      if (i >= -1 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) vlx += vx.get(f.idx(i, j)) * dxw * dyw;
     }
   }
   for (int i = inx; i <= inx + 1; i++) {
     double dxw = delta_x(bp, g, i, x);
     for (int j = imy - 1; j <= imy; j++) {
       double dyw = delta_y(bp, g, j, y);
-      if (i >= 0 && i <= f.X + 1 && j >= -1 && j <= f.Y + 1) vly += vy[f.idx(i, j)] * dxw * dyw;
+      if (i >= 0 && i <= f.X + 1 && j >= -1 && j <= f.Y + 1) vly += vy.get(f.idx(i, j)) * dxw * dyw;
     }
   }
   b.vbx[n] = vlx;
@@ -414,84 +392,186 @@ __global__ void bin_sort(const int* __restrict__ start, int* __restrict__ idx, i
   }
 }
 
-// BubbleInterpolationScalarKernel (:361-395) and BubbleRadiusKernel (:471-554)
-// for one bubble, then the bubble's void-fraction contribution to the cells of
-// its stencil (VoidFractionReverseLookupKernel, :595-617) stored for the gather.
-__global__ void __launch_bounds__(128) bubble_rp(const __grid_constant__ GridParams g,
-                                                 const __grid_constant__ BubbleParams bp, BubbleArrays b,
-                                                 const double* __restrict__ px, const double* __restrict__ py,
-                                                 double t_cur, long long* __restrict__ substep_max,
-                                                 int* __restrict__ err) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= b.n) return;
+// Per-bubble state of BubbleRadiusKernel (inc/bubble_CUDA_kernel.cuh:471-554)
+// while its sub-steps run.
+struct RpState {
+  double Rt, Rp, Rn, d1Rp, PGp, dtL, remain, time, PC0, PC1, PC2, heat, vis, re_n;
+  BubbleR0 r;
+  long long count;
+};
+
+// BubbleInterpolationScalarKernel (:361-395) for bubble n, then the set-up of
+// BubbleRadiusKernel from the state stored at the start of the step (:488-504).
+template <typename S>
+__device__ __forceinline__ void rp_begin(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
+                                         const S& px, const S& py, double t_cur, int n, RpState& s) {
   const Frame& f = g.f;
   const double x = b.x[n], y = b.y[n];
   const int inx = b.ibnx[n], iny = b.ibny[n];
-  double dxw[2], dyw[2];
-  for (int q = 0; q < 2; q++) {
-    dxw[q] = delta_x(bp, g, inx + q, x);
-    dyw[q] = delta_y(bp, g, iny + q, y);
-  }
   double PLp = 0.0;
   for (int qi = 0; qi < 2; qi++) {
-    int i = inx + qi;
+    const int i = inx + qi;
+    const double dxw = delta_x(bp, g, i, x);
     for (int qj = 0; qj < 2; qj++) {
-      int j = iny + qj;
-      if (i >= 0 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) PLp += p0_at(g, px, py, i, j, t_cur) * dxw[qi] * dyw[qj];
+      const int j = iny + qj;
+      const double dyw = delta_y(bp, g, j, y);
+      if (i >= 0 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) PLp += p0_at(g, px, py, i, j, t_cur) * dxw * dyw;
     }
   }
   b.PL_p[n] = PLp;
-
-  const BubbleR0 r = bubble_r0(bp, b.R0[n]);
+  s.r = bubble_r0(bp, b.R0[n]);
   const double dt = g.dt;
-  double Rt = b.R_t[n];
-  double Rp = b.R_pn[n], Rn = b.R_nn[n], d1Rp = b.d1_R_n[n], PGp = b.PG_n[n], dtL = b.dt_n[n];
-  const double re_n = b.re_n[n];
-  double remain = re_n + dt;
-  double time = -re_n;
+  s.Rt = b.R_t[n];
+  s.Rp = b.R_pn[n];
+  s.Rn = b.R_nn[n];
+  s.d1Rp = b.d1_R_n[n];
+  s.PGp = b.PG_n[n];
+  s.dtL = b.dt_n[n];
+  s.re_n = b.re_n[n];
+  s.remain = s.re_n + dt;
+  s.time = -s.re_n;
   const double PLn = b.PL_n[n], PLm = b.PL_m[n];
-  const double PC0 = PLn + bp.PL0;
-  const double PC1 = 0.5 * (PLp - PLm) / dt;
-  const double PC2 = 0.5 * (PLp + PLm - 2.0 * PLn) / (dt * dt);
-  double heat = 0.0, vis = 0.0;
-  long long count = 0;
-  while (remain > 0.0) {
-    if (count >= bp.step_cap) {
-      atomicOr(err, 1);
-      break;
-    }
-    double PGn = PGp;
-    double PL = PC2 * time * time + PC1 * time + PC0;
-    rp_substep(Rt, Rp, Rn, d1Rp, PGn, PL, dtL, remain, bp);
-    time = time + dtL;
-    C64 alpha;
-    double omega = omega_n(alpha, PGn, Rn, bp, r);
-    C64 lp = lp_n(alpha, Rn);
-    PGp = gas_pressure(PGn, Rp, Rn, omega, dtL, lp, bp, r);
-    double s0 = 0.5 * (Rp + Rn);
-    double s1 = 1.0 / (lp.re * lp.re + lp.im * lp.im) * bp.T0 / (r.PG0 * r.R03);
-    double dTdr = lp.re * s1 * (r.PG0 * r.R03 - 0.5 * (PGp + PGn) * s0 * s0 * s0) +
-                  lp.im * s1 * (PGp * Rp * Rp * Rp - PGn * Rn * Rn * Rn) / (omega * dtL);
-    heat -= 4.0 * bp.pi * Rp * Rp * bp.K0 * dTdr * dtL;
-    vis += 4.0 * bp.pi * Rp * Rp * 4.0 * bp.mu * d1Rp / Rp * d1Rp * dtL;
-    count++;
-  }
-  b.R_t[n] = Rt;
-  b.R_p[n] = Rp;
-  b.R_n[n] = Rn;
-  b.d1_R_p[n] = d1Rp;
-  b.PG_p[n] = PGp;
-  b.dt[n] = dtL;
-  b.re[n] = remain;
-  b.Q_B[n] = (heat + vis) / (dt - remain + re_n);
-  atomicMax(substep_max, count);
+  s.PC0 = PLn + bp.PL0;
+  s.PC1 = 0.5 * (PLp - PLm) / dt;
+  s.PC2 = 0.5 * (PLp + PLm - 2.0 * PLn) / (dt * dt);
+  s.heat = 0.0;
+  s.vis = 0.0;
+  s.count = 0;
+}
+
+// One pass of the sub-step loop of BubbleRadiusKernel (:506-539).  T is the
+// real type of the thermal model (omega_N, alpha_N, Lp_N); everything else is FP64.
+template <typename T>
+__device__ __forceinline__ void rp_substep_full(const BubbleParams& bp, RpState& s) {
+  const double PGn = s.PGp;
+  const double PL = s.PC2 * s.time * s.time + s.PC1 * s.time + s.PC0;
+  rp_substep(s.Rt, s.Rp, s.Rn, s.d1Rp, PGn, PL, s.dtL, s.remain, bp);
+  s.time = s.time + s.dtL;
+  Cx<T> alpha_t;
+  const double omega = (double)omega_n<T>(alpha_t, (T)PGn, (T)s.Rn, bp, s.r);
+  const Cx<T> lp_t = lp_n<T>(alpha_t, (T)s.Rn);
+  const C64 lp{(double)lp_t.re, (double)lp_t.im};
+  s.PGp = gas_pressure(PGn, s.Rp, s.Rn, omega, s.dtL, lp, bp, s.r);
+  const double Rp = s.Rp, Rn = s.Rn, PGp = s.PGp;
+  const double s0 = 0.5 * (Rp + Rn);
+  const double s1 = 1.0 / (lp.re * lp.re + lp.im * lp.im) * bp.T0 / (s.r.PG0 * s.r.R03);
+  const double dTdr = lp.re * s1 * (s.r.PG0 * s.r.R03 - 0.5 * (PGp + PGn) * s0 * s0 * s0) +
+                      lp.im * s1 * (PGp * Rp * Rp * Rp - PGn * Rn * Rn * Rn) / (omega * s.dtL);
+  s.heat -= 4.0 * bp.pi * Rp * Rp * bp.K0 * dTdr * s.dtL;
+  s.vis += 4.0 * bp.pi * Rp * Rp * 4.0 * bp.mu * s.d1Rp / Rp * s.d1Rp * s.dtL;
+  s.count++;
+}
+
+// Results of BubbleRadiusKernel (:542-550), then the bubble's void-fraction
+// contribution to the four cells of its stencil (VoidFractionReverseLookupKernel,
+// :595-617), stored for the per-cell gather.
+__device__ __forceinline__ void rp_end(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b, int n,
+                                       const RpState& s) {
+  const double dt = g.dt;
+  b.R_t[n] = s.Rt;
+  b.R_p[n] = s.Rp;
+  b.R_n[n] = s.Rn;
+  b.d1_R_p[n] = s.d1Rp;
+  b.PG_p[n] = s.PGp;
+  b.dt[n] = s.dtL;
+  b.re[n] = s.remain;
+  b.Q_B[n] = (s.heat + s.vis) / (dt - s.remain + s.re_n);
+  b.nsub[n] = (int)min(s.count, (long long)INT32_MAX);
+  const double x = b.x[n], y = b.y[n];
+  const int inx = b.ibnx[n], iny = b.ibny[n];
+  const double dx0 = delta_x(bp, g, inx, x), dx1 = delta_x(bp, g, inx + 1, x);
+  const double dy0 = delta_y(bp, g, iny, y), dy1 = delta_y(bp, g, iny + 1, y);
+  const double Rt = s.Rt;
   const double vol = g.cyl ? bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy / x
                            : bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy;
   double* c = b.contrib + 4 * (long)n;
-  c[0] = vol * dxw[0] * dyw[0];
-  c[1] = vol * dxw[0] * dyw[1];
-  c[2] = vol * dxw[1] * dyw[0];
-  c[3] = vol * dxw[1] * dyw[1];
+  c[0] = vol * dx0 * dy0;
+  c[1] = vol * dx0 * dy1;
+  c[2] = vol * dx1 * dy0;
+  c[3] = vol * dx1 * dy1;
+}
+
+// Persistent radius solve with a work queue.  Every lane takes the next bubble
+// from `order` (bubbles sorted by their previous sub-step count, heaviest
+// first) as soon as its current bubble finishes, and the loop advances every
+// active lane by one sub-step per pass, so a bubble that needs thousands of
+// sub-steps near collapse occupies one lane, not a warp, and no lane idles
+// while the queue has work.  Each bubble's arithmetic is the same as a
+// thread-per-bubble solve, so results do not depend on the schedule.
+constexpr int kRpThreads = 128;
+
+template <typename P>
+__global__ void __launch_bounds__(kRpThreads) bubble_rp(const __grid_constant__ GridParams g,
+                                                        const __grid_constant__ BubbleParams bp, BubbleArrays b,
+                                                        const typename P::S px, const typename P::S py,
+                                                        double t_cur, const int* __restrict__ order,
+                                                        int* __restrict__ next, long long* __restrict__ substep_max,
+                                                        int* __restrict__ err) {
+  RpState s;
+  int n = -1;
+  bool drained = false;
+  long long worst = 0;
+  for (;;) {
+    if (n < 0 && !drained) {
+      const int q = atomicAdd(next, 1);
+      if (q < b.n) {
+        n = order[q];
+        rp_begin(g, bp, b, px, py, t_cur, n, s);
+      } else {
+        drained = true;
+      }
+    }
+    if (!__any_sync(0xffffffffu, n >= 0)) break;
+    if (n >= 0) {
+      if (s.remain > 0.0 && s.count < bp.step_cap) {
+        rp_substep_full<typename P::T>(bp, s);
+      } else {
+        if (s.remain > 0.0) atomicOr(err, 1);
+        rp_end(g, bp, b, n, s);
+        worst = max(worst, s.count);
+        n = -1;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) worst = max(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+  if ((threadIdx.x & 31) == 0 && worst > 0) atomicMax(substep_max, worst);
+}
+
+// Work order for the next radius solves: bubbles bucketed by the binary
+// logarithm of their last sub-step count, heaviest bucket first.
+constexpr int kLptBuckets = 32;
+
+__device__ __forceinline__ int lpt_bucket(int nsub) {
+  return kLptBuckets - 1 - min(kLptBuckets - 1, 31 - __clz(max(nsub, 1)));
+}
+
+__global__ void lpt_count(const int* __restrict__ nsub, int n, int* __restrict__ hist) {
+  __shared__ int s_h[kLptBuckets];
+  if (threadIdx.x < kLptBuckets) s_h[threadIdx.x] = 0;
+  __syncthreads();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) atomicAdd(&s_h[lpt_bucket(nsub[k])], 1);
+  __syncthreads();
+  if (threadIdx.x < kLptBuckets && s_h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], s_h[threadIdx.x]);
+}
+
+// hist -> exclusive starts (one warp); hist is left zeroed for the next count.
+__global__ void lpt_scan(int* __restrict__ hist, int* __restrict__ cursor) {
+  const int lane = threadIdx.x;
+  int v = hist[lane];
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  cursor[lane] = x - v;
+  hist[lane] = 0;
+}
+
+__global__ void lpt_scatter(const int* __restrict__ nsub, int n, int* __restrict__ cursor, int* __restrict__ order) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  order[atomicAdd(&cursor[lpt_bucket(nsub[k])], 1)] = k;
 }
 
 // Void fraction of one cell from the bubbles of the four bins whose stencils
@@ -509,15 +589,13 @@ __device__ __forceinline__ double gather_fg(const Frame& f, const int* __restric
   return s;
 }
 
+template <typename P>
 struct CoupleArgs {
-  const double* vx;
-  const double* vy;
-  const double* pnx;
-  const double* pny;
-  double* px;
-  double* py;
-  double* fg;         // receives the gathered void fraction
-  const double* fgn;
+  typename P::V vx, vy;
+  typename P::S pnx, pny;
+  typename P::S px, py;
+  typename P::G fg;   // receives the gathered void fraction
+  typename P::G fgn;
   const int* start;
   const int* idx;
   const double* contrib;
@@ -528,7 +606,8 @@ struct CoupleArgs {
 // calculate_void_fraction (memset, scatter, VoidFractionCylinderKernel fold:
 // :1198-1218, :559-573) as a gather, then MixturePressureKernel (:816-867) on
 // the new void fraction and the residual of calculate_pressure_field.
-__global__ void __launch_bounds__(256) couple_press(const __grid_constant__ GridParams g, const CoupleArgs a) {
+template <typename P>
+__global__ void __launch_bounds__(256) couple_press(const __grid_constant__ GridParams g, const CoupleArgs<P> a) {
   const Frame& f = g.f;
   const int X = f.X, Y = f.Y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;       // 0..X+1
@@ -541,31 +620,33 @@ __global__ void __launch_bounds__(256) couple_press(const __grid_constant__ Grid
     else
       fgv = gather_fg(f, a.start, a.idx, a.contrib, i, j);
     long k = f.idx(i, j);
-    a.fg[k] = fgv;
+    a.fg.put(k, fgv);
+    fgv = a.fg.get(k);  // the stored value (FP32 in the mixed path) is what the step uses
     if (i >= 1 && i <= X && j >= 1 && j <= Y) {
       const double s3p = g.dt * g.rho_inf * g.c_inf * g.c_inf;
       const double s4p = 0.5 * g.dt * g.c_inf;
-      double vxl = a.vx[f.idx(i - 1, j)], vxr = a.vx[k];
+      double vxl = a.vx.get(f.idx(i - 1, j)), vxr = a.vx.get(k);
       double s1x = g.cyl ? (-g.xu[i] * vxl + g.xu[i + 1] * vxr) * g.rdx * g.rxp[i] : (-vxl + vxr) * g.rdx;
-      double s1y = (-a.vy[f.idx(i, j - 1)] + a.vy[k]) * g.rdy;
-      double fgn = a.fgn[k];
+      double s1y = (-a.vy.get(f.idx(i, j - 1)) + a.vy.get(k)) * g.rdy;
+      double fgn = a.fgn.get(k);
       double s5 = -(fgv - fgn) / g.dt / (1.0 - 0.5 * (fgv + fgn));
       double s2x = s4p * g.mx[i], s2y = s4p * g.my[j];
       double h = 0.5 * s5;
-      double qx = a.pnx[k] * (1.0 - s2x) - s3p * (s1x + h) / (1.0 + s2x);
-      double qy = a.pny[k] * (1.0 - s2y) - s3p * (s1y + h) / (1.0 + s2y);
+      double qx = a.pnx.get(k) * (1.0 - s2x) - s3p * (s1x + h) / (1.0 + s2x);
+      double qy = a.pny.get(k) * (1.0 - s2y) - s3p * (s1y + h) / (1.0 + s2y);
       bool forced = g.source_row > 0 && src_pressure(g) && j == g.source_row;
-      if (!forced) res = fabs((a.px[k] + a.py[k]) - (qx + qy));
-      a.px[k] = qx;
-      a.py[k] = qy;
+      if (!forced) res = fabs((a.px.get(k) + a.py.get(k)) - (qx + qy));
+      a.px.put(k, qx);
+      a.py.put(k, qy);
     }
   }
   block_max_to(res, a.residual);
 }
 
 // p0 with its boundary values into a dense (X+2) x (Y+2) array, for readback.
-__global__ void materialize_p0(const __grid_constant__ GridParams g, const double* __restrict__ px,
-                               const double* __restrict__ py, double t, double* __restrict__ out) {
+template <typename S>
+__global__ void materialize_p0(const __grid_constant__ GridParams g, const S px, const S py, double t,
+                               double* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i > g.f.X + 1 || j > g.f.Y + 1) return;
@@ -637,11 +718,16 @@ struct Sim {
   // Device memory: one allocation carved into aligned pieces.
   char* pool = nullptr;
   size_t pool_bytes = 0;
-  double* vx[2]{};
-  double* vy[2]{};
-  double* px[2]{};
-  double* py[2]{};
-  double* fg[3]{};
+  // Field buffers, 8 bytes per frame cell: one double (FP64 path) or an FP32
+  // value array followed by its FP32 compensation array (mixed path; f_g uses
+  // the first half only).
+  void* vx[2]{};
+  void* vy[2]{};
+  void* px[2]{};
+  void* py[2]{};
+  void* fg[3]{};
+  size_t cells = 0;  // frame cells per field
+  bool mixed = false;
   double* scratch = nullptr;  // dense (X+2) x (Y+2) doubles for readback
   double* d_sigma = nullptr;
   BubbleArrays bub{};
@@ -651,12 +737,20 @@ struct Sim {
     unsigned long long residual;  // max |dp0| as the bit pattern of a non-negative double
     long long substep_max;        // largest RP sub-step count of one bubble
     int err;                      // nonzero: a bubble hit the sub-step cap
+    int next;                     // work-queue head of the radius solve
   };
   Scalars* d_scalars = nullptr;
   unsigned long long* d_residual = nullptr;
   long long* d_substep_max = nullptr;
   int* d_err = nullptr;
+  int* d_next = nullptr;
   Scalars* h_scalars = nullptr;  // pinned
+  struct Lpt {
+    int* hist;    // kLptBuckets
+    int* cursor;  // kLptBuckets
+    int* order;   // n
+  } lpt{};
+  int rp_grid = 1;
 
   MinMax mm;       // running min/max of written rawdata values
   int cur_v = 0;   // velocity buffer holding the latest velocities
@@ -681,7 +775,7 @@ struct Sim {
 
   size_t layout(bool dry) {
     const Frame& f = gp.f;
-    size_t cells = (size_t)f.pitch * (f.Y + 4);
+    cells = (size_t)f.pitch * (f.Y + 4);
     size_t off = 0;
     for (int k = 0; k < 2; k++) {
       vx[k] = carve<double>(cells, off, dry);
@@ -697,6 +791,7 @@ struct Sim {
       d_residual = &d_scalars->residual;
       d_substep_max = &d_scalars->substep_max;
       d_err = &d_scalars->err;
+      d_next = &d_scalars->next;
     }
     const int n = hs.nb;
     bub.n = n;
@@ -705,7 +800,7 @@ struct Sim {
                      &bub.re, &bub.re_n, &bub.vbx, &bub.vby, &bub.R0};
     for (double** p : dp) *p = carve<double>(std::max(n, 1), off, dry);
     bub.contrib = carve<double>(4 * (size_t)std::max(n, 1), off, dry);
-    int** ip[] = {&bub.ibmx, &bub.ibmy, &bub.ibnx, &bub.ibny, &bub.bin};
+    int** ip[] = {&bub.ibmx, &bub.ibmy, &bub.ibnx, &bub.ibny, &bub.bin, &bub.nsub};
     for (int** p : ip) *p = carve<int>(std::max(n, 1), off, dry);
     bins.nbx = f.X + 3;
     bins.nby = f.Y + 3;
@@ -714,8 +809,15 @@ struct Sim {
     bins.start = carve<int>(bins.nbins + 1, off, dry);
     bins.idx = carve<int>(std::max(n, 1), off, dry);
     bins.partial = carve<int>((bins.nbins + kScanThreads - 1) / kScanThreads + 1, off, dry);
+    lpt.hist = carve<int>(kLptBuckets, off, dry);
+    lpt.cursor = carve<int>(kLptBuckets, off, dry);
+    lpt.order = carve<int>(std::max(n, 1), off, dry);
     return off;
   }
+
+  // Typed views of the raw field buffers.
+  template <typename A>
+  A view(void* b) const;
 
   // Launch one kernel (the callable enqueues it on `stream`), counted by class
   // and bracketed by profiling events when profiling is on.
@@ -736,8 +838,9 @@ struct Sim {
     if (st != CRP_OK) return st;
     if (cfg.sim_order != 2 || cfg.sim_smooth_delta_band != 2)
       return fail(CRP_ERR_UNSUPPORTED, "the CUDA path implements simulation.order = 2 and smooth_delta_band = 2");
-    if (cfg.ext_precision != CRP_PREC_FP64)
-      return fail(CRP_ERR_UNSUPPORTED, "ext.precision = mixed is not available in this build");
+    if (cfg.ext_precision != CRP_PREC_FP64 && cfg.ext_precision != CRP_PREC_MIXED)
+      return fail(CRP_ERR_INVALID, "ext.precision must be fp64 or mixed");
+    mixed = cfg.ext_precision == CRP_PREC_MIXED;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CRP_ERR_NO_DEVICE, "no CUDA device");
     if (user_stream) {
@@ -752,6 +855,16 @@ struct Sim {
     layout(false);
     CRP_CUDA(cudaMemsetAsync(pool, 0, pool_bytes, stream));
     CRP_CUDA(cudaMallocHost(&h_scalars, sizeof(Scalars)));
+    {
+      int dev = 0, sms = 0, per_sm = 0;
+      CRP_CUDA(cudaGetDevice(&dev));
+      CRP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      if (mixed)
+        CRP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bubble_rp<PrecMixed>, kRpThreads, 0));
+      else
+        CRP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bubble_rp<PrecFP64>, kRpThreads, 0));
+      rp_grid = std::max(1, std::min(sms * std::max(per_sm, 1), (hs.nb + kRpThreads - 1) / kRpThreads));
+    }
     // PML profiles and metrics.
     CRP_CUDA(cudaMemcpyAsync(d_sigma, hs.sigma_block.data(), sizeof(double) * hs.sigma_block.size(),
                              cudaMemcpyHostToDevice, stream));
@@ -778,7 +891,7 @@ struct Sim {
       CRP_CUDA(build_bins());
       CRP_CUDA(launch_contrib_only());
       CRP_CUDA(launch_couple(/*pressure=*/false));
-      size_t bytes = sizeof(double) * (size_t)gp.f.pitch * (gp.f.Y + 4);
+      size_t bytes = sizeof(double) * cells;
       CRP_CUDA(cudaMemcpyAsync(fg[fg_b], fg[fg_a], bytes, cudaMemcpyDeviceToDevice, stream));
       CRP_CUDA(cudaMemcpyAsync(fg[fg_c], fg[fg_a], bytes, cudaMemcpyDeviceToDevice, stream));
     }
@@ -869,6 +982,19 @@ struct Sim {
     return launch(kClassOther, [&] { bin_sort<<<(nbins + 255) / 256, 256, 0, stream>>>(bins.start, bins.idx, nbins); });
   }
 
+  // Radius-solve order from the last sub-step counts (heaviest first).
+  cudaError_t build_order() {
+    const int n = bub.n;
+    cudaError_t e;
+    if ((e = launch(kClassOther, [&] { lpt_count<<<(n + 255) / 256, 256, 0, stream>>>(bub.nsub, n, lpt.hist); })) !=
+        cudaSuccess)
+      return e;
+    if ((e = launch(kClassOther, [&] { lpt_scan<<<1, 32, 0, stream>>>(lpt.hist, lpt.cursor); })) != cudaSuccess)
+      return e;
+    return launch(kClassOther,
+                  [&] { lpt_scatter<<<(n + 255) / 256, 256, 0, stream>>>(bub.nsub, n, lpt.cursor, lpt.order); });
+  }
+
   // Void-fraction contributions of the initial radii (no RP step).
   cudaError_t launch_contrib_only();
 
@@ -893,40 +1019,16 @@ struct Sim {
     // Ring rotation of store_variables: the predicted f_g goes to the f_gm buffer.
     const int a = fg_a, b = fg_b, c = fg_c;
     CRP_CUDA(cudaMemsetAsync(d_residual, 0, sizeof(unsigned long long), stream));
-    FdtdArgs fa;
-    fa.vx_old = vx[cur_v];
-    fa.vy_old = vy[cur_v];
-    fa.vx_new = vx[nv];
-    fa.vy_new = vy[nv];
-    fa.pnx = px[cur_p];
-    fa.pny = py[cur_p];
-    fa.px = px[np];
-    fa.py = py[np];
-    fa.fgA = fg[a];
-    fa.fgB = fg[b];
-    fa.fgC = fg[c];
-    fa.t_prev = t_prev;
-    fa.t_cur = tstep;
-    fa.rho_const = stats.steps == 0 ? 1 : 0;
-    fa.residual = d_residual;
-    dim3 grid((gp.f.X + (kFdtdThreads - 2) - 1) / (kFdtdThreads - 2), (gp.f.Y + kFdtdRows - 1) / kFdtdRows);
-    CRP_CUDA(launch(kClassFdtd, [&] { fdtd_step<<<grid, kFdtdThreads, 0, stream>>>(gp, fa); }));
-    int ng = std::max(gp.f.X, gp.f.Y) + 3;
-    double* vxn = vx[nv];
-    double* vyn = vy[nv];
-    CRP_CUDA(launch(kClassOther, [&] { vghost<<<(ng + 255) / 256, 256, 0, stream>>>(gp, vxn, vyn); }));
+    CRP_CUDA(mixed ? launch_fdtd<PrecMixed>(nv, np, a, b, c) : launch_fdtd<PrecFP64>(nv, np, a, b, c));
     cur_v = nv;
     cur_p = np;
     fg_a = c;  // predicted f_g
     fg_b = a;  // f_gn
     fg_c = b;  // f_gm
     if (hs.nb > 0) {
-      const double* vxc = vx[cur_v];
-      const double* vyc = vy[cur_v];
-      CRP_CUDA(launch(kClassOther, [&] {
-        bubble_move<<<(bub.n + 255) / 256, 256, 0, stream>>>(gp, bp, bub, vxc, vyc, bins.count);
-      }));
+      CRP_CUDA(mixed ? launch_move<PrecMixed>() : launch_move<PrecFP64>());
       CRP_CUDA(build_bins());
+      CRP_CUDA(build_order());
     }
     crp_status st = read_scalars();
     if (st != CRP_OK) return st;
@@ -937,12 +1039,8 @@ struct Sim {
         if (loop >= cfg.ext_picard_cap) return fail(CRP_ERR_PICARD, "Picard iteration cap reached");
         loop++;
         CRP_CUDA(cudaMemsetAsync(d_residual, 0, sizeof(unsigned long long), stream));
-        const double* pxc = px[cur_p];
-        const double* pyc = py[cur_p];
-        const double tc = tstep;
-        CRP_CUDA(launch(kClassRp, [&] {
-          bubble_rp<<<(bub.n + 127) / 128, 128, 0, stream>>>(gp, bp, bub, pxc, pyc, tc, d_substep_max, d_err);
-        }));
+        CRP_CUDA(cudaMemsetAsync(d_next, 0, sizeof(int), stream));
+        CRP_CUDA(mixed ? launch_rp<PrecMixed>() : launch_rp<PrecFP64>());
         CRP_CUDA(launch_couple(true));
         st = read_scalars();
         if (st != CRP_OK) return st;
@@ -979,37 +1077,51 @@ struct Sim {
     return d;
   }
 
-  crp_status read_field(crp_field which, double* host) {
+  // Copy the window [ilo, ihi] x [jlo, jhi] of a field buffer into a dense
+  // double array.  kind: 0 FP64, 1 FP32 value + compensation, 2 FP32.
+  crp_status copy_window(const void* buf, int kind, int ilo, int ihi, int jlo, int jhi, double* host) {
     const Frame& f = gp.f;
-    auto copy_window = [&](const double* base, int ilo, int ihi, int jlo, int jhi) -> crp_status {
-      int w = ihi - ilo + 1, h = jhi - jlo + 1;
-      CRP_CUDA(cudaMemcpy2DAsync(host, sizeof(double) * w, base + f.idx(ilo, jlo), sizeof(double) * f.pitch,
+    const int w = ihi - ilo + 1, h = jhi - jlo + 1;
+    const long off = f.idx(ilo, jlo);
+    if (kind == 0) {
+      CRP_CUDA(cudaMemcpy2DAsync(host, sizeof(double) * w, (const double*)buf + off, sizeof(double) * f.pitch,
                                  sizeof(double) * w, h, cudaMemcpyDeviceToHost, stream));
       CRP_CUDA(cudaStreamSynchronize(stream));
       return CRP_OK;
-    };
-    const int X = f.X, Y = f.Y;
+    }
+    std::vector<float> hi((size_t)w * h), lo(kind == 1 ? (size_t)w * h : 0);
+    const float* fb = (const float*)buf;
+    CRP_CUDA(cudaMemcpy2DAsync(hi.data(), sizeof(float) * w, fb + off, sizeof(float) * f.pitch, sizeof(float) * w, h,
+                               cudaMemcpyDeviceToHost, stream));
+    if (kind == 1)
+      CRP_CUDA(cudaMemcpy2DAsync(lo.data(), sizeof(float) * w, fb + cells + off, sizeof(float) * f.pitch,
+                                 sizeof(float) * w, h, cudaMemcpyDeviceToHost, stream));
+    CRP_CUDA(cudaStreamSynchronize(stream));
+    for (size_t q = 0; q < hi.size(); q++) host[q] = (double)hi[q] + (kind == 1 ? (double)lo[q] : 0.0);
+    return CRP_OK;
+  }
+
+  crp_status read_field(crp_field which, double* host) {
+    const int X = gp.f.X, Y = gp.f.Y;
+    const int kv = mixed ? 1 : 0, kg = mixed ? 2 : 0;
     switch (which) {
       case CRP_FIELD_P0: {
-        dim3 blk(32, 8), grd((X + 2 + 31) / 32, (Y + 2 + 7) / 8);
-        const double* pxc = px[cur_p];
-        const double* pyc = py[cur_p];
-        CRP_CUDA(launch(kClassOther, [&] { materialize_p0<<<grd, blk, 0, stream>>>(gp, pxc, pyc, tstep, scratch); }));
+        CRP_CUDA(mixed ? launch_p0<PrecMixed>() : launch_p0<PrecFP64>());
         CRP_CUDA(cudaMemcpyAsync(host, scratch, sizeof(double) * (X + 2) * (Y + 2), cudaMemcpyDeviceToHost, stream));
         CRP_CUDA(cudaStreamSynchronize(stream));
         return CRP_OK;
       }
-      case CRP_FIELD_PX: return copy_window(px[cur_p], 0, X + 1, 0, Y + 1);
-      case CRP_FIELD_PY: return copy_window(py[cur_p], 0, X + 1, 0, Y + 1);
-      case CRP_FIELD_PNX: return copy_window(px[cur_p ^ 1], 0, X + 1, 0, Y + 1);
-      case CRP_FIELD_PNY: return copy_window(py[cur_p ^ 1], 0, X + 1, 0, Y + 1);
-      case CRP_FIELD_VX: return copy_window(vx[cur_v], -1, X + 1, 0, Y + 1);
-      case CRP_FIELD_VY: return copy_window(vy[cur_v], 0, X + 1, -1, Y + 1);
-      case CRP_FIELD_FG: return copy_window(fg[fg_a], 0, X + 1, 0, Y + 1);
-      case CRP_FIELD_FGN: return copy_window(fg[fg_b], 0, X + 1, 0, Y + 1);
-      case CRP_FIELD_FGM: return copy_window(fg[fg_c], 0, X + 1, 0, Y + 1);
+      case CRP_FIELD_PX: return copy_window(px[cur_p], kv, 0, X + 1, 0, Y + 1, host);
+      case CRP_FIELD_PY: return copy_window(py[cur_p], kv, 0, X + 1, 0, Y + 1, host);
+      case CRP_FIELD_PNX: return copy_window(px[cur_p ^ 1], kv, 0, X + 1, 0, Y + 1, host);
+      case CRP_FIELD_PNY: return copy_window(py[cur_p ^ 1], kv, 0, X + 1, 0, Y + 1, host);
+      case CRP_FIELD_VX: return copy_window(vx[cur_v], kv, -1, X + 1, 0, Y + 1, host);
+      case CRP_FIELD_VY: return copy_window(vy[cur_v], kv, 0, X + 1, -1, Y + 1, host);
+      case CRP_FIELD_FG: return copy_window(fg[fg_a], kg, 0, X + 1, 0, Y + 1, host);
+      case CRP_FIELD_FGN: return copy_window(fg[fg_b], kg, 0, X + 1, 0, Y + 1, host);
+      case CRP_FIELD_FGM: return copy_window(fg[fg_c], kg, 0, X + 1, 0, Y + 1, host);
       case CRP_FIELD_RHO_M: {
-        crp_status st = copy_window(fg[fg_a], 0, X + 1, 0, Y + 1);
+        crp_status st = copy_window(fg[fg_a], kg, 0, X + 1, 0, Y + 1, host);
         if (st != CRP_OK) return st;
         size_t n = (size_t)(X + 2) * (Y + 2);
         for (size_t k = 0; k < n; k++) host[k] = stats.steps == 0 ? gp.rho_inf : (1.0 - host[k]) * gp.rho_inf;
@@ -1018,6 +1130,69 @@ struct Sim {
     }
     return fail(CRP_ERR_INVALID, "unknown field");
   }
+
+  // Per-precision launches.
+  template <typename P>
+  cudaError_t launch_fdtd(int nv, int np, int a, int b, int c) {
+    using V = typename P::V;
+    using S = typename P::S;
+    using G = typename P::G;
+    FdtdArgs<P> fa;
+    fa.vx_old = view<V>(vx[cur_v]);
+    fa.vy_old = view<V>(vy[cur_v]);
+    fa.vx_new = view<V>(vx[nv]);
+    fa.vy_new = view<V>(vy[nv]);
+    fa.pnx = view<S>(px[cur_p]);
+    fa.pny = view<S>(py[cur_p]);
+    fa.px = view<S>(px[np]);
+    fa.py = view<S>(py[np]);
+    fa.fgA = view<G>(fg[a]);
+    fa.fgB = view<G>(fg[b]);
+    fa.fgC = view<G>(fg[c]);
+    fa.t_prev = t_prev;
+    fa.t_cur = tstep;
+    fa.rho_const = stats.steps == 0 ? 1 : 0;
+    fa.residual = d_residual;
+    dim3 grid((gp.f.X + 2 + kFdtdBX - 1) / kFdtdBX, (gp.f.Y + 2 + kFdtdBY - 1) / kFdtdBY);
+    dim3 block(kFdtdBX, kFdtdBY);
+    cudaError_t e = launch(kClassFdtd, [&] { fdtd_step<P><<<grid, block, 0, stream>>>(gp, fa); });
+    if (e != cudaSuccess) return e;
+    const int ng = std::max(gp.f.X, gp.f.Y) + 3;
+    const V vxn = view<V>(vx[nv]), vyn = view<V>(vy[nv]);
+    return launch(kClassOther, [&] { vghost<V><<<(ng + 255) / 256, 256, 0, stream>>>(gp, vxn, vyn); });
+  }
+
+  template <typename P>
+  cudaError_t launch_move() {
+    using V = typename P::V;
+    const V vxc = view<V>(vx[cur_v]), vyc = view<V>(vy[cur_v]);
+    return launch(kClassOther, [&] {
+      bubble_move<V><<<(bub.n + 255) / 256, 256, 0, stream>>>(gp, bp, bub, vxc, vyc, bins.count);
+    });
+  }
+
+  template <typename P>
+  cudaError_t launch_rp() {
+    using S = typename P::S;
+    const S pxc = view<S>(px[cur_p]), pyc = view<S>(py[cur_p]);
+    const double tc = tstep;
+    return launch(kClassRp, [&] {
+      bubble_rp<P><<<rp_grid, kRpThreads, 0, stream>>>(gp, bp, bub, pxc, pyc, tc, lpt.order, d_next, d_substep_max,
+                                                        d_err);
+    });
+  }
+
+  template <typename P>
+  cudaError_t launch_p0() {
+    using S = typename P::S;
+    const S pxc = view<S>(px[cur_p]), pyc = view<S>(py[cur_p]);
+    dim3 blk(32, 8), grd((gp.f.X + 2 + 31) / 32, (gp.f.Y + 2 + 7) / 8);
+    return launch(kClassOther,
+                  [&] { materialize_p0<S><<<grd, blk, 0, stream>>>(gp, pxc, pyc, tstep, scratch); });
+  }
+
+  template <typename P>
+  cudaError_t launch_couple_t(bool pressure);
 
   crp_status read_bubbles(crp_bubble_field w, double* host) {
     const int n = bub.n;
@@ -1046,6 +1221,7 @@ struct Sim {
       case CRP_BUB_IBM_Y: isrc = bub.ibmy; break;
       case CRP_BUB_IBN_X: isrc = bub.ibnx; break;
       case CRP_BUB_IBN_Y: isrc = bub.ibny; break;
+      case CRP_BUB_SUBSTEPS: isrc = bub.nsub; break;
       default: return fail(CRP_ERR_INVALID, "unknown bubble field");
     }
     if (src) {
@@ -1090,7 +1266,8 @@ __global__ void bubble_contrib(const __grid_constant__ GridParams g, const __gri
 }
 
 // Gather-only variant of couple_press for the initial void fraction.
-__global__ void __launch_bounds__(256) couple_fg_only(const __grid_constant__ GridParams g, const CoupleArgs a) {
+template <typename P>
+__global__ void __launch_bounds__(256) couple_fg_only(const __grid_constant__ GridParams g, const CoupleArgs<P> a) {
   const Frame& f = g.f;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1100,31 +1277,52 @@ __global__ void __launch_bounds__(256) couple_fg_only(const __grid_constant__ Gr
     fgv = gather_fg(f, a.start, a.idx, a.contrib, 0, j) + gather_fg(f, a.start, a.idx, a.contrib, 1, j);
   else
     fgv = gather_fg(f, a.start, a.idx, a.contrib, i, j);
-  a.fg[f.idx(i, j)] = fgv;
+  a.fg.put(f.idx(i, j), fgv);
 }
 
 cudaError_t Sim::launch_contrib_only() {
   return launch(kClassOther, [&] { bubble_contrib<<<(bub.n + 255) / 256, 256, 0, stream>>>(gp, bp, bub); });
 }
 
-cudaError_t Sim::launch_couple(bool pressure) {
-  CoupleArgs ca;
-  ca.vx = vx[cur_v];
-  ca.vy = vy[cur_v];
-  ca.pnx = px[cur_p ^ 1];
-  ca.pny = py[cur_p ^ 1];
-  ca.px = px[cur_p];
-  ca.py = py[cur_p];
-  ca.fg = fg[fg_a];
-  ca.fgn = fg[fg_b];
+template <>
+F64 Sim::view<F64>(void* b) const {
+  return F64{(double*)b};
+}
+template <>
+F32c Sim::view<F32c>(void* b) const {
+  return F32c{(float*)b, (float*)b + cells};
+}
+template <>
+F32 Sim::view<F32>(void* b) const {
+  return F32{(float*)b};
+}
+
+template <typename P>
+cudaError_t Sim::launch_couple_t(bool pressure) {
+  using V = typename P::V;
+  using S = typename P::S;
+  using G = typename P::G;
+  CoupleArgs<P> ca;
+  ca.vx = view<V>(vx[cur_v]);
+  ca.vy = view<V>(vy[cur_v]);
+  ca.pnx = view<S>(px[cur_p ^ 1]);
+  ca.pny = view<S>(py[cur_p ^ 1]);
+  ca.px = view<S>(px[cur_p]);
+  ca.py = view<S>(py[cur_p]);
+  ca.fg = view<G>(fg[fg_a]);
+  ca.fgn = view<G>(fg[fg_b]);
   ca.start = bins.start;
   ca.idx = bins.idx;
   ca.contrib = bub.contrib;
   ca.t_cur = tstep;
   ca.residual = d_residual;
   dim3 blk(32, 8), grd((gp.f.X + 2 + 31) / 32, (gp.f.Y + 2 + 7) / 8);
-  if (pressure) return launch(kClassCouple, [&] { couple_press<<<grd, blk, 0, stream>>>(gp, ca); });
-  return launch(kClassOther, [&] { couple_fg_only<<<grd, blk, 0, stream>>>(gp, ca); });
+  if (pressure) return launch(kClassCouple, [&] { couple_press<P><<<grd, blk, 0, stream>>>(gp, ca); });
+  return launch(kClassOther, [&] { couple_fg_only<P><<<grd, blk, 0, stream>>>(gp, ca); });
+}
+
+cudaError_t Sim::launch_couple(bool pressure) {
+  return mixed ? launch_couple_t<PrecMixed>(pressure) : launch_couple_t<PrecFP64>(pressure);
 }
 
 }  // namespace crp

@@ -133,7 +133,8 @@ typedef enum crp_bubble_field {
   CRP_BUB_D1R = 5, CRP_BUB_PG = 6, CRP_BUB_PL_P = 7, CRP_BUB_PL_N = 8, CRP_BUB_PL_M = 9,
   CRP_BUB_DT = 10, CRP_BUB_RE = 11, CRP_BUB_Q_B = 12, CRP_BUB_N_B = 13, CRP_BUB_R0 = 14,
   CRP_BUB_VX = 15, CRP_BUB_VY = 16,
-  CRP_BUB_IBM_X = 17, CRP_BUB_IBM_Y = 18, CRP_BUB_IBN_X = 19, CRP_BUB_IBN_Y = 20
+  CRP_BUB_IBM_X = 17, CRP_BUB_IBM_Y = 18, CRP_BUB_IBN_X = 19, CRP_BUB_IBN_Y = 20,
+  CRP_BUB_SUBSTEPS = 21  /* RP sub-steps of the bubble's last radius solve */
 } crp_bubble_field;
 
 typedef struct crp_dims {

@@ -31,10 +31,11 @@ echo "#include \"$ref/src/SphDataType.cpp\"" > "$out/ref_sph.cpp"
 NVCC="${NVCC:-nvcc}"
 inc=(-I"$out/stubs" -I"$here/ref_stubs")
 arch=(-gencode arch=compute_100a,code=sm_100a)
-# The reference's C++ relies on -O0 host code in one place: save_ascii
-# (src/output_styles.cpp:139-341) has no return statement.
+# save_ascii (src/output_styles.cpp:139-341) has no return statement; GCC 13
+# turns the end of such a function into a trap even at -O0, so that unit is
+# built with -fno-unreachable-traps.
 "$NVCC" -std=c++17 "${arch[@]}" "${inc[@]}" -w -Xcompiler -fPIC -Xcompiler -O2 -c "$out/ref_main.cu" -o "$out/ref_main.o"
-"$NVCC" -std=c++17 "${arch[@]}" "${inc[@]}" -w -Xcompiler -fPIC -Xcompiler -O0 -c "$out/ref_output.cu" -o "$out/ref_output.o"
+"$NVCC" -std=c++17 "${arch[@]}" "${inc[@]}" -w -Xcompiler -fPIC -Xcompiler -O0 -Xcompiler -fno-unreachable-traps -c "$out/ref_output.cu" -o "$out/ref_output.o"
 g++ -std=c++17 -fPIC -O0 -w "${inc[@]}" -c "$out/ref_sph.cpp" -o "$out/ref_sph.o"
 "$NVCC" -shared "${arch[@]}" -o "$out/libcrp_ref.so" "$out/ref_main.o" "$out/ref_output.o" "$out/ref_sph.o" -lpthread
 echo "build_ref: built $out/libcrp_ref.so"

@@ -365,7 +365,7 @@ struct crpo_sim {
   std::vector<BubConst> bc;
   std::vector<double> x, y, R_t, R_p, R_pn, R_n, R_nn, d1_R_p, d1_R_n, PG_p, PG_n, PL_p, PL_n, PL_m, Q_B,
       n_B, dtb, dt_n, re, re_n, vbx, vby;
-  std::vector<int> ibmx, ibmy, ibnx, ibny;
+  std::vector<int> ibmx, ibmy, ibnx, ibny, nsub;
   double tstep = 0.0, tstepx = 0.0;
   int64_t nstep = 0;
   crp_stats stats{};
@@ -488,6 +488,7 @@ struct crpo_sim {
     ibmy.push_back(0);
     ibnx.push_back(0);
     ibny.push_back(0);
+    nsub.push_back(0);
   }
 
   crp_status init_bubbles(const crp_bubbles_in* bin) {
@@ -820,6 +821,7 @@ struct crpo_sim {
       dtb[b] = dtL;
       re[b] = remain;
       Q_B[b] = (heat + vis) / (dt - remain + re_n[b]);
+      nsub[b] = (int)std::min<int64_t>(count, INT32_MAX);
       worst = std::max(worst, count);
     }
     return capped ? -1 : worst;
@@ -964,6 +966,7 @@ crp_status crpo_read_bubbles(crpo_sim* s, crp_bubble_field w, double* host) {
     case CRP_BUB_IBM_Y: iv = &s->ibmy; break;
     case CRP_BUB_IBN_X: iv = &s->ibnx; break;
     case CRP_BUB_IBN_Y: iv = &s->ibny; break;
+    case CRP_BUB_SUBSTEPS: iv = &s->nsub; break;
     case CRP_BUB_R0:
       for (int b = 0; b < s->nb; b++) host[b] = s->bc[b].R0;
       return CRP_OK;
@@ -1045,6 +1048,36 @@ void crpo_host_scalars(const crp_config* cfg, double* out) {
                   d.T_inf, b.PG0, b.R03, b.coeff_alpha, d.bub_dt0, (double)d.mbs, (double)d.mbe,
                   (double)d.nbs, (double)d.nbe, d.focal_dist};
   std::memcpy(out, o, sizeof(o));
+}
+
+int64_t crpo_bubble_history(const double* bp, double R_init, double dt_mix, double dpl, int32_t nsteps, double* R_out,
+                            double* PG_out) {
+  // One bubble of BubbleRadiusKernel (inc/bubble_CUDA_kernel.cuh:485-550) advanced
+  // nsteps mixture steps in a liquid held at PL0 + dpl, from rest at R_init.
+  BubConst b = bub_from(bp);
+  double Rt = R_init, Rp = R_init, Rn = R_init, d1R = 0.0, PGp = b.PG0 * std::pow(b.R0 / R_init, 3.0 * b.gam),
+         dtL = b.dt0, re = 0.0;
+  int64_t total = 0;
+  for (int s = 0; s < nsteps; s++) {
+    double remain = re + dt_mix, time = -re;
+    double PC0 = dpl + b.PL0;
+    while (remain > 0.0) {
+      double PGn = PGp;
+      double PL = 0.0 * time * time + 0.0 * time + PC0;
+      rp_substep(Rt, Rp, Rn, d1R, PGn, PL, dtL, remain, b);
+      time = time + dtL;
+      Cplx alpha;
+      double omega = thermal_omega(alpha, PGn, Rn, b);
+      Cplx lp = thermal_lp(alpha, Rn);
+      PGp = gas_pressure(PGn, Rp, Rn, omega, dtL, lp, b);
+      total++;
+      if (total > 100000000) return -1;
+    }
+    re = remain;
+    R_out[s] = Rt;
+    PG_out[s] = PGp;
+  }
+  return total;
 }
 
 crp_status crpo_host_sigma(const crp_config* cfg, double* mx, double* my, double* nx, double* ny, double* xu,

@@ -44,6 +44,12 @@ double crpo_omega_n(const double* bp, double PG, double R, double* alpha /* re, 
 void crpo_upsilon_lp(double are, double aim, double gam, double R, double* out /* U re,im, Lp re,im */);
 double crpo_solve_pg(const double* bp, double PGn, double Rp, double Rn, double omega_N, double dt,
                      double lp_re, double lp_im);
+/* One bubble from rest at R_init advanced nsteps mixture steps (length dt_mix)
+ * in a liquid held at P0 + dpl, with the sub-stepping and thermal gas model of
+ * the radius kernel.  R_out/PG_out get R_t and PG after each step.  Returns the
+ * total number of sub-steps (-1 if it exceeded 1e8). */
+int64_t crpo_bubble_history(const double* bp, double R_init, double dt_mix, double dpl, int32_t nsteps, double* R_out,
+                            double* PG_out);
 /* Derived scalars in the order of crp_ref_host_scalars (oracle/ref_harness.inc). */
 void crpo_host_scalars(const crp_config* cfg, double* out);
 /* PML profiles and cylindrical metrics: mx[i1m], my[j1m], nx[i2n], ny[j2n], xu[i2n], rxp[i2m]. */
