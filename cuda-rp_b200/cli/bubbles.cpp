@@ -51,7 +51,7 @@ const char* kFileKeys =
     "  debug.p debug.p_max debug.v debug.v_min debug.v_max debug.bubbles\n"
     "  ext.rho_inf ext.c_inf ext.p_inf ext.source_row ext.ramp_cycles ext.precision\n"
     "  ext.picard_cap ext.rp_step_cap ext.bubble_count ext.bubble_seed ext.r0_sigma_ln\n"
-    "  ext.cloud_shape ext.cloud_r ext.cloud_h ext.n_b\n";
+    "  ext.cloud_shape ext.cloud_r ext.cloud_h ext.n_b ext.picard_tol\n";
 
 // Optional overrides of the *_minmax.txt values (src/bubbles.cpp:275-294).  The
 // reference registers the p_min key as "debug p_min" (a typo), so only

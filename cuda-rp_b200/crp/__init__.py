@@ -45,7 +45,7 @@ class Config(ctypes.Structure):
         ("ext_source_row", c_int), ("ext_ramp_cycles", c_dbl), ("ext_precision", c_int),
         ("ext_picard_cap", c_int), ("ext_rp_step_cap", c_int), ("ext_bubble_count", c_int),
         ("ext_bubble_seed", ctypes.c_uint64), ("ext_r0_sigma_ln", c_dbl), ("ext_cloud_shape", c_int),
-        ("ext_cloud_r", c_dbl), ("ext_cloud_h", c_dbl), ("ext_n_b", c_dbl),
+        ("ext_cloud_r", c_dbl), ("ext_cloud_h", c_dbl), ("ext_n_b", c_dbl), ("ext_picard_tol", c_dbl),
     ]
 
 

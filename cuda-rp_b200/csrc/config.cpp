@@ -156,6 +156,7 @@ const Key kKeys[] = {
     K("ext.cloud_r", kDouble, ext_cloud_r),
     K("ext.cloud_h", kDouble, ext_cloud_h),
     K("ext.n_b", kDouble, ext_n_b),
+    K("ext.picard_tol", kDouble, ext_picard_tol),
 };
 #undef K
 

@@ -36,6 +36,8 @@ struct GridParams {
   double amp, pamp, freq, omega;
   double on_time, period, ramp_time;
   double ctl_x, ctl_y, focal_dist;  // focal_point_c, focal_dist_c
+  double dt_rho;    // dt / rho_inf
+  double s3p, s4p;  // dt rho_inf c_inf^2 and dt c_inf / 2 of MixturePressureKernel (:852-853)
   // PML profiles and cylindrical metrics, indexed by logical i or j:
   // mx[i] i in [0,X+1], my[j] j in [0,Y+1], nx[i+1] i in [-1,X+1], ny[j+1] j in [-1,Y+1],
   // xu[i+1] i in [-1,X+1], rxp[i] i in [0,X+1].
@@ -161,6 +163,10 @@ template <typename R>
 struct Cx {
   R re, im;
 };
+// Division in the thermal model: IEEE in FP64, the fast approximate FP32
+// division (max 2 ulp) in the mixed path.
+__device__ __forceinline__ double xdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float xdiv(float a, float b) { return __fdividef(a, b); }
 template <typename R>
 __device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
   return {a.re * b.re - a.im * b.im, a.im * b.re + a.re * b.im};
@@ -168,12 +174,12 @@ __device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
 template <typename R>
 __device__ __forceinline__ Cx<R> cdiv(Cx<R> a, Cx<R> b) {
   R c = b.re * b.re + b.im * b.im;
-  return {(a.re * b.re + a.im * b.im) / c, (a.im * b.re - a.re * b.im) / c};
+  return {xdiv(a.re * b.re + a.im * b.im, c), xdiv(a.im * b.re - a.re * b.im, c)};
 }
 template <typename R>
 __device__ __forceinline__ Cx<R> rdiv(R a, Cx<R> b) {
   R c = b.re * b.re + b.im * b.im;
-  return {a * b.re / c, -a * b.im / c};
+  return {xdiv(a * b.re, c), xdiv(-a * b.im, c)};
 }
 template <typename R>
 __device__ __forceinline__ Cx<R> cscl(Cx<R> a, R s) {
@@ -212,7 +218,7 @@ __device__ __forceinline__ Cx<R> upsilon(Cx<R> a, R gam) {
     Cx<R> ac = cmul(a, ccoth(a));
     t = cdiv(Cx<R>{ac.re - R(1), ac.im}, aa);
   } else {
-    Cx<R> q = cmul(aa, Cx<R>{R(2.0 / 945.0) - aa.re / R(4725.0), -aa.im / R(4725.0)});
+    Cx<R> q = cmul(aa, Cx<R>{R(2.0 / 945.0) - xdiv(aa.re, R(4725.0)), xdiv(-aa.im, R(4725.0))});
     Cx<R> m = cmul(aa, Cx<R>{R(-1.0 / 45.0) + q.re, q.im});
     t = Cx<R>{R(1.0 / 3.0) + m.re, m.im};
   }
@@ -231,7 +237,7 @@ __device__ __forceinline__ Cx<R> lp_n(Cx<R> a, R Rb) {
     c = cdiv(Cx<R>{aa.re - R(3) * c.re, aa.im - R(3) * c.im}, cmul(aa, c));
   } else {
     Cx<R> a37 = cscl(aa, R(37));
-    Cx<R> q = cmul(aa, Cx<R>{R(2.0 / 7875.0) - a37.re / R(3031875.0), -a37.im / R(3031875.0)});
+    Cx<R> q = cmul(aa, Cx<R>{R(2.0 / 7875.0) - xdiv(a37.re, R(3031875.0)), xdiv(-a37.im, R(3031875.0))});
     Cx<R> m = cmul(aa, Cx<R>{R(-1.0 / 175.0) + q.re, q.im});
     c = Cx<R>{R(1.0 / 5.0) + m.re, m.im};
   }
@@ -243,23 +249,23 @@ template <typename R>
 __device__ __forceinline__ R omega_n(Cx<R>& alpha, R PG, R Rb, const BubbleParams& b, const BubbleR0& r) {
   const R eps = R(2.22044604925031308e-016);
   const R rho = R(b.rho), sig = R(b.sig), mu = R(b.mu), gam = R(b.gam), ca = R(r.coeff_alpha);
-  R Rx = Rb / R(r.R0);
-  R coef1 = R(r.PG0) / (PG * Rx * Rx * Rx);
+  R Rx = xdiv(Rb, R(r.R0));
+  R coef1 = xdiv(R(r.PG0), PG * Rx * Rx * Rx);
   R coef2 = PG * rho;
-  R coef3 = R(4) / (Rb * Rb);
-  R value1 = R(-2) * sig * rho / Rb;
+  R coef3 = xdiv(R(4), Rb * Rb);
+  R value1 = xdiv(R(-2) * sig * rho, Rb);
   R ups_re = R(3) * gam * coef1;
   R mu_eff = mu;
   R eta = ups_re * coef2 + value1 - mu_eff * mu_eff * coef3;
-  R omega = sqrt(fmax(eta, R(1.0e-6) * eps)) / (rho * Rb);
+  R omega = xdiv(sqrt(fmax(eta, R(1.0e-6) * eps)), rho * Rb);
   for (int k = 0; k < 3; k++) {
-    R s = sqrt(ca / Rb * omega);
+    R s = sqrt(xdiv(ca, Rb) * omega);
     Cx<R> u = cscl(upsilon(Cx<R>{s, s}, gam), coef1);
-    mu_eff = mu + u.im * PG / (R(4) * omega);
+    mu_eff = mu + xdiv(u.im * PG, R(4) * omega);
     eta = u.re * coef2 + value1 - mu_eff * mu_eff * coef3;
-    omega = sqrt(fmax(eta, R(1.0e-6) * eps)) / (rho * Rb);
+    omega = xdiv(sqrt(fmax(eta, R(1.0e-6) * eps)), rho * Rb);
   }
-  R s = sqrt(ca / Rb * omega);
+  R s = sqrt(xdiv(ca, Rb) * omega);
   alpha = Cx<R>{s, s};
   return omega;
 }

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -82,13 +83,32 @@ __device__ __forceinline__ void block_max_to(double v, unsigned long long* out) 
 
 // Velocity update of VelocityKernel (inc/bubble_CUDA_kernel.cuh:658-676) for one
 // face, with the coefficients of the reference.
+// Outside the PML (sigma = 0) and where both densities are rho_inf the same
+// value is computed without its divisions: x / 1.0, v * 1.0 and
+// dt / ((rho + rho) * 0.5) = dt / rho are exact.
 __device__ __forceinline__ double velocity_face(const GridParams& g, double v_old, double p0a, double p0b, double rhoa,
                                                 double rhob, double sigma) {
-  double s1 = (rhoa + rhob) * 0.5;
-  double s2 = (-p0a + p0b) * g.rdx;  // rdx on both faces, as :661 and :671
+  const double s2 = (-p0a + p0b) * g.rdx;  // rdx on both faces, as :661 and :671
+  const double q = (rhoa == g.rho_inf && rhob == g.rho_inf) ? g.dt_rho : g.dt / ((rhoa + rhob) * 0.5);
+  if (sigma == 0.0) return v_old - q * s2;
   double s3 = (g.c_inf + g.c_inf) * 0.5;
   s3 = s3 * 0.5 * g.dt * sigma;
-  return (v_old * (1.0 - s3) - g.dt / s1 * s2) / (1.0 + s3);
+  return (v_old * (1.0 - s3) - q * s2) / (1.0 + s3);
+}
+
+// Split-pressure update of MixturePressureKernel (:856-859) for one component:
+// pn (1 - s2) - s3 (s1 + s5/2) / (1 + s2), with s2 = dt c sigma / 2.
+__device__ __forceinline__ double pressure_component(const GridParams& g, double pn, double sigma, double s1,
+                                                     double h) {
+  if (sigma == 0.0) return pn - g.s3p * (s1 + h);
+  const double s2 = g.s4p * sigma;
+  return pn * (1.0 - s2) - g.s3p * (s1 + h) / (1.0 + s2);
+}
+
+// s5 / 2 of :854: the void-fraction rate term; zero where f_g stays zero.
+__device__ __forceinline__ double void_rate_half(const GridParams& g, double fg, double fgn) {
+  if (fg == 0.0 && fgn == 0.0) return 0.0;
+  return 0.5 * (-(fg - fgn) / g.dt / (1.0 - 0.5 * (fg + fgn)));
 }
 
 // One thread per cell (i, j) of the f_g window [0, X+1] x [0, Y+1].  Interior
@@ -159,15 +179,11 @@ __global__ void __launch_bounds__(kFdtdBX * kFdtdBY) fdtd_step(const __grid_cons
         if (!g.pml_y0) a.vy_new.put(f.idx(i, -1), pre_d);
       }
       // Pressure (MixturePressureKernel :840-864) with the predicted f_g.
-      const double s3p = g.dt * g.rho_inf * g.c_inf * g.c_inf;
-      const double s4p = 0.5 * g.dt * g.c_inf;
       const double s1x = g.cyl ? (-g.xu[i] * vxl + g.xu[i + 1] * vxr) * g.rdx * g.rxp[i] : (-vxl + vxr) * g.rdx;
       const double s1y = (-vyd + vyu) * g.rdy;
-      const double s5 = -(fgp - fgA) / g.dt / (1.0 - 0.5 * (fgp + fgA));
-      const double s2x = s4p * g.mx[i], s2y = s4p * g.my[j];
-      const double h = 0.5 * s5;
-      const double qx = pnx * (1.0 - s2x) - s3p * (s1x + h) / (1.0 + s2x);
-      const double qy = pny * (1.0 - s2y) - s3p * (s1y + h) / (1.0 + s2y);
+      const double h = void_rate_half(g, fgp, fgA);
+      const double qx = pressure_component(g, pnx, g.mx[i], s1x, h);
+      const double qy = pressure_component(g, pny, g.my[j], s1y, h);
       a.px.put(k, qx);
       a.py.put(k, qy);
       double p0new = qx + qy;
@@ -244,7 +260,7 @@ __device__ __forceinline__ int bin_of(const Frame& f, int bx, int by) {
 // plus the cell count for the bin sort.
 template <typename V>
 __global__ void bubble_move(const __grid_constant__ GridParams g, const __grid_constant__ BubbleParams bp,
-                            BubbleArrays b, const V vx, const V vy, int* __restrict__ bin_count) {
+                            BubbleArrays b, const V vx, const V vy, int* __restrict__ moved) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= b.n) return;
   const Frame& f = g.f;
@@ -285,9 +301,19 @@ __global__ void bubble_move(const __grid_constant__ GridParams g, const __grid_c
   iny = (int)floor(y * g.rdy + 0.5);
   b.ibnx[n] = inx;
   b.ibny[n] = iny;
-  int c = bin_of(f, inx, iny);
-  b.bin[n] = c;
-  if (c >= 0) atomicAdd(&bin_count[c], 1);
+  const int c = bin_of(f, inx, iny);
+  if (c != b.bin[n]) {
+    b.bin[n] = c;
+    atomicOr(moved, 1);
+  }
+}
+
+// Bin counts for a rebuild of the cell bins.
+__global__ void bin_count_kernel(const int* __restrict__ bin, int n, int* __restrict__ count) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int c = bin[k];
+  if (c >= 0) atomicAdd(&count[c], 1);
 }
 
 // Cell indices of the initial positions (BubbleUpdateIndexKernel, :345-358) and bin counts.
@@ -301,9 +327,7 @@ __global__ void bubble_index(const __grid_constant__ GridParams g, BubbleArrays 
   int iny = (int)floor(y * g.rdy + 0.5);
   b.ibnx[n] = inx;
   b.ibny[n] = iny;
-  int c = bin_of(g.f, inx, iny);
-  b.bin[n] = c;
-  if (c >= 0) atomicAdd(&bin_count[c], 1);
+  b.bin[n] = bin_of(g.f, inx, iny);
 }
 
 // Exclusive scan of the bin counts: per-block scan, scan of block sums, add.
@@ -623,17 +647,12 @@ __global__ void __launch_bounds__(256) couple_press(const __grid_constant__ Grid
     a.fg.put(k, fgv);
     fgv = a.fg.get(k);  // the stored value (FP32 in the mixed path) is what the step uses
     if (i >= 1 && i <= X && j >= 1 && j <= Y) {
-      const double s3p = g.dt * g.rho_inf * g.c_inf * g.c_inf;
-      const double s4p = 0.5 * g.dt * g.c_inf;
       double vxl = a.vx.get(f.idx(i - 1, j)), vxr = a.vx.get(k);
       double s1x = g.cyl ? (-g.xu[i] * vxl + g.xu[i + 1] * vxr) * g.rdx * g.rxp[i] : (-vxl + vxr) * g.rdx;
       double s1y = (-a.vy.get(f.idx(i, j - 1)) + a.vy.get(k)) * g.rdy;
-      double fgn = a.fgn.get(k);
-      double s5 = -(fgv - fgn) / g.dt / (1.0 - 0.5 * (fgv + fgn));
-      double s2x = s4p * g.mx[i], s2y = s4p * g.my[j];
-      double h = 0.5 * s5;
-      double qx = a.pnx.get(k) * (1.0 - s2x) - s3p * (s1x + h) / (1.0 + s2x);
-      double qy = a.pny.get(k) * (1.0 - s2y) - s3p * (s1y + h) / (1.0 + s2y);
+      const double h = void_rate_half(g, fgv, a.fgn.get(k));
+      double qx = pressure_component(g, a.pnx.get(k), g.mx[i], s1x, h);
+      double qy = pressure_component(g, a.pny.get(k), g.my[j], s1y, h);
       bool forced = g.source_row > 0 && src_pressure(g) && j == g.source_row;
       if (!forced) res = fabs((a.px.get(k) + a.py.get(k)) - (qx + qy));
       a.px.put(k, qx);
@@ -738,13 +757,18 @@ struct Sim {
     long long substep_max;        // largest RP sub-step count of one bubble
     int err;                      // nonzero: a bubble hit the sub-step cap
     int next;                     // work-queue head of the radius solve
+    int moved;                    // nonzero: a bubble changed cell bin this step
   };
   Scalars* d_scalars = nullptr;
   unsigned long long* d_residual = nullptr;
   long long* d_substep_max = nullptr;
   int* d_err = nullptr;
   int* d_next = nullptr;
+  int* d_moved = nullptr;
   Scalars* h_scalars = nullptr;  // pinned
+  double picard_tol = 1.0e-7f;
+  bool bins_stale = false;  // a bubble changed cell since the bins were built
+  bool debug_picard = std::getenv("CRP_DEBUG_PICARD") != nullptr;  // residual of every Picard iteration to stderr
   struct Lpt {
     int* hist;    // kLptBuckets
     int* cursor;  // kLptBuckets
@@ -792,6 +816,7 @@ struct Sim {
       d_substep_max = &d_scalars->substep_max;
       d_err = &d_scalars->err;
       d_next = &d_scalars->next;
+      d_moved = &d_scalars->moved;
     }
     const int n = hs.nb;
     bub.n = n;
@@ -841,6 +866,7 @@ struct Sim {
     if (cfg.ext_precision != CRP_PREC_FP64 && cfg.ext_precision != CRP_PREC_MIXED)
       return fail(CRP_ERR_INVALID, "ext.precision must be fp64 or mixed");
     mixed = cfg.ext_precision == CRP_PREC_MIXED;
+    picard_tol = cfg.ext_picard_tol > 0.0 ? cfg.ext_picard_tol : (mixed ? 1.0e-5 : (double)1.0e-7f);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CRP_ERR_NO_DEVICE, "no CUDA device");
     if (user_stream) {
@@ -934,6 +960,9 @@ struct Sim {
     gp.ctl_x = d.ctl_x;
     gp.ctl_y = d.ctl_y;
     gp.focal_dist = d.focal_dist;
+    gp.dt_rho = d.dt / d.rho_inf;
+    gp.s3p = d.dt * d.rho_inf * d.c_inf * d.c_inf;
+    gp.s4p = 0.5 * d.dt * d.c_inf;
     bp.PL0 = cfg.bub_P0;
     bp.T0 = cfg.bub_T0;
     bp.gam = cfg.bub_gamma;
@@ -964,6 +993,10 @@ struct Sim {
     const int nbins = bins.nbins;
     const int nblk = (nbins + kScanThreads - 1) / kScanThreads;
     cudaError_t e;
+    if ((e = launch(kClassOther, [&] {
+           bin_count_kernel<<<(bub.n + 255) / 256, 256, 0, stream>>>(bub.bin, bub.n, bins.count);
+         })) != cudaSuccess)
+      return e;
     if ((e = launch(kClassOther, [&] {
            bin_scan_blocks<<<nblk, kScanThreads, 0, stream>>>(bins.count, bins.start, bins.partial, nbins);
          })) != cudaSuccess)
@@ -1019,23 +1052,28 @@ struct Sim {
     // Ring rotation of store_variables: the predicted f_g goes to the f_gm buffer.
     const int a = fg_a, b = fg_b, c = fg_c;
     CRP_CUDA(cudaMemsetAsync(d_residual, 0, sizeof(unsigned long long), stream));
+    CRP_CUDA(cudaMemsetAsync(d_moved, 0, sizeof(int), stream));
     CRP_CUDA(mixed ? launch_fdtd<PrecMixed>(nv, np, a, b, c) : launch_fdtd<PrecFP64>(nv, np, a, b, c));
     cur_v = nv;
     cur_p = np;
     fg_a = c;  // predicted f_g
     fg_b = a;  // f_gn
     fg_c = b;  // f_gm
-    if (hs.nb > 0) {
-      CRP_CUDA(mixed ? launch_move<PrecMixed>() : launch_move<PrecFP64>());
-      CRP_CUDA(build_bins());
-      CRP_CUDA(build_order());
-    }
+    if (hs.nb > 0) CRP_CUDA(mixed ? launch_move<PrecMixed>() : launch_move<PrecFP64>());
     crp_status st = read_scalars();
     if (st != CRP_OK) return st;
     double resimax = __longlong_as_double_host(h_scalars->residual) / gp.P_inf;
     int loop = 0;
+    bins_stale = bins_stale || h_scalars->moved != 0;
+    if (hs.nb > 0 && resimax > picard_tol) {
+      // Bins change only when a bubble crosses into another cell; the solve
+      // order follows the latest sub-step counts.
+      if (bins_stale) CRP_CUDA(build_bins());
+      bins_stale = false;
+      CRP_CUDA(build_order());
+    }
     if (hs.nb > 0) {
-      while (resimax > 1.0e-7f) {
+      while (resimax > picard_tol) {
         if (loop >= cfg.ext_picard_cap) return fail(CRP_ERR_PICARD, "Picard iteration cap reached");
         loop++;
         CRP_CUDA(cudaMemsetAsync(d_residual, 0, sizeof(unsigned long long), stream));
@@ -1046,6 +1084,8 @@ struct Sim {
         if (st != CRP_OK) return st;
         if (h_scalars->err) return fail(CRP_ERR_RP_STEPS, "Rayleigh-Plesset sub-step cap reached");
         resimax = __longlong_as_double_host(h_scalars->residual) / gp.P_inf;
+        if (debug_picard && loop <= 40)
+          fprintf(stderr, "step %lld picard %d residual %.6e\n", (long long)stats.steps + 1, loop, resimax);
       }
     }
     if (std::isnan(resimax)) return fail(CRP_ERR_NONFINITE, "non-finite pressure");
@@ -1167,7 +1207,7 @@ struct Sim {
     using V = typename P::V;
     const V vxc = view<V>(vx[cur_v]), vyc = view<V>(vy[cur_v]);
     return launch(kClassOther, [&] {
-      bubble_move<V><<<(bub.n + 255) / 256, 256, 0, stream>>>(gp, bp, bub, vxc, vyc, bins.count);
+      bubble_move<V><<<(bub.n + 255) / 256, 256, 0, stream>>>(gp, bp, bub, vxc, vyc, d_moved);
     });
   }
 

@@ -110,6 +110,8 @@ typedef struct crp_config {
   int32_t ext_cloud_shape;   /* 0 cylinder (r <= cloud_r, |z - focus| <= cloud_h/2), 1 sphere, 2 gaussian */
   double ext_cloud_r, ext_cloud_h;
   double ext_n_b;            /* weight n_B of each seeded bubble, default 1 */
+  double ext_picard_tol;     /* Picard residual threshold, max|dp0|/P_inf; 0 selects the reference's
+                                1e-7 (FP64) or 1e-5 (mixed: FP32 storage has a higher noise floor) */
 } crp_config;
 
 /* Dense host layouts of the readable fields, in the reference's index order:

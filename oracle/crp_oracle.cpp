@@ -847,7 +847,8 @@ struct crpo_sim {
     double resimax = pressure();
     int loop = 0;
     if (bubbles_on) {
-      while (resimax > 1.0e-7f) {
+      const double tol = cfg.ext_picard_tol > 0.0 ? cfg.ext_picard_tol : (double)1.0e-7f;
+      while (resimax > tol) {
         if (loop >= cfg.ext_picard_cap) return CRP_ERR_PICARD;
         loop++;
         interpolate_pressure();

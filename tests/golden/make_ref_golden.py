@@ -49,9 +49,12 @@ RUN_CASES = {
                          tr_amp=0.1),
     # PML on x0 too, plane velocity source, bubbles off
     "plane_v_nobub": dict(steps=150, pml_x0=1, tr_focused_p=0, tr_plane_v=1, bub_enable=0),
-    # tiny grid for the rawdata text comparison
-    "tiny": dict(steps=40, grid_x=12, grid_y=20, grid_lx=1.2e-3, grid_ly=2.0e-3, pml_grid_number=4,
-                 tr_focal_dist=1.6e-3, tr_box_size=0.6e-3, sim_save_interval=40),
+    # small grid for the rawdata text comparison.  38 columns give i1m = 40, where
+    # the pitched widths of p (double2) and p0 (double) coincide; MixturePressureKernel
+    # indexes p0 with p's index (inc/bubble_CUDA_kernel.cuh:862-864), which scrambles
+    # p0 when they differ (with 512-byte pitch alignment, when i1m mod 64 is in [1, 32]).
+    "tiny": dict(steps=60, grid_x=38, grid_y=38, grid_lx=3.8e-3, grid_ly=3.8e-3, pml_grid_number=6,
+                 tr_focal_dist=3.0e-3, tr_box_size=1.0e-3, sim_save_interval=60),
 }
 
 FIELDS = ["p0", "p", "pn", "vx", "vy", "f_g", "f_gn", "f_gm", "rho_m"]
@@ -160,6 +163,11 @@ def run_case(name: str, outdir: str) -> None:
         a = np.zeros(shapes[fname])
         assert r.crp_ref_read_field(fname.encode(), _p(a)) == 0
         out[fname] = a
+    # p0 must equal px + py on interior cells; it does not when the p0 index quirk
+    # above is active for this grid, and the fixture is then not a comparison target.
+    p = out["p"]
+    ok = np.array_equal(out["p0"][1:-1, 1:-1], (p[:, 0::2] + p[:, 1::2])[1:-1, 1:-1])
+    out["p0_consistent"] = np.bool_(ok)
     if cfg.bub_enable:
         for bname in BUBBLE_FIELDS:
             a = np.zeros(2 * nb if bname in ("pos", "ibm", "ibn") else nb)

@@ -29,7 +29,19 @@ _mrg = importlib.util.module_from_spec(_spec)
 _spec.loader.exec_module(_mrg)
 CASES = [c for c in _mrg.RUN_CASES if os.path.exists(os.path.join(GOLD, f"ref_run_{c}.npz"))]
 
+
+def test_fixtures_are_p0_consistent():
+    """Every committed fixture comes from a grid where the reference's p0 indexing
+    quirk (inc/bubble_CUDA_kernel.cuh:862-864) is inactive: p0 = px + py inside."""
+    for c in CASES:
+        g = np.load(os.path.join(GOLD, f"ref_run_{c}.npz"))
+        p = g["p"]
+        assert np.array_equal(g["p0"][1:-1, 1:-1], (p[:, 0::2] + p[:, 1::2])[1:-1, 1:-1]), c
+
 REL_TOL = 1e-9
+# Rates and their integrals (radial velocity, bubble heat) are differences of
+# nearly equal radii over sub-steps; they carry ~100x the relative rounding.
+REL_TOL_RATES = {"bub_d1_R_p": 1e-7, "bub_Q_B": 1e-7}
 
 
 def ref_fields(g):
@@ -65,7 +77,7 @@ def compare(sim, g, tol):
             continue
         errs["bub_" + k] = rel_err(a, ref, FLOOR.get("bub_" + k, 1e-12))
     print({k: f"{v:.1e}" for k, v in errs.items()})
-    bad = {k: v for k, v in errs.items() if not v <= tol}
+    bad = {k: v for k, v in errs.items() if not v <= max(tol, REL_TOL_RATES.get(k, 0.0))}
     assert not bad, bad
 
 
