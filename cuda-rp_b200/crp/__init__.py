@@ -127,6 +127,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "crp_last_error": (ctypes.c_char_p, [vp]),
         "crp_status_string": (ctypes.c_char_p, [c_int]),
         "crp_destroy": (None, [vp]),
+        "crp_void_fraction_noalloc_scratch": (ctypes.c_size_t, [c_int, c_int, c_int]),
+        "crp_void_fraction_noalloc": (c_int, [P(Config), c_int, vp, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -370,6 +370,7 @@ const char* crp_status_string(crp_status s) {
     case CRP_ERR_IO: return "I/O error";
     case CRP_ERR_PARSE: return "configuration parse error";
     case CRP_ERR_NO_DEVICE: return "no CUDA device";
+    case CRP_ERR_TOO_LARGE: return "input larger than the library's fixed scratch buffer";
   }
   return "unknown status";
 }

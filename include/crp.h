@@ -45,7 +45,8 @@ typedef enum crp_status {
   CRP_ERR_NONFINITE = 7,    /* a NaN/Inf was found in the state */
   CRP_ERR_IO = 8,           /* file could not be read or written */
   CRP_ERR_PARSE = 9,        /* configuration file syntax or value error */
-  CRP_ERR_NO_DEVICE = 10    /* no usable CUDA device */
+  CRP_ERR_NO_DEVICE = 10,   /* no usable CUDA device */
+  CRP_ERR_TOO_LARGE = 11    /* input larger than a fixed-size buffer of this library */
 } crp_status;
 
 /* Arithmetic of the grid fields. */
@@ -221,6 +222,34 @@ crp_status crp_set_profiling(crp_sim* sim, int32_t enable);
 
 /* Device stream the simulation runs on (a cudaStream_t). */
 void* crp_stream(crp_sim* sim);
+
+/* Void fraction of a bubble population, computed without allocating anything.
+ *
+ * No counterpart in the reference, which only forms the void fraction inside a
+ * simulation (calculate_void_fraction, src/bubble_CUDA.cu:1198-1218).  It is for
+ * callers that may not allocate device memory when they need the result: loops
+ * where cudaMalloc/cudaFree would synchronise the device, and programs whose
+ * own pool owns the GPU's memory.
+ *
+ * Inputs are device arrays of n bubbles: x, y (m), r (radius, m), n_b (bubbles
+ * per point).  Output f_g is a dense device array of (grid_y + 2) x (grid_x + 2)
+ * doubles, row j at f_g + j * (grid_x + 2), i and j from 0: the same values and
+ * summation order crp_create forms for its initial void fraction from x, y, R0
+ * and n_B (smooth delta of band 2 only; other bands give CRP_ERR_UNSUPPORTED).
+ * Kernels are queued on stream (a cudaStream_t, NULL for the default stream);
+ * the call does not wait for them.
+ *
+ * Scratch space is one static device array of CRP_NOALLOC_SCRATCH_BYTES per
+ * GPU, shared by all calls: calls whose kernels overlap on a GPU race on it and
+ * must be ordered (one stream, or events).  crp_void_fraction_noalloc_scratch
+ * gives the bytes a call needs; a call that needs more returns
+ * CRP_ERR_TOO_LARGE and queues nothing.  The first call on each device looks up
+ * the array's device address (cudaGetSymbolAddress, with that device current):
+ * make it before any stream capture. */
+#define CRP_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+size_t crp_void_fraction_noalloc_scratch(int32_t grid_x, int32_t grid_y, int32_t n);
+crp_status crp_void_fraction_noalloc(const crp_config* cfg, int32_t n, const double* x, const double* y,
+                                     const double* r, const double* n_b, double* f_g, void* stream);
 
 const char* crp_last_error(const crp_sim* sim);
 const char* crp_status_string(crp_status s);
