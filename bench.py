@@ -6,10 +6,15 @@
 One bench step is S mixture time steps (default 100, one save interval of the
 workload) of the full hot path: fused FDTD/PML update, bubble motion and
 binning, and every Picard iteration of Rayleigh-Plesset + void-fraction
-gather + pressure re-evaluation the step needs.  The timed window starts after
-P untimed mixture steps (default: the burst has reached the bubble cloud) plus
-W untimed bench steps, so it measures the driven regime.  The state (about
-200 MB at 1024 x 2048) is larger than L2, so no flush is needed between steps.
+gather + pressure re-evaluation the step needs.  The run starts at t = 0 (or
+after P untimed mixture steps, --preroll), takes W untimed bench steps and
+times K: with the defaults, mixture steps 300-1300 of the workload, which end
+as the burst's leading edge reaches the bubble cloud.  The "driven" object then
+times up to D further chunks of 10 mixture steps of the same run
+(--driven-chunks, --driven-chunk, bounded by --driven-seconds of wall time) in the regime where the burst drives the cloud,
+and records where the run stops if a step fails (the workloads' drive grows the
+bubbles until the mixture model stops converging).  The state (about 200 MB at
+1024 x 2048) is larger than L2, so no flush is needed between steps.
 
 metric: Mcell-upd/s — interior cells x mixture steps / device time (CUDA events
 on the simulation's stream, max over ranks).  Also reported: bubble-steps/s,
@@ -48,14 +53,12 @@ WORKLOADS = {
     "axisym_1024x2048": os.path.join(PKG, "configs", "axisym_1024x2048.conf"),
     "axisym_256x512": os.path.join(PKG, "configs", "axisym_256x512.conf"),
 }
-# Mixture steps before the burst's leading edge reaches the bubble cloud
-# (about (focus depth - cloud half length - source row depth) / c / dt).
-PREROLL = {"axisym_1024x2048": 1300, "axisym_256x512": 700}
-# Compulsory HBM traffic of the fused FDTD pass per cell (DESIGN.md §5): FP64
+# Compulsory HBM traffic of the fused FDTD pass per cell: FP64
 # reads px, py, vx, vy, f_g, f_gn, f_gm and writes px, py, vx, vy, predicted f_g;
 # mixed stores each velocity/pressure value as two FP32 words and f_g as FP32.
 BYTES_PER_CELL = {"fp64": 96, "mixed": 80}
-DTYPE = {"fp64": "f64", "mixed": "f32 fields + f32 compensation (f64 arithmetic), f32 thermal model, f64 RP"}
+DTYPE = {"fp64": "f64", "mixed": "f32 fields + f32 compensation (f64 arithmetic), f32 void fraction, "
+                                  "f32 thermal model while |R/R0-1| <= 1e-3, f64 RP"}
 
 
 def parse():
@@ -66,7 +69,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="axisym_1024x2048", choices=list(WORKLOADS))
     ap.add_argument("--chunk", type=int, default=100)
-    ap.add_argument("--preroll", type=int, default=None)
+    ap.add_argument("--preroll", type=int, default=0)
+    ap.add_argument("--driven-chunks", type=int, default=10)
+    ap.add_argument("--driven-chunk", type=int, default=10)
+    ap.add_argument("--driven-seconds", type=float, default=60.0)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -133,6 +139,19 @@ def peaks():
         d = json.load(open(p))
         return d["hbm_gbs"], "measured"
     return 6650.0, "fallback"
+
+
+def traffic(workload, precision):
+    """DRAM bytes (read + write) of one fdtd_strip launch from the committed ncu
+    summary of this workload and precision, or None when there is none."""
+    p = os.path.join(ROOT, "profiles", f"fdtd_strip_{workload}_{precision}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("| traffic per launch (read + write) |"):
+            mb = float(line.split("|")[2].split()[0])
+            return int(mb * 1e6)
+    return None
 
 
 def load_workload(name):
@@ -239,6 +258,46 @@ def timed_run(cfg, bub, args, preroll, dist, dev):
     return ms, s0, sim.stats(), sim, clk.summary()
 
 
+def driven_sample(sim, args, cells, nb):
+    """Further chunks of the primary run, timed one by one with CUDA events,
+    until args.driven_chunks are done, the wall budget is spent or a step fails."""
+    import torch
+
+    import crp
+
+    stream = torch.cuda.ExternalStream(sim.stream)
+    out = {"start_step": int(sim.stats().steps), "chunks": [], "stopped": None}
+    t_wall = time.perf_counter()
+    ms_tot, steps_tot = 0.0, 0
+    for _ in range(args.driven_chunks):
+        if time.perf_counter() - t_wall > args.driven_seconds:
+            out["stopped"] = "wall budget"
+            break
+        s0 = sim.stats()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        try:
+            sim.step(args.driven_chunk)
+        except crp.CrpError as e:
+            torch.cuda.synchronize()
+            out["stopped"] = f"step {sim.stats().steps + 1}: {e}"
+            break
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        s1 = sim.stats()
+        ms_tot += ms
+        steps_tot += args.driven_chunk
+        out["chunks"].append({"ms": ms, "picard_per_step": (s1.picard_total - s0.picard_total) / args.driven_chunk,
+                              "rp_substeps_max": int(s1.rp_substeps_max),
+                              "R_max_over_R0": float(np.max(sim.bubbles("R_t") / sim.bubbles("R0")))})
+    if steps_tot:
+        out["value"] = cells * steps_tot / (ms_tot * 1e-3) / 1e6
+        out["unit"] = "Mcell-upd/s"
+        out["bubble_steps_per_s"] = nb * steps_tot / (ms_tot * 1e-3)
+    return out
+
+
 def focal_mask(sim, cfg, radius=2e-3):
     d = sim.dims
     fy = cfg.tr_focal_dist * 0.5 * np.sqrt(3.0)
@@ -260,7 +319,7 @@ def run_ours(args, rank, world, dist):
     torch.cuda.set_device(dev)
     cfg, bub = load_workload(args.workload)
     cells = cfg.grid_x * cfg.grid_y
-    preroll = PREROLL[args.workload] if args.preroll is None else args.preroll
+    preroll = args.preroll
     S = args.chunk
     mix_steps = args.steps * S
 
@@ -292,6 +351,7 @@ def run_ours(args, rank, world, dist):
     n_fdtd = p1s.fdtd_launches - p0s.fdtd_launches
     fdtd_ms = (p1s.ms_fdtd - p0s.ms_fdtd) / max(n_fdtd, 1)
     prof = {k: (getattr(p1s, k) - getattr(p0s, k)) for k in ("ms_fdtd", "ms_rp", "ms_couple", "ms_other")}
+    driven = driven_sample(sim, args, cells, nb) if rank == 0 and args.driven_chunks > 0 and world == 1 else None
     hbm, kind = peaks()
     bpc = BYTES_PER_CELL[primary]
     achieved = bpc * cells / (fdtd_ms * 1e-3) / 1e9
@@ -307,12 +367,15 @@ def run_ours(args, rank, world, dist):
             "bubble_steps_per_s": nb * mix_steps * world / (ms * 1e-3),
             "picard_iterations_per_step": picard / mix_steps,
             "gpu_launches": int(launches),
-            "roofline": {"kernel": "fdtd_step", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "peak_kind": kind, "traffic": None, "bytes_per_cell": bpc,
+            "roofline": {"kernel": "fdtd_strip", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_kind": kind, "traffic": traffic(args.workload, primary),
+                         "bytes_per_cell": bpc,
                          "ms_per_launch": fdtd_ms},
             "kernel_ms_per_chunk": prof,
             "clocks": run["clocks"],
         }
+        if driven is not None:
+            result["driven"] = driven
         for prec, r in runs.items():
             result[f"{prec}_path"] = {"value": cells * mix_steps * world / (r["ms"] * 1e-3) / 1e6,
                                       "ms_per_step": r["ms"] / args.steps,

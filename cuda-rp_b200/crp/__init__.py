@@ -59,7 +59,8 @@ class Stats(ctypes.Structure):
                 ("picard_last", c_int), ("picard_max", c_int), ("rp_substeps_max", ctypes.c_int64),
                 ("residual_last", c_dbl), ("kernel_launches", ctypes.c_int64), ("fdtd_launches", ctypes.c_int64),
                 ("rp_launches", ctypes.c_int64), ("couple_launches", ctypes.c_int64),
-                ("ms_fdtd", c_dbl), ("ms_rp", c_dbl), ("ms_couple", c_dbl), ("ms_other", c_dbl)]
+                ("ms_fdtd", c_dbl), ("ms_rp", c_dbl), ("ms_couple", c_dbl), ("ms_other", c_dbl),
+                ("picard_stalls", ctypes.c_int64)]
 
 
 class BubblesIn(ctypes.Structure):

@@ -12,6 +12,8 @@
 // exactly the value MixturePropertiesKernel stores
 // (inc/bubble_CUDA_kernel.cuh:1122), so neither p0 nor rho_m occupies HBM.
 #pragma once
+#include <cuda_pipeline.h>
+
 #include <cstdint>
 
 namespace crp {
@@ -106,6 +108,12 @@ struct F64 {
   double* p;
   __device__ __forceinline__ double get(long k) const { return p[k]; }
   __device__ __forceinline__ void put(long k, double v) const { p[k] = v; }
+  // The value get() returns after put(v).
+  __device__ static __forceinline__ double stored(double v) { return v; }
+  // Asynchronous copy of element k into an 8-byte shared-memory slot, and the
+  // value of a slot once the copy has landed.
+  __device__ __forceinline__ void stage(void* dst, long k) const { __pipeline_memcpy_async(dst, p + k, 8); }
+  __device__ static __forceinline__ double staged(const void* src) { return *(const double*)src; }
 };
 struct F32c {
   float* hi;
@@ -116,12 +124,27 @@ struct F32c {
     hi[k] = h;
     lo[k] = (float)(v - (double)h);
   }
+  __device__ static __forceinline__ double stored(double v) {
+    const float h = (float)v;
+    return (double)h + (double)(float)(v - (double)h);
+  }
+  __device__ __forceinline__ void stage(void* dst, long k) const {
+    __pipeline_memcpy_async(dst, hi + k, 4);
+    __pipeline_memcpy_async((char*)dst + 4, lo + k, 4);
+  }
+  __device__ static __forceinline__ double staged(const void* src) {
+    const float* v = (const float*)src;
+    return (double)v[0] + (double)v[1];
+  }
 };
 // Void-fraction history of the mixed path: FP32 storage (sums are FP64).
 struct F32 {
   float* p;
   __device__ __forceinline__ double get(long k) const { return (double)p[k]; }
   __device__ __forceinline__ void put(long k, double v) const { p[k] = (float)v; }
+  __device__ static __forceinline__ double stored(double v) { return (double)(float)v; }
+  __device__ __forceinline__ void stage(void* dst, long k) const { __pipeline_memcpy_async(dst, p + k, 4); }
+  __device__ static __forceinline__ double staged(const void* src) { return (double)*(const float*)src; }
 };
 
 // Mixture pressure p0 at logical (i, j), i in [0, X+1], j in [0, Y+1], from the

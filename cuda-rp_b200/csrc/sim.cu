@@ -1,19 +1,23 @@
 // B200 implementation of CUDA-RP's simulation path behind the crp C ABI.
 //
 // One mixture time step (the main loop of solve_bubbles, src/bubble_CUDA.cu:206-285):
-//   fdtd_step      fused: void-fraction prediction (VFPredictionKernel), velocity
-//                  update with its boundary overrides (VelocityKernel,
-//                  VelocityBoundaryKernel), first pressure evaluation
-//                  (MixturePressureKernel) and its residual, one HBM pass
+//   fdtd_strip     fused: void-fraction prediction, velocity update with its
+//                  boundary overrides (VelocityKernel, VelocityBoundaryKernel),
+//                  first pressure evaluation (MixturePressureKernel) and its
+//                  residual, one HBM pass in column strips
 //   vghost         velocity ghost cells (the rest of VelocityBoundaryKernel)
 //   bubble_move    bubble state rotation (store_variables), velocity gather,
-//                  motion, cell indices, bin counts
-//   bin_scan/fill/sort  counting sort of bubbles by cell (deterministic order)
+//                  motion, cell indices, occupied-bin box
+//   bin_*          counting sort of bubbles by cell (deterministic order), only
+//                  when a bubble changed cell
+//   lpt_*          radius-solve order, heaviest sub-step counts first
 //   Picard loop while max|dp0|/P_inf > 1e-7 (src/bubble_CUDA.cu:243):
 //     bubble_rp    pressure gather + Rayleigh-Plesset sub-stepping + the void
-//                  fraction contribution of each bubble to its four cells
+//                  fraction contribution of each bubble to its four cells,
+//                  persistent with a work queue
 //     couple_press gather of the void fraction per cell (no atomics), axis fold,
-//                  pressure re-evaluation and residual
+//                  pressure re-evaluation and residual, over the cells whose
+//                  void fraction can be nonzero
 // Buffers rotate instead of being copied: velocity and pressure ping-pong, the
 // void-fraction history is a three-buffer ring.
 #include <cuda_runtime.h>
@@ -34,9 +38,6 @@
 namespace crp {
 
 // ---------------------------------------------------------------------------
-// Kernels, FP64 fields.
-
-
 // Storage of each field class and the real type of the bubble thermal model.
 struct PrecFP64 {
   using V = F64;  // velocity
@@ -111,91 +112,241 @@ __device__ __forceinline__ double void_rate_half(const GridParams& g, double fg,
   return 0.5 * (-(fg - fgn) / g.dt / (1.0 - 0.5 * (fg + fgn)));
 }
 
-// One thread per cell (i, j) of the f_g window [0, X+1] x [0, Y+1].  Interior
-// threads compute the four velocity faces around their cell (the west and
-// south faces duplicate a neighbour's east/north face; those values are
-// identical, and only the owner writes them), then the pressure of the cell.
-// Neighbour loads hit L1/L2, so HBM sees each array about once per step.
-constexpr int kFdtdBX = 32, kFdtdBY = 8;
+// The rarely taken parts of the strip update live in out-of-line functions so
+// that their transcendental code does not raise the register count of the
+// update loop.
+//
+// North face jf on the y0 face or the [ext] source row (VelocityBoundaryKernel
+// :734-798): v is the face from the update; pre receives the face before the
+// y0 source overwrites it (the value the reference mirrors into row -1).
+__device__ __noinline__ double vy_face_special(const GridParams& g, int jf, double v, double xm, double t_cur,
+                                               double* pre) {
+  if (jf == 0 && !g.pml_y0) {
+    if (!src_pressure(g)) v = 0.0;
+    *pre = v;
+    double s;
+    if (g.source_row == 0 && source_value(g, false, xm, 0.0, t_cur, s)) v = s;
+  }
+  if (g.source_row > 0 && jf == g.source_row) {
+    double s;
+    if (source_value(g, false, xm, (double)g.source_row * g.dy, t_cur, s)) v = s;
+  }
+  return v;
+}
+
+// North face jf of a column (VelocityKernel :668-676 with the y sections of
+// VelocityBoundaryKernel): y0 wall or source, [ext] source row, y1 wall.
+__device__ __forceinline__ double vy_face_value(const GridParams& g, int jf, double v_old, double p0a, double p0b,
+                                                double ra, double rb, double xm, double t_cur, double& pre) {
+  double v = velocity_face(g, v_old, p0a, p0b, ra, rb, g.ny[jf + 1]);
+  pre = v;
+  if ((jf == 0 && !g.pml_y0) || (g.source_row > 0 && jf == g.source_row)) v = vy_face_special(g, jf, v, xm, t_cur, &pre);
+  if (jf == g.f.Y && !g.pml_y1) v = 0.0;
+  return v;
+}
+
+template <typename S>
+__device__ __noinline__ double p0_edge(const GridParams& g, const S px, const S py, int i, int j, double t) {
+  return p0_at(g, px, py, i, j, t);
+}
+
+// Pressure source value on the [ext] source row.
+__device__ __noinline__ double source_row_pressure(const GridParams& g, double xm, double t) {
+  double sv = 0.0;
+  source_value(g, true, xm, ((double)g.source_row - 0.5) * g.dy, t, sv);
+  return sv;
+}
+
+// One mixture step of the grid, fused: void-fraction prediction (store_variables,
+// src/bubble_CUDA.cu:1160-1162), VelocityKernel with VelocityBoundaryKernel's
+// faces (inc/bubble_CUDA_kernel.cuh:658-798), MixturePressureKernel with the
+// predicted void fraction (:816-867) and the residual of calculate_pressure_field.
+// The work is organised as column strips.  A warp holds the
+// 32 adjacent columns i = 30 s + lane of strip s and marches up a chunk of
+// rows: lanes 1..30 update their cells, lanes 0 and 31 only provide the values
+// across the strip's edges.  Left/right neighbour values arrive by warp
+// shuffle, the row below stays in registers, so every array element is read
+// once per step (the two edge columns of a strip and the row under a chunk
+// once more, from L2), with 256-byte coalesced rows per warp load.  Rows are
+// staged through a per-warp ring in shared memory by asynchronous copies
+// issued kStripStages - 2 rows ahead, so each warp keeps several rows of all
+// seven input arrays in flight instead of one dependent round trip per row.
+constexpr int kStripCells = 30;
+constexpr int kStripWarps = 4;
+constexpr int kStripRows = 8;    // rows per chunk; the grid is a few waves of 148 SMs at 1024 x 2048
+constexpr int kStripStages = 6;  // ring slots (rows) per warp
+constexpr int kStripFields = 7;  // pnx, pny, fgA, vx_old, vy_old, fgB, fgC
 
 template <typename P>
-__global__ void __launch_bounds__(kFdtdBX * kFdtdBY) fdtd_step(const __grid_constant__ GridParams g,
-                                                               const FdtdArgs<P> a) {
+__global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_constant__ GridParams g,
+                                                               const FdtdArgs<P> a, int rows) {
+  using G = typename P::G;
+  using S = typename P::S;
+  using V = typename P::V;
+  __shared__ __align__(16) double ring[kStripWarps][kStripStages][kStripFields][32];
   const Frame& f = g.f;
   const int X = f.X, Y = f.Y;
-  const int i = blockIdx.x * kFdtdBX + threadIdx.x;
-  const int j = blockIdx.y * kFdtdBY + threadIdx.y;
-  double res = 0.0;
-  if (i <= X + 1 && j <= Y + 1) {
-    const long k = f.idx(i, j);
-    const double fgA = a.fgA.get(k);
-    // Predicted f_g, rounded to its storage precision before use.
-    a.fgC.put(k, 3.0 * fgA - 3.0 * a.fgB.get(k) + a.fgC.get(k));
-    const double fgp = a.fgC.get(k);
-    if (i >= 1 && i <= X && j >= 1 && j <= Y) {
-      const double xm = ((double)i - 0.5) * g.dx;
-      auto rho_at = [&](long kk) -> double { return a.rho_const ? g.rho_inf : (1.0 - a.fgA.get(kk)) * g.rho_inf; };
-      // p0 of the previous step (interior: px + py; boundary values by p0_at).
-      const double pnx = a.pnx.get(k), pny = a.pny.get(k);
-      const bool forced_here = g.source_row > 0 && j == g.source_row && src_pressure(g);
-      const double p0c = forced_here ? p0_at(g, a.pnx, a.pny, i, j, a.t_prev) : pnx + pny;
-      const double p0l = p0_at(g, a.pnx, a.pny, i - 1, j, a.t_prev);
-      const double p0r = p0_at(g, a.pnx, a.pny, i + 1, j, a.t_prev);
-      const double p0d = p0_at(g, a.pnx, a.pny, i, j - 1, a.t_prev);
-      const double p0u = p0_at(g, a.pnx, a.pny, i, j + 1, a.t_prev);
-      const double rc = a.rho_const ? g.rho_inf : (1.0 - fgA) * g.rho_inf;
-      const double rl = rho_at(f.idx(i - 1, j)), rr = rho_at(f.idx(i + 1, j));
-      const double rd = rho_at(f.idx(i, j - 1)), ru = rho_at(f.idx(i, j + 1));
-      // x faces (VelocityKernel :658-666, VelocityBoundaryKernel :704-720).
-      double vxl = velocity_face(g, a.vx_old.get(f.idx(i - 1, j)), p0l, p0c, rl, rc, g.nx[i]);
-      if (i - 1 == 0 && !g.pml_x0) vxl = 0.0;
-      double vxr = velocity_face(g, a.vx_old.get(k), p0c, p0r, rc, rr, g.nx[i + 1]);
-      if (i == X && !g.pml_x1) vxr = 0.0;
-      // y faces (:668-676, :734-798): y0 wall/source, [ext] source row, y1 wall.
-      auto vy_face = [&](int jf, double v_old, double p0a, double p0b, double ra, double rb, double& pre) -> double {
-        double v = velocity_face(g, v_old, p0a, p0b, ra, rb, g.ny[jf + 1]);
-        pre = v;
-        if (jf == 0 && !g.pml_y0) {
-          if (!src_pressure(g)) v = 0.0;
-          pre = v;
-          double s;
-          if (g.source_row == 0 && source_value(g, false, xm, 0.0, a.t_cur, s)) v = s;
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x;
+  const int i = (blockIdx.x * kStripWarps + threadIdx.y) * kStripCells + lane;
+  const bool inwin = i <= X + 1;                                 // column inside the window [0, X+1]
+  const bool cell = lane >= 1 && lane <= kStripCells && i <= X;  // updates cell (i, j)
+  const bool face = lane <= kStripCells && i <= X;               // east face F(i) needed
+  // Owner of the f_g prediction of this column.
+  const bool own = inwin && ((lane >= 1 && lane <= kStripCells) || (lane == 0 && i == 0) ||
+                             (lane == 31 && i == X + 1));
+  const int j0 = 1 + blockIdx.y * rows;
+  const int j1 = min(Y, j0 + rows - 1);
+  const double xm = ((double)i - 0.5) * g.dx;
+  const bool inner_col = i >= 1 && i <= X;
+  const bool src_rows = g.source_row > 0 && src_pressure(g);
+  auto p0_of = [&](int r, double px_, double py_) -> double {
+    if (!inwin) return 0.0;
+    if (inner_col && r >= 1 && r <= Y && !(src_rows && r == g.source_row)) return px_ + py_;
+    return p0_edge(g, a.pnx, a.pny, i, r, a.t_prev);
+  };
+  auto rho_of = [&](double fa) -> double { return a.rho_const ? g.rho_inf : (1.0 - fa) * g.rho_inf; };
+  auto predict = [&](long k, double fa) -> double {
+    const double v = G::stored(3.0 * fa - 3.0 * a.fgB.get(k) + a.fgC.get(k));
+    a.fgC.put(k, v);
+    return v;
+  };
+  // Ring slot of field fld of row r (each lane only touches its own column).
+  auto slot = [&](int r, int fld) -> double* { return &ring[threadIdx.y][r % kStripStages][fld][lane]; };
+  // Queue the copies of row r: pnx, pny, fgA for rows j0-1..j1+1, vy_old for
+  // j0-1..j1, vx_old, fgB, fgC for j0..j1.  One commit group per row, empty
+  // past the chunk, so that a fixed wait count always means "row j+1 landed".
+  auto issue = [&](int r) {
+    if (inwin && r <= j1 + 1) {
+      const long k = f.idx(i, r);
+      a.pnx.stage(slot(r, 0), k);
+      a.pny.stage(slot(r, 1), k);
+      a.fgA.stage(slot(r, 2), k);
+      if (r <= j1) {
+        a.vy_old.stage(slot(r, 4), k);
+        if (r >= j0) {
+          a.vx_old.stage(slot(r, 3), k);
+          if (own) {
+            a.fgB.stage(slot(r, 5), k);
+            a.fgC.stage(slot(r, 6), k);
+          }
         }
-        if (g.source_row > 0 && jf == g.source_row) {
-          double s;
-          if (source_value(g, false, xm, (double)g.source_row * g.dy, a.t_cur, s)) v = s;
-        }
-        if (jf == Y && !g.pml_y1) v = 0.0;
-        return v;
-      };
-      double pre_d, pre_u;
-      const double vyd = vy_face(j - 1, a.vy_old.get(f.idx(i, j - 1)), p0d, p0c, rd, rc, pre_d);
-      const double vyu = vy_face(j, a.vy_old.get(k), p0c, p0u, rc, ru, pre_u);
-      a.vx_new.put(k, vxr);
-      a.vy_new.put(k, vyu);
-      if (i == 1) a.vx_new.put(f.idx(0, j), vxl);
-      if (j == 1) {
-        a.vy_new.put(f.idx(i, 0), vyd);
-        if (!g.pml_y0) a.vy_new.put(f.idx(i, -1), pre_d);
       }
-      // Pressure (MixturePressureKernel :840-864) with the predicted f_g.
-      const double s1x = g.cyl ? (-g.xu[i] * vxl + g.xu[i + 1] * vxr) * g.rdx * g.rxp[i] : (-vxl + vxr) * g.rdx;
-      const double s1y = (-vyd + vyu) * g.rdy;
-      const double h = void_rate_half(g, fgp, fgA);
-      const double qx = pressure_component(g, pnx, g.mx[i], s1x, h);
-      const double qy = pressure_component(g, pny, g.my[j], s1y, h);
+    }
+    __pipeline_commit();
+  };
+  for (int r = j0 - 1; r < j0 - 1 + kStripStages; r++) issue(r);
+  __pipeline_wait_prior(kStripStages - 2);  // rows j0-1 and j0 have landed
+
+  // Row below the chunk and the chunk's first row.
+  double pxc = 0.0, pyc = 0.0, fac = 0.0, p0b = 0.0, rhob = 0.0, vyob = 0.0;
+  if (inwin) {
+    const double pxb = S::staged(slot(j0 - 1, 0)), pyb = S::staged(slot(j0 - 1, 1));
+    const double fab = G::staged(slot(j0 - 1, 2));
+    vyob = V::staged(slot(j0 - 1, 4));
+    pxc = S::staged(slot(j0, 0));
+    pyc = S::staged(slot(j0, 1));
+    fac = G::staged(slot(j0, 2));
+    p0b = p0_of(j0 - 1, pxb, pyb);
+    rhob = rho_of(fab);
+    if (j0 == 1 && own) predict(f.idx(i, 0), fab);
+  }
+  issue(j0 - 1 + kStripStages);  // reuses the slot of row j0-1
+  double p0c = p0_of(j0, pxc, pyc), rhoc = rho_of(fac);
+  double vyd = 0.0;
+  if (cell) {
+    double pre_d;
+    vyd = vy_face_value(g, j0 - 1, vyob, p0b, p0c, rhob, rhoc, xm, a.t_cur, pre_d);
+    if (j0 == 1) {
+      a.vy_new.put(f.idx(i, 0), vyd);
+      if (!g.pml_y0) a.vy_new.put(f.idx(i, -1), pre_d);
+    }
+  }
+
+  // Per-column coefficients: PML profiles of the east face and the cell, and
+  // the cylindrical metrics.
+  const double nx_e = face ? g.nx[i + 1] : 0.0;
+  const double mx_c = cell ? g.mx[i] : 0.0;
+  const double xu_w = cell && g.cyl ? g.xu[i] : 0.0, xu_e = cell && g.cyl ? g.xu[i + 1] : 0.0;
+  const double rxp_c = cell && g.cyl ? g.rxp[i] : 0.0;
+  const bool zero_e = (i == 0 && !g.pml_x0) || (i == X && !g.pml_x1);
+
+  unsigned long long res = 0ull;  // max |dp0| as a bit pattern (NaN sorts above every number)
+#pragma unroll 1
+  for (int j = j0; j <= j1; j++) {
+    const long k = f.idx(i, j);
+    __pipeline_wait_prior(kStripStages - 2);  // row j+1 has landed
+    double pxn = 0.0, pyn = 0.0, fan = 0.0, vxo = 0.0, vyo = 0.0, fgp = 0.0;
+    if (inwin) {
+      pxn = S::staged(slot(j + 1, 0));
+      pyn = S::staged(slot(j + 1, 1));
+      fan = G::staged(slot(j + 1, 2));
+      vxo = V::staged(slot(j, 3));
+      vyo = V::staged(slot(j, 4));
+    }
+    if (own) {
+      fgp = G::stored(3.0 * fac - 3.0 * G::staged(slot(j, 5)) + G::staged(slot(j, 6)));
+      a.fgC.put(k, fgp);
+    }
+    const double p0n = p0_of(j + 1, pxn, pyn), rhon = rho_of(fan);
+    const double p0r = __shfl_down_sync(full, p0c, 1), rhor = __shfl_down_sync(full, rhoc, 1);
+    const double my_j = g.my[j], ny_n = g.ny[j + 1];
+    // Cells with no PML, no void fraction and rho_m = rho_inf around them, away
+    // from the source row, take the division-free forms of the updates (the
+    // values are the same: the skipped factors are exactly 1 and 0).  The
+    // choice is made for the whole warp so that the general forms do not run
+    // predicated on every lane.
+    const bool plain_e = !face || (nx_e == 0.0 && rhoc == g.rho_inf && rhor == g.rho_inf);
+    const bool plain_c = !cell || (ny_n == 0.0 && rhon == g.rho_inf && mx_c == 0.0 && my_j == 0.0 && fgp == 0.0 &&
+                                   fac == 0.0 && !(g.source_row > 0 && j == g.source_row));
+    double fe = 0.0, vyu = 0.0, qx = 0.0, qy = 0.0;
+    if (__all_sync(full, plain_e && plain_c)) {
+      if (face) fe = zero_e ? 0.0 : vxo - g.dt_rho * ((-p0c + p0r) * g.rdx);
+      const double fw = __shfl_up_sync(full, fe, 1);
+      if (cell) {
+        vyu = (j == Y && !g.pml_y1) ? 0.0 : vyo - g.dt_rho * ((-p0c + p0n) * g.rdx);
+        const double s1x = g.cyl ? (-xu_w * fw + xu_e * fe) * g.rdx * rxp_c : (-fw + fe) * g.rdx;
+        const double s1y = (-vyd + vyu) * g.rdy;
+        qx = pxc - g.s3p * (s1x + 0.0);
+        qy = pyc - g.s3p * (s1y + 0.0);
+      }
+    } else {
+      if (face) {
+        fe = velocity_face(g, vxo, p0c, p0r, rhoc, rhor, nx_e);
+        if (zero_e) fe = 0.0;
+      }
+      const double fw = __shfl_up_sync(full, fe, 1);
+      if (cell) {
+        double pre_u;
+        vyu = vy_face_value(g, j, vyo, p0c, p0n, rhoc, rhon, xm, a.t_cur, pre_u);
+        const double s1x = g.cyl ? (-xu_w * fw + xu_e * fe) * g.rdx * rxp_c : (-fw + fe) * g.rdx;
+        const double s1y = (-vyd + vyu) * g.rdy;
+        const double h = void_rate_half(g, fgp, fac);
+        qx = pressure_component(g, pxc, mx_c, s1x, h);
+        qy = pressure_component(g, pyc, my_j, s1y, h);
+      }
+    }
+    if (cell) {
+      a.vx_new.put(k, fe);
+      a.vy_new.put(k, vyu);
       a.px.put(k, qx);
       a.py.put(k, qy);
       double p0new = qx + qy;
-      if (forced_here) {
-        double s;
-        source_value(g, true, xm, ((double)g.source_row - 0.5) * g.dy, a.t_cur, s);
-        p0new = s;
-      }
-      res = fabs(p0c - p0new);
+      if (src_rows && j == g.source_row) p0new = source_row_pressure(g, xm, a.t_cur);
+      res = max(res, (unsigned long long)__double_as_longlong(fabs(p0c - p0new)));
+      vyd = vyu;
+    } else if (lane == 0 && i == 0) {
+      a.vx_new.put(k, fe);  // the x0 face, vx(0, j)
     }
+    pxc = pxn;
+    pyc = pyn;
+    fac = fan;
+    p0c = p0n;
+    rhoc = rhon;
+    issue(j + kStripStages);  // reuses the slot of row j
   }
-  block_max_to(res, a.residual);
+  if (j1 == Y && own) predict(f.idx(i, Y + 1), fac);
+  block_max_to(__longlong_as_double((long long)res), a.residual);
 }
 
 // Velocity ghost cells (VelocityBoundaryKernel, inc/bubble_CUDA_kernel.cuh:701-811,
@@ -258,11 +409,13 @@ __device__ __forceinline__ int bin_of(const Frame& f, int bx, int by) {
 // store_variables' bubble rotation (inc/bubble_CUDA_kernel.cuh:1241-1248),
 // BubbleInterpolationVelocityKernel (:398-448) and BubbleMotionKernel (:451-468),
 // plus the cell count for the bin sort.
+constexpr int kBoxOff = 4;
+
+constexpr int kMoveThreads = 256;
+
 template <typename V>
-__global__ void bubble_move(const __grid_constant__ GridParams g, const __grid_constant__ BubbleParams bp,
-                            BubbleArrays b, const V vx, const V vy, int* __restrict__ moved) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= b.n) return;
+__device__ __forceinline__ void move_one(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
+                                         const V& vx, const V& vy, int* __restrict__ moved, int n, int* s_box) {
   const Frame& f = g.f;
   b.R_pn[n] = b.R_p[n];
   b.R_nn[n] = b.R_n[n];
@@ -275,18 +428,20 @@ __global__ void bubble_move(const __grid_constant__ GridParams g, const __grid_c
   double x = b.x[n], y = b.y[n];
   int imx = b.ibmx[n], imy = b.ibmy[n], inx = b.ibnx[n], iny = b.ibny[n];
   double vlx = 0.0, vly = 0.0;
+  // Delta weights of the two rows/columns of each stencil (the same values the
+  // reference recomputes inside its loops).
+  const double dyn[2] = {delta_y(bp, g, iny, y), delta_y(bp, g, iny + 1, y)};
+  const double dym[2] = {delta_y(bp, g, imy - 1, y), delta_y(bp, g, imy, y)};
   for (int i = imx - 1; i <= imx; i++) {
     double dxw = delta_x(bp, g, i, x);
     for (int j = iny; j <= iny + 1; j++) {
-      double dyw = delta_y(bp, g, j, y);
-      if (i >= -1 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) vlx += vx.get(f.idx(i, j)) * dxw * dyw;
+      if (i >= -1 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) vlx += vx.get(f.idx(i, j)) * dxw * dyn[j - iny];
     }
   }
   for (int i = inx; i <= inx + 1; i++) {
     double dxw = delta_x(bp, g, i, x);
     for (int j = imy - 1; j <= imy; j++) {
-      double dyw = delta_y(bp, g, j, y);
-      if (i >= 0 && i <= f.X + 1 && j >= -1 && j <= f.Y + 1) vly += vy.get(f.idx(i, j)) * dxw * dyw;
+      if (i >= 0 && i <= f.X + 1 && j >= -1 && j <= f.Y + 1) vly += vy.get(f.idx(i, j)) * dxw * dym[j - imy + 1];
     }
   }
   b.vbx[n] = vlx;
@@ -302,10 +457,39 @@ __global__ void bubble_move(const __grid_constant__ GridParams g, const __grid_c
   b.ibnx[n] = inx;
   b.ibny[n] = iny;
   const int c = bin_of(f, inx, iny);
+  {
+    // Bounding box of the occupied bins, encoded so that every value is
+    // positive and zero means "no bubble": moved[1..4] receive the maxima of
+    // kBoxOff - bx, kBoxOff + bx, kBoxOff - by, kBoxOff + by (warp, then
+    // block, then one atomic per block).
+    const bool in = c >= 0;
+    const unsigned m = __activemask();
+    const int e0 = __reduce_max_sync(m, in ? kBoxOff - inx : 0), e1 = __reduce_max_sync(m, in ? kBoxOff + inx : 0);
+    const int e2 = __reduce_max_sync(m, in ? kBoxOff - iny : 0), e3 = __reduce_max_sync(m, in ? kBoxOff + iny : 0);
+    if ((threadIdx.x & 31) == __ffs(m) - 1 && e1 > 0) {
+      atomicMax(s_box + 0, e0);
+      atomicMax(s_box + 1, e1);
+      atomicMax(s_box + 2, e2);
+      atomicMax(s_box + 3, e3);
+    }
+  }
   if (c != b.bin[n]) {
     b.bin[n] = c;
     atomicOr(moved, 1);
   }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kMoveThreads) bubble_move(const __grid_constant__ GridParams g,
+                                                            const __grid_constant__ BubbleParams bp, BubbleArrays b,
+                                                            const V vx, const V vy, int* __restrict__ moved) {
+  __shared__ int s_box[4];
+  if (threadIdx.x < 4) s_box[threadIdx.x] = 0;
+  __syncthreads();
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < b.n) move_one(g, bp, b, vx, vy, moved, n, s_box);
+  __syncthreads();
+  if (threadIdx.x < 4 && s_box[threadIdx.x] > 0) atomicMax(moved + 1 + threadIdx.x, s_box[threadIdx.x]);
 }
 
 // Bin counts for a rebuild of the cell bins.
@@ -466,15 +650,31 @@ __device__ __forceinline__ void rp_begin(const GridParams& g, const BubbleParams
 // One pass of the sub-step loop of BubbleRadiusKernel (:506-539).  T is the
 // real type of the thermal model (omega_N, alpha_N, Lp_N); everything else is FP64.
 template <typename T>
+__device__ __forceinline__ void thermal_model(const BubbleParams& bp, const RpState& s, double PGn, double& omega,
+                                              C64& lp) {
+  Cx<T> alpha_t;
+  omega = (double)omega_n<T>(alpha_t, (T)PGn, (T)s.Rn, bp, s.r);
+  const Cx<T> lp_t = lp_n<T>(alpha_t, (T)s.Rn);
+  lp = C64{(double)lp_t.re, (double)lp_t.im};
+}
+
+// Relative radius excursion |R/R0 - 1| above which the mixed path evaluates
+// the thermal model in FP64: FP32 is accurate for the small oscillations of a
+// quiet bubble, and its rounding is amplified once the bubble is driven.
+constexpr double kThermalFp64Excursion = 1.0e-3;
+
+template <typename T>
 __device__ __forceinline__ void rp_substep_full(const BubbleParams& bp, RpState& s) {
   const double PGn = s.PGp;
   const double PL = s.PC2 * s.time * s.time + s.PC1 * s.time + s.PC0;
   rp_substep(s.Rt, s.Rp, s.Rn, s.d1Rp, PGn, PL, s.dtL, s.remain, bp);
   s.time = s.time + s.dtL;
-  Cx<T> alpha_t;
-  const double omega = (double)omega_n<T>(alpha_t, (T)PGn, (T)s.Rn, bp, s.r);
-  const Cx<T> lp_t = lp_n<T>(alpha_t, (T)s.Rn);
-  const C64 lp{(double)lp_t.re, (double)lp_t.im};
+  double omega;
+  C64 lp;
+  if (sizeof(T) == sizeof(double) || fabs(s.Rn - s.r.R0) > kThermalFp64Excursion * s.r.R0)
+    thermal_model<double>(bp, s, PGn, omega, lp);
+  else
+    thermal_model<T>(bp, s, PGn, omega, lp);
   s.PGp = gas_pressure(PGn, s.Rp, s.Rn, omega, s.dtL, lp, bp, s.r);
   const double Rp = s.Rp, Rn = s.Rn, PGp = s.PGp;
   const double s0 = 0.5 * (Rp + Rn);
@@ -523,9 +723,13 @@ __device__ __forceinline__ void rp_end(const GridParams& g, const BubbleParams& 
 // while the queue has work.  Each bubble's arithmetic is the same as a
 // thread-per-bubble solve, so results do not depend on the schedule.
 constexpr int kRpThreads = 128;
+// At least 5 resident blocks per SM (at most 102 registers a thread): more
+// warps to hide the FP64 latency chains of the sub-step, measured faster than
+// the unconstrained 128 registers despite a few spilled values.
+constexpr int kRpMinBlocks = 5;
 
 template <typename P>
-__global__ void __launch_bounds__(kRpThreads) bubble_rp(const __grid_constant__ GridParams g,
+__global__ void __launch_bounds__(kRpThreads, kRpMinBlocks) bubble_rp(const __grid_constant__ GridParams g,
                                                         const __grid_constant__ BubbleParams bp, BubbleArrays b,
                                                         const typename P::S px, const typename P::S py,
                                                         double t_cur, const int* __restrict__ order,
@@ -535,14 +739,24 @@ __global__ void __launch_bounds__(kRpThreads) bubble_rp(const __grid_constant__ 
   int n = -1;
   bool drained = false;
   long long worst = 0;
+  const int lane = threadIdx.x & 31;
   for (;;) {
-    if (n < 0 && !drained) {
-      const int q = atomicAdd(next, 1);
-      if (q < b.n) {
-        n = order[q];
-        rp_begin(g, bp, b, px, py, t_cur, n, s);
-      } else {
-        drained = true;
+    // Lanes without a bubble claim the next ones from the queue together:
+    // one atomic per warp instead of one per lane.
+    const unsigned need = __ballot_sync(0xffffffffu, n < 0 && !drained);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(next, __popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need & (1u << lane)) {
+        const int q = base + __popc(need & ((1u << lane) - 1u));
+        if (q < b.n) {
+          n = order[q];
+          rp_begin(g, bp, b, px, py, t_cur, n, s);
+        } else {
+          drained = true;
+        }
       }
     }
     if (!__any_sync(0xffffffffu, n >= 0)) break;
@@ -592,10 +806,31 @@ __global__ void lpt_scan(int* __restrict__ hist, int* __restrict__ cursor) {
   hist[lane] = 0;
 }
 
-__global__ void lpt_scatter(const int* __restrict__ nsub, int n, int* __restrict__ cursor, int* __restrict__ order) {
+// Bubbles into their buckets' ranges.  Slots are reserved per warp (shared
+// atomics) and then per block (one global atomic per bucket), because most
+// bubbles usually share one bucket and per-bubble atomics on one counter
+// serialise.  The order inside a bucket is not fixed; it only affects scheduling.
+constexpr int kLptScatterThreads = 1024;
+
+__global__ void __launch_bounds__(kLptScatterThreads)
+    lpt_scatter(const int* __restrict__ nsub, int n, int* __restrict__ cursor, int* __restrict__ order) {
+  __shared__ int s_cnt[kLptBuckets], s_base[kLptBuckets];
+  if (threadIdx.x < kLptBuckets) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  order[atomicAdd(&cursor[lpt_bucket(nsub[k])], 1)] = k;
+  const int lane = threadIdx.x & 31;
+  const bool on = k < n;
+  const int bkt = on ? lpt_bucket(nsub[k]) : -1;
+  const unsigned peers = __match_any_sync(0xffffffffu, bkt);
+  const int leader = __ffs(peers) - 1;
+  int wbase = 0;
+  if (on && lane == leader) wbase = atomicAdd(&s_cnt[bkt], __popc(peers));
+  wbase = __shfl_sync(0xffffffffu, wbase, leader);
+  __syncthreads();
+  if (threadIdx.x < kLptBuckets && s_cnt[threadIdx.x])
+    s_base[threadIdx.x] = atomicAdd(&cursor[threadIdx.x], s_cnt[threadIdx.x]);
+  __syncthreads();
+  if (on) order[s_base[bkt] + wbase + __popc(peers & ((1u << lane) - 1u))] = k;
 }
 
 // Void fraction of one cell from the bubbles of the four bins whose stencils
@@ -625,6 +860,7 @@ struct CoupleArgs {
   const double* contrib;
   double t_cur;
   unsigned long long* residual;
+  int i0, j0, i1, j1;  // cells to update (inclusive)
 };
 
 // calculate_void_fraction (memset, scatter, VoidFractionCylinderKernel fold:
@@ -634,10 +870,10 @@ template <typename P>
 __global__ void __launch_bounds__(256) couple_press(const __grid_constant__ GridParams g, const CoupleArgs<P> a) {
   const Frame& f = g.f;
   const int X = f.X, Y = f.Y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;       // 0..X+1
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;       // 0..Y+1
+  const int i = a.i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = a.j0 + blockIdx.y * blockDim.y + threadIdx.y;
   double res = 0.0;
-  if (i <= X + 1 && j <= Y + 1) {
+  if (i <= a.i1 && j <= a.j1) {
     double fgv;
     if (g.cyl && i <= 1)
       fgv = gather_fg(f, a.start, a.idx, a.contrib, 0, j) + gather_fg(f, a.start, a.idx, a.contrib, 1, j);
@@ -758,6 +994,7 @@ struct Sim {
     int err;                      // nonzero: a bubble hit the sub-step cap
     int next;                     // work-queue head of the radius solve
     int moved;                    // nonzero: a bubble changed cell bin this step
+    int bbox[4];                  // bins occupied this step, encoded (bubble_move)
   };
   Scalars* d_scalars = nullptr;
   unsigned long long* d_residual = nullptr;
@@ -767,6 +1004,16 @@ struct Sim {
   int* d_moved = nullptr;
   Scalars* h_scalars = nullptr;  // pinned
   double picard_tol = 1.0e-7f;
+  // Cell boxes {i0, j0, i1, j1} (empty when i0 > i1).  supp[q] bounds the
+  // nonzero void fraction of step n-1-q; the coupling kernel updates only the
+  // union of the bubbles' box and supp[0..2]: outside it both the gathered and
+  // the predicted void fraction are zero, so the pressure from the FDTD pass
+  // already has its final value there.
+  struct Box {
+    int i0, j0, i1, j1;
+  };
+  Box supp[3];
+  Box couple_box;
   bool bins_stale = false;  // a bubble changed cell since the bins were built
   bool debug_picard = std::getenv("CRP_DEBUG_PICARD") != nullptr;  // residual of every Picard iteration to stderr
   struct Lpt {
@@ -876,6 +1123,8 @@ struct Sim {
       own_stream = true;
     }
     fill_params();
+    supp[0] = supp[1] = supp[2] = full_box();
+    couple_box = full_box();
     pool_bytes = layout(true);
     CRP_CUDA(cudaMalloc(&pool, pool_bytes));
     layout(false);
@@ -1025,13 +1274,39 @@ struct Sim {
     if ((e = launch(kClassOther, [&] { lpt_scan<<<1, 32, 0, stream>>>(lpt.hist, lpt.cursor); })) != cudaSuccess)
       return e;
     return launch(kClassOther,
-                  [&] { lpt_scatter<<<(n + 255) / 256, 256, 0, stream>>>(bub.nsub, n, lpt.cursor, lpt.order); });
+                  [&] {
+                    lpt_scatter<<<(n + kLptScatterThreads - 1) / kLptScatterThreads, kLptScatterThreads, 0, stream>>>(
+                        bub.nsub, n, lpt.cursor, lpt.order);
+                  });
   }
 
   // Void-fraction contributions of the initial radii (no RP step).
   cudaError_t launch_contrib_only();
 
   cudaError_t launch_couple(bool pressure);
+
+  Box full_box() const { return Box{0, 0, gp.f.X + 1, gp.f.Y + 1}; }
+  static bool box_empty(const Box& b) { return b.i0 > b.i1 || b.j0 > b.j1; }
+  static Box box_union(const Box& a, const Box& b) {
+    if (box_empty(a)) return b;
+    if (box_empty(b)) return a;
+    return Box{std::min(a.i0, b.i0), std::min(a.j0, b.j0), std::max(a.i1, b.i1), std::max(a.j1, b.j1)};
+  }
+  // Cells reached by the stencils of the occupied bins (bin (bx, by) feeds
+  // cells bx..bx+1, by..by+1; with the axis fold cells 0 and 1 go together).
+  Box bubble_box() const {
+    const int* e = h_scalars->bbox;
+    if (e[1] == 0) return Box{1, 1, 0, 0};
+    const int X = gp.f.X, Y = gp.f.Y;
+    Box b{std::max(0, kBoxOff - e[0]), std::max(0, kBoxOff - e[2]), std::min(X + 1, e[1] - kBoxOff + 1),
+          std::min(Y + 1, e[3] - kBoxOff + 1)};
+    if (box_empty(b)) return b;
+    if (gp.cyl && b.i0 <= 1) {
+      b.i0 = 0;
+      b.i1 = std::max(b.i1, 1);
+    }
+    return b;
+  }
 
   crp_status read_scalars() {
     CRP_CUDA(cudaMemcpyAsync(h_scalars, d_scalars, sizeof(Scalars), cudaMemcpyDeviceToHost, stream));
@@ -1052,7 +1327,7 @@ struct Sim {
     // Ring rotation of store_variables: the predicted f_g goes to the f_gm buffer.
     const int a = fg_a, b = fg_b, c = fg_c;
     CRP_CUDA(cudaMemsetAsync(d_residual, 0, sizeof(unsigned long long), stream));
-    CRP_CUDA(cudaMemsetAsync(d_moved, 0, sizeof(int), stream));
+    CRP_CUDA(cudaMemsetAsync(d_moved, 0, sizeof(int) * 5, stream));
     CRP_CUDA(mixed ? launch_fdtd<PrecMixed>(nv, np, a, b, c) : launch_fdtd<PrecFP64>(nv, np, a, b, c));
     cur_v = nv;
     cur_p = np;
@@ -1065,6 +1340,8 @@ struct Sim {
     double resimax = __longlong_as_double_host(h_scalars->residual) / gp.P_inf;
     int loop = 0;
     bins_stale = bins_stale || h_scalars->moved != 0;
+    const Box bnow = hs.nb > 0 ? bubble_box() : Box{1, 1, 0, 0};
+    couple_box = box_union(box_union(bnow, supp[0]), box_union(supp[1], supp[2]));
     if (hs.nb > 0 && resimax > picard_tol) {
       // Bins change only when a bubble crosses into another cell; the solve
       // order follows the latest sub-step counts.
@@ -1073,6 +1350,7 @@ struct Sim {
       CRP_CUDA(build_order());
     }
     if (hs.nb > 0) {
+      double prev = resimax;
       while (resimax > picard_tol) {
         if (loop >= cfg.ext_picard_cap) return fail(CRP_ERR_PICARD, "Picard iteration cap reached");
         loop++;
@@ -1086,9 +1364,20 @@ struct Sim {
         resimax = __longlong_as_double_host(h_scalars->residual) / gp.P_inf;
         if (debug_picard && loop <= 40)
           fprintf(stderr, "step %lld picard %d residual %.6e\n", (long long)stats.steps + 1, loop, resimax);
+        if (mixed && loop >= 3 && resimax > picard_tol && resimax > 0.5 * prev && resimax < CRP_MIXED_STALL_RESIDUAL) {
+          stats.picard_stalls++;
+          break;
+        }
+        prev = resimax;
       }
     }
     if (std::isnan(resimax)) return fail(CRP_ERR_NONFINITE, "non-finite pressure");
+    // Support of this step's void fraction: the gather's when it ran, else the
+    // prediction's.
+    const Box snow = loop > 0 ? bnow : box_union(supp[0], box_union(supp[1], supp[2]));
+    supp[2] = supp[1];
+    supp[1] = supp[0];
+    supp[0] = snow;
     stats.steps++;
     stats.time = tstep;
     stats.picard_last = loop;
@@ -1193,9 +1482,11 @@ struct Sim {
     fa.t_cur = tstep;
     fa.rho_const = stats.steps == 0 ? 1 : 0;
     fa.residual = d_residual;
-    dim3 grid((gp.f.X + 2 + kFdtdBX - 1) / kFdtdBX, (gp.f.Y + 2 + kFdtdBY - 1) / kFdtdBY);
-    dim3 block(kFdtdBX, kFdtdBY);
-    cudaError_t e = launch(kClassFdtd, [&] { fdtd_step<P><<<grid, block, 0, stream>>>(gp, fa); });
+    const int strips = (gp.f.X + kStripCells - 1) / kStripCells;
+    const int rows = kStripRows;
+    dim3 grid((strips + kStripWarps - 1) / kStripWarps, (gp.f.Y + rows - 1) / rows);
+    dim3 block(32, kStripWarps);
+    cudaError_t e = launch(kClassFdtd, [&] { fdtd_strip<P><<<grid, block, 0, stream>>>(gp, fa, rows); });
     if (e != cudaSuccess) return e;
     const int ng = std::max(gp.f.X, gp.f.Y) + 3;
     const V vxn = view<V>(vx[nv]), vyn = view<V>(vy[nv]);
@@ -1207,7 +1498,7 @@ struct Sim {
     using V = typename P::V;
     const V vxc = view<V>(vx[cur_v]), vyc = view<V>(vy[cur_v]);
     return launch(kClassOther, [&] {
-      bubble_move<V><<<(bub.n + 255) / 256, 256, 0, stream>>>(gp, bp, bub, vxc, vyc, d_moved);
+      bubble_move<V><<<(bub.n + kMoveThreads - 1) / kMoveThreads, kMoveThreads, 0, stream>>>(gp, bp, bub, vxc, vyc, d_moved);
     });
   }
 
@@ -1356,8 +1647,18 @@ cudaError_t Sim::launch_couple_t(bool pressure) {
   ca.contrib = bub.contrib;
   ca.t_cur = tstep;
   ca.residual = d_residual;
-  dim3 blk(32, 8), grd((gp.f.X + 2 + 31) / 32, (gp.f.Y + 2 + 7) / 8);
-  if (pressure) return launch(kClassCouple, [&] { couple_press<P><<<grd, blk, 0, stream>>>(gp, ca); });
+  dim3 blk(32, 8);
+  if (pressure) {
+    const Box& b = couple_box;
+    if (box_empty(b)) return cudaSuccess;
+    ca.i0 = b.i0;
+    ca.j0 = b.j0;
+    ca.i1 = b.i1;
+    ca.j1 = b.j1;
+    dim3 grd((b.i1 - b.i0 + 1 + 31) / 32, (b.j1 - b.j0 + 1 + 7) / 8);
+    return launch(kClassCouple, [&] { couple_press<P><<<grd, blk, 0, stream>>>(gp, ca); });
+  }
+  dim3 grd((gp.f.X + 2 + 31) / 32, (gp.f.Y + 2 + 7) / 8);
   return launch(kClassOther, [&] { couple_fg_only<P><<<grd, blk, 0, stream>>>(gp, ca); });
 }
 

@@ -52,8 +52,10 @@ typedef enum crp_status {
 /* Arithmetic of the grid fields. */
 typedef enum crp_precision {
   CRP_PREC_FP64 = 0,   /* all state and arithmetic in FP64 (the reference's precision) */
-  CRP_PREC_MIXED = 1   /* FP32 fields with compensated (Kahan) accumulation; FP64 void
-                          fraction and FP64 bubble dynamics in the stiff phase */
+  CRP_PREC_MIXED = 1   /* velocity and pressure stored as an FP32 value plus an FP32
+                          compensation term (FP64 arithmetic); void fraction stored in
+                          FP32 (FP64 sums); bubble thermal model in FP32 while
+                          |R/R0 - 1| <= 1e-3, FP64 otherwise; radius update FP64 */
 } crp_precision;
 
 /* Every key of the reference configuration (src/bubbles.cpp:76-132) plus the
@@ -160,7 +162,16 @@ typedef struct crp_stats {
    * (crp_set_profiling): the fused FDTD kernel, the RP kernel, the coupling
    * gather + pressure kernel, and everything else (ghosts, motion, binning). */
   double ms_fdtd, ms_rp, ms_couple, ms_other;
+  /* Steps whose Picard loop the mixed path ended on stagnation: the residual
+   * stopped falling (less than halved by an iteration, from the third on)
+   * while below CRP_MIXED_STALL_RESIDUAL.  Always 0 in the FP64 path. */
+  int64_t picard_stalls;
 } crp_stats;
+
+/* Residual (max |dp0| / P_inf) below which the mixed path accepts a stagnating
+ * Picard loop.  FP32 storage of the void fraction puts a floor of about 1e-6
+ * under the residual, and a loop can settle into a short cycle above it. */
+#define CRP_MIXED_STALL_RESIDUAL 1.0e-3
 
 /* Explicit bubble population: n bubbles with position (x, y), equilibrium
  * radius R0 and weight n_B.  Replaces the per-cell lattice of the reference
