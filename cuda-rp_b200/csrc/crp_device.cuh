@@ -55,6 +55,12 @@ struct GridParams {
 // per-bubble R0-derived values live in the bubble arrays.
 struct BubbleParams {
   double PL0, T0, gam, sig, mu, rho, K0, dt0;
+  double inv_rho;  // 1 / rho
+  // Smallest |a|^2 whose square root exceeds 0.1 in FP64 / FP32: the series
+  // switch of Upsilon and Lp (cabs(a) > 0.1) without a square root on the
+  // sub-step's critical path, deciding exactly as the square root would.
+  double abs2_cut64;
+  float abs2_cut32;
   double pi, pi4r3;
   double dcx, dcy, dcz;  // delta_coef (src/bubble_CUDA.cu:1469-1471)
   long long step_cap;
@@ -212,34 +218,53 @@ template <typename R>
 __device__ __forceinline__ R cabsx(Cx<R> a) {
   return sqrt(a.re * a.re + a.im * a.im);
 }
+// cabs(a) > 0.1, decided on |a|^2 (see BubbleParams::abs2_cut64).
 template <typename R>
-__device__ __forceinline__ Cx<R> ccoth(Cx<R> a) {
-  R x = tanh(a.re), y = tan(a.im);
-  return cdiv(Cx<R>{R(1), x * y}, Cx<R>{x, y});
+__device__ __forceinline__ bool above_series_cut(Cx<R> a, R cut2) {
+  return a.re * a.re + a.im * a.im >= cut2;
+}
+// coth(a) = N / D with N = (1, tanh(re) tan(im)) and D = (tanh(re), tan(im))
+// (inc/complex.cuh's coth before its division).  Callers fold the division into
+// their own, so a sub-step carries one complex division per Upsilon / Lp
+// evaluation on its critical path instead of three.
+template <typename R>
+__device__ __forceinline__ void coth_parts(Cx<R> a, Cx<R>& N, Cx<R>& D) {
+  const R x = tanh(a.re), y = tan(a.im);
+  N = Cx<R>{R(1), x * y};
+  D = Cx<R>{x, y};
 }
 using C64 = Cx<double>;
 
 // Per-bubble constants derived from its R0 (init_bub_params, src/bubble_CUDA.cu:666-670).
 struct BubbleR0 {
-  double R0, PG0, R03, coeff_alpha;
+  double R0, PG0, R03, coeff_alpha, inv_R0, inv_PG0;
 };
 __device__ __forceinline__ BubbleR0 bubble_r0(const BubbleParams& b, double R0) {
   BubbleR0 r;
   r.R0 = R0;
+  r.inv_R0 = 1.0 / R0;
   r.R03 = R0 * R0 * R0;
   r.PG0 = b.PL0 + 2.0 * b.sig / R0;
+  r.inv_PG0 = 1.0 / r.PG0;
   r.coeff_alpha = b.gam * r.PG0 * r.R03 / (2.0 * (b.gam - 1.0) * b.T0 * b.K0);
   return r;
 }
 
-// Upsilon (:297-307).
+// Upsilon (:297-307): 3 gam / (1 + 3 (gam - 1) t), t = (a coth(a) - 1) / a^2.
+// With coth(a) = N / D and M = a N - D (so a coth(a) - 1 = M / D) this is
+// 3 gam D a^2 / (D a^2 + 3 (gam - 1) M): the same quantity with one division.
 template <typename R>
-__device__ __forceinline__ Cx<R> upsilon(Cx<R> a, R gam) {
+__device__ __forceinline__ Cx<R> upsilon(Cx<R> a, R gam, R cut2) {
   Cx<R> aa = cmul(a, a);
   Cx<R> t;
-  if (cabsx(a) > R(1.0e-1)) {
-    Cx<R> ac = cmul(a, ccoth(a));
-    t = cdiv(Cx<R>{ac.re - R(1), ac.im}, aa);
+  if (above_series_cut(a, cut2)) {
+    Cx<R> N, D;
+    coth_parts(a, N, D);
+    const Cx<R> aN = cmul(a, N);
+    const Cx<R> M{aN.re - D.re, aN.im - D.im};
+    const Cx<R> Da = cmul(D, aa);
+    const R g3 = R(3) * (gam - R(1));
+    return cdiv(cscl(Da, R(3) * gam), Cx<R>{Da.re + g3 * M.re, Da.im + g3 * M.im});
   } else {
     Cx<R> q = cmul(aa, Cx<R>{R(2.0 / 945.0) - xdiv(aa.re, R(4725.0)), xdiv(-aa.im, R(4725.0))});
     Cx<R> m = cmul(aa, Cx<R>{R(-1.0 / 45.0) + q.re, q.im});
@@ -251,13 +276,18 @@ __device__ __forceinline__ Cx<R> upsilon(Cx<R> a, R gam) {
 
 // solveLp (:310-323).
 template <typename R>
-__device__ __forceinline__ Cx<R> lp_n(Cx<R> a, R Rb) {
+__device__ __forceinline__ Cx<R> lp_n(Cx<R> a, R Rb, R cut2) {
   Cx<R> aa = cmul(a, a);
   Cx<R> c;
-  if (cabsx(a) > R(1.0e-1)) {
-    Cx<R> ac = cmul(a, ccoth(a));
-    c = Cx<R>{ac.re - R(1), ac.im};
-    c = cdiv(Cx<R>{aa.re - R(3) * c.re, aa.im - R(3) * c.im}, cmul(aa, c));
+  if (above_series_cut(a, cut2)) {
+    // (a^2 - 3 c) / (a^2 c) with c = a coth(a) - 1 = M / D:
+    // (a^2 D - 3 M) / (a^2 M), one division.
+    Cx<R> N, D;
+    coth_parts(a, N, D);
+    const Cx<R> aN = cmul(a, N);
+    const Cx<R> M{aN.re - D.re, aN.im - D.im};
+    const Cx<R> Da = cmul(aa, D);
+    c = cdiv(Cx<R>{Da.re - R(3) * M.re, Da.im - R(3) * M.im}, cmul(aa, M));
   } else {
     Cx<R> a37 = cscl(aa, R(37));
     Cx<R> q = cmul(aa, Cx<R>{R(2.0 / 7875.0) - xdiv(a37.re, R(3031875.0)), xdiv(-a37.im, R(3031875.0))});
@@ -265,6 +295,17 @@ __device__ __forceinline__ Cx<R> lp_n(Cx<R> a, R Rb) {
     c = Cx<R>{R(1.0 / 5.0) + m.re, m.im};
   }
   return cscl(c, Rb);
+}
+
+template <typename R>
+__device__ __forceinline__ R series_cut(const BubbleParams& b);
+template <>
+__device__ __forceinline__ double series_cut<double>(const BubbleParams& b) {
+  return b.abs2_cut64;
+}
+template <>
+__device__ __forceinline__ float series_cut<float>(const BubbleParams& b) {
+  return b.abs2_cut32;
 }
 
 // solveOmegaN (:263-288): omega_N and alpha_N for gas pressure PG at radius Rb.
@@ -280,15 +321,20 @@ __device__ __forceinline__ R omega_n(Cx<R>& alpha, R PG, R Rb, const BubbleParam
   R ups_re = R(3) * gam * coef1;
   R mu_eff = mu;
   R eta = ups_re * coef2 + value1 - mu_eff * mu_eff * coef3;
-  R omega = xdiv(sqrt(fmax(eta, R(1.0e-6) * eps)), rho * Rb);
+  // Loop invariants as reciprocals/quotients, so that the iteration's chain is
+  // sqrt -> Upsilon (one division) -> sqrt.
+  const R inv_rho_Rb = xdiv(R(1), rho * Rb);
+  const R ca_Rb = xdiv(ca, Rb);
+  R omega = sqrt(fmax(eta, R(1.0e-6) * eps)) * inv_rho_Rb;
   for (int k = 0; k < 3; k++) {
-    R s = sqrt(xdiv(ca, Rb) * omega);
-    Cx<R> u = cscl(upsilon(Cx<R>{s, s}, gam), coef1);
-    mu_eff = mu + xdiv(u.im * PG, R(4) * omega);
+    R s = sqrt(ca_Rb * omega);
+    const R pg_4w = xdiv(PG, R(4) * omega);  // independent of Upsilon
+    Cx<R> u = cscl(upsilon(Cx<R>{s, s}, gam, series_cut<R>(b)), coef1);
+    mu_eff = mu + u.im * pg_4w;
     eta = u.re * coef2 + value1 - mu_eff * mu_eff * coef3;
-    omega = xdiv(sqrt(fmax(eta, R(1.0e-6) * eps)), rho * Rb);
+    omega = sqrt(fmax(eta, R(1.0e-6) * eps)) * inv_rho_Rb;
   }
-  R s = sqrt(xdiv(ca, Rb) * omega);
+  R s = sqrt(ca_Rb * omega);
   alpha = Cx<R>{s, s};
   return omega;
 }
@@ -297,16 +343,18 @@ __device__ __forceinline__ R omega_n(Cx<R>& alpha, R PG, R Rb, const BubbleParam
 __device__ __forceinline__ double gas_pressure(double PGn, double Rp, double Rn, double omega, double dt, C64 lp,
                                                const BubbleParams& b, const BubbleR0& r) {
   double R = 0.5 * (Rp + Rn);
-  double Rx = R / r.R0;
-  double Rpx = Rp / r.R0;
-  double Rnx = Rn / r.R0;
-  double den = lp.re * lp.re + lp.im * lp.im;
-  double lpr = lp.re / den;
-  double lpi = lp.im / den;
-  double c0 = dt * 3.0 * (b.gam - 1.0) * b.K0 * b.T0 / (R * r.PG0);
-  double c3 = 1.5 * b.gam * (Rp - Rn) / R + c0 * lpr * 0.5 * Rx * Rx * Rx;
-  double c1 = 1.0 + c3 - c0 * lpi / (omega * dt) * Rpx * Rpx * Rpx;
-  double c2 = 1.0 - c3 - c0 * lpi / (omega * dt) * Rnx * Rnx * Rnx;
+  double Rx = R * r.inv_R0;
+  double Rpx = Rp * r.inv_R0;
+  double Rnx = Rn * r.inv_R0;
+  const double inv_R = 1.0 / R;
+  const double inv_den = 1.0 / (lp.re * lp.re + lp.im * lp.im);
+  double lpr = lp.re * inv_den;
+  double lpi = lp.im * inv_den;
+  double c0 = dt * 3.0 * (b.gam - 1.0) * b.K0 * b.T0 * inv_R * r.inv_PG0;
+  double c3 = 1.5 * b.gam * (Rp - Rn) * inv_R + c0 * lpr * 0.5 * Rx * Rx * Rx;
+  const double w = c0 * lpi / (omega * dt);
+  double c1 = 1.0 + c3 - w * Rpx * Rpx * Rpx;
+  double c2 = 1.0 - c3 - w * Rnx * Rnx * Rnx;
   return (c2 * PGn + c0 * lpr * r.PG0) / c1;
 }
 
@@ -316,20 +364,21 @@ __device__ __forceinline__ void rp_substep(double& Rt, double& Rp, double& Rn, d
   const double eps = 2.22044604925031308e-016;
   double Rm = Rn;
   Rn = Rp;
-  double acc = (PG - PL - 2.0 * b.sig / Rn - 4.0 * b.mu / Rn * d1R) / b.rho - 1.5 * d1R * d1R;
+  const double inv_Rn = 1.0 / Rn;
+  double acc = (PG - PL - 2.0 * b.sig * inv_Rn - 4.0 * b.mu * inv_Rn * d1R) * b.inv_rho - 1.5 * d1R * d1R;
   double dtm = dt;
   double dtp = fmin(1.01 * dt, b.dt0);
   if (fabs(d1R) > eps) dtp = fmin(dtp, 0.01 * Rn / fabs(d1R));
   if (fabs(acc) > eps) dtp = fmin(dtp, 0.1 * Rn / sqrt(fabs(acc)));
   double q = dtp / dtm;
-  Rt = Rp = (1.0 + q) * Rn - q * Rm + (dtp / Rn) * (0.5 * (dtp + dtm) * acc);
+  Rt = Rp = (1.0 + q) * Rn - q * Rm + (dtp * inv_Rn) * (0.5 * (dtp + dtm) * acc);
   d1R = (dtm * dtm * Rp + (-dtm * dtm + dtp * dtp) * Rn - dtp * dtp * Rm) / (dtm * dtp * (dtm + dtp)) +
-        (dtp / Rn) * acc;
+        (dtp * inv_Rn) * acc;
   dt = dtp;
   if (dtp >= remain) {
     dtp = remain;
     double qr = dtp / dtm;
-    Rt = (1.0 + qr) * Rn - qr * Rm + (dtp / Rn) * (0.5 * (dtp + dtm) * acc);
+    Rt = (1.0 + qr) * Rn - qr * Rm + (dtp * inv_Rn) * (0.5 * (dtp + dtm) * acc);
   }
   remain -= dtp;
 }

@@ -654,7 +654,7 @@ __device__ __forceinline__ void thermal_model(const BubbleParams& bp, const RpSt
                                               C64& lp) {
   Cx<T> alpha_t;
   omega = (double)omega_n<T>(alpha_t, (T)PGn, (T)s.Rn, bp, s.r);
-  const Cx<T> lp_t = lp_n<T>(alpha_t, (T)s.Rn);
+  const Cx<T> lp_t = lp_n<T>(alpha_t, (T)s.Rn, series_cut<T>(bp));
   lp = C64{(double)lp_t.re, (double)lp_t.im};
 }
 
@@ -1218,6 +1218,18 @@ struct Sim {
     bp.sig = cfg.bub_sigma;
     bp.mu = cfg.bub_mu;
     bp.rho = cfg.bub_rho;
+    bp.inv_rho = 1.0 / cfg.bub_rho;
+    {
+      // Smallest squared modulus whose square root is above 0.1, per precision.
+      double c = 0.01;
+      while (std::sqrt(c) > 0.1) c = std::nextafter(c, 0.0);
+      while (!(std::sqrt(c) > 0.1)) c = std::nextafter(c, 1.0);
+      bp.abs2_cut64 = c;
+      float cf = 0.01f;
+      while (std::sqrt(cf) > 0.1f) cf = std::nextafter(cf, 0.0f);
+      while (!(std::sqrt(cf) > 0.1f)) cf = std::nextafter(cf, 1.0f);
+      bp.abs2_cut32 = cf;
+    }
     bp.K0 = cfg.bub_K0;
     bp.dt0 = d.bub_dt0;
     bp.pi = d.pi;
