@@ -73,7 +73,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="axisym_1024x2048", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="axisym_1024x2048", choices=list(WORKLOADS) + ["sweep_64"])
     ap.add_argument("--chunk", type=int, default=100)
     ap.add_argument("--preroll", type=int, default=0)
     ap.add_argument("--driven-start", type=int, default=None)
@@ -209,7 +209,14 @@ def run_reference(args, rank, world):
         return None
     import _bind as B
 
-    cfg, bub = load_workload(args.workload)
+    if args.workload == "sweep_64":
+        import crp
+
+        cfgs, _ = sweep_configs()
+        cfg = cfgs[0]
+        bub = crp.seed_bubbles(cfg)
+    else:
+        cfg, bub = load_workload(args.workload)
     threads = os.cpu_count() or 1
     o = B.OracleSim(cfg, bub, threads=threads)
     for _ in range(args.warmup):
@@ -435,6 +442,101 @@ def run_ours(args, rank, world, dist):
     return result
 
 
+SWEEP_SEED = 0xC0DA0004
+
+
+def sweep_configs(n=64):
+    """The batched-sweep workload: n axisymmetric simulations with grids X in
+    [128, 512] (Y = 2X, dx = 0.1 mm), 1k-64k seeded bubbles (log-uniform), R0
+    median 2-5 um (sigma_ln 0.3), 0.2-2.5 MPa surface drive at 0.5-2 MHz, the
+    focus at 60 % of the length, and 2000-8000 steps each (the nominal length;
+    the bench times a bounded number of them)."""
+    import crp
+
+    rng = np.random.default_rng(SWEEP_SEED)
+    base = crp.parse_file(WORKLOADS["axisym_256x512"])
+    cfgs, steps = [], []
+    for k in range(n):
+        c = crp.Config.from_buffer_copy(base)
+        X = int(rng.integers(128, 513)) // 8 * 8
+        c.grid_x, c.grid_y = X, 2 * X
+        c.grid_lx, c.grid_ly = X * 1e-4, 2 * X * 1e-4
+        c.tr_amp = float(rng.uniform(0.2e6, 2.5e6)) / (998.0 * 1482.0)
+        c.tr_freq = float(rng.uniform(0.5e6, 2.0e6))
+        c.tr_focal_dist = 0.6 * c.grid_ly * 2.0 / np.sqrt(3.0)
+        c.ext_bubble_count = int(round(np.exp(rng.uniform(np.log(1e3), np.log(6.4e4)))))
+        c.bub_R0 = float(rng.uniform(2e-6, 5e-6))
+        c.ext_bubble_seed = SWEEP_SEED + 1 + k
+        c.ext_cloud_r = 0.1 * c.grid_lx
+        c.ext_cloud_h = 0.2 * c.grid_ly
+        cfgs.append(c)
+        steps.append(int(rng.integers(2000, 8001)))
+    return cfgs, steps
+
+
+def run_sweep(args, rank, world):
+    """Batched sweep on one GPU (crp_batch): every simulation advances
+    args.chunk mixture steps per bench step from t = 0; device time from
+    events on every simulation's stream (first start to last end)."""
+    import torch
+
+    import crp
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    cfgs, nominal = sweep_configs()
+    n = len(cfgs)
+    for c in cfgs:
+        c.ext_precision = 1 if args.primary == "mixed" else 0
+    with crp.Batch(cfgs) as batch:
+        streams = [torch.cuda.ExternalStream(s.stream) for s in batch.sims]
+        failed = {}
+
+        def run(k_steps):
+            try:
+                batch.run([k_steps] * n)
+            except crp.CrpError:
+                for k, s in enumerate(batch.sims):
+                    if k not in failed and s.stats().steps < batch_done[k] + k_steps:
+                        failed[k] = int(s.stats().steps)
+
+        batch_done = [0] * n
+        run(args.warmup * args.chunk)
+        batch_done = [s.stats().steps for s in batch.sims]
+        s0 = [s.stats() for s in batch.sims]
+        e0 = [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+        e1 = [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+        torch.cuda.synchronize()
+        with Clocks(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+            for k in range(n):
+                e0[k].record(streams[k])
+            t0 = time.perf_counter()
+            run(args.steps * args.chunk)
+            wall = time.perf_counter() - t0
+            for k in range(n):
+                e1[k].record(streams[k])
+            torch.cuda.synchronize()
+        s1 = [s.stats() for s in batch.sims]
+        ms = max(e0[0].elapsed_time(e1[k]) for k in range(n)) - min(
+            e0[0].elapsed_time(e0[k]) for k in range(n))
+        cell_steps = sum(c.grid_x * c.grid_y * (b.steps - a.steps) for c, a, b in zip(cfgs, s0, s1))
+        bub_steps = sum(sim.dims.num_bubbles * (b.steps - a.steps) for sim, a, b in zip(batch.sims, s0, s1))
+        launches = sum(b.kernel_launches - a.kernel_launches for a, b in zip(s0, s1))
+        value = cell_steps / (ms * 1e-3) / 1e6
+        return {
+            "metric": "Mcell-upd/s", "value": value, "unit": "Mcell-upd/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": DTYPE[args.primary], "data": "synthetic (seeded sweep and bubbles)",
+            "config": {"workload": "sweep_64", "simulations": n,
+                       "cells": int(sum(c.grid_x * c.grid_y for c in cfgs)),
+                       "bubbles": int(sum(sim.dims.num_bubbles for sim in batch.sims)),
+                       "mixture_steps_per_step": args.chunk, "start": f"t = 0 + {args.warmup * args.chunk} steps",
+                       "nominal_steps": [min(nominal), max(nominal)], "parallelism": "concurrent streams x64",
+                       "l2": "state > L2 (no flush needed)"},
+            "bubble_steps_per_s": bub_steps / (ms * 1e-3), "gpu_launches": int(launches),
+            "failed_simulations": failed, "wall_s": wall, "clocks": clk.summary(),
+        }
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", 0))
@@ -456,7 +558,7 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
     try:
-        res = run_ours(args, rank, world, dist)
+        res = run_sweep(args, rank, world) if args.workload == "sweep_64" else run_ours(args, rank, world, dist)
         if rank == 0 and res is not None:
             print(json.dumps(res), flush=True)
     finally:

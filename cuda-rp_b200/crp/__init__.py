@@ -130,6 +130,11 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "crp_destroy": (None, [vp]),
         "crp_void_fraction_noalloc_scratch": (ctypes.c_size_t, [c_int, c_int, c_int]),
         "crp_void_fraction_noalloc": (c_int, [P(Config), c_int, vp, vp, vp, vp, vp, vp]),
+        "crp_batch_create": (c_int, [c_int, P(Config), P(BubblesIn), P(vp)]),
+        "crp_batch_run": (c_int, [vp, P(c_int), c_int, P(c_int)]),
+        "crp_batch_count": (c_int, [vp]),
+        "crp_batch_sim": (vp, [vp, c_int]),
+        "crp_batch_destroy": (None, [vp]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -237,6 +242,64 @@ class Sim:
     def close(self):
         if getattr(self, "h", None):
             self.lib.crp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class _BatchSim(Sim):
+    """A simulation owned by a Batch (not destroyed on its own)."""
+
+    def __init__(self, lib, h, keep):
+        self.lib = lib
+        self._keep = keep
+        self.h = ctypes.c_void_p(h)
+        self.dims = Dims()
+        self._check(self.lib.crp_get_dims(self.h, ctypes.byref(self.dims)))
+
+    def close(self):
+        self.h = None
+
+
+class Batch:
+    """Independent simulations advanced concurrently (crp_batch)."""
+
+    def __init__(self, cfgs: list[Config], bubbles: list[Bubbles | None] | None = None):
+        self.lib = load()
+        n = len(cfgs)
+        self._cfgs = (Config * n)(*cfgs)
+        bubbles = bubbles or [None] * n
+        self._bub = bubbles
+        self._bin = (BubblesIn * n)(*[b.as_c() if b is not None else BubblesIn() for b in bubbles])
+        h = ctypes.c_void_p()
+        st = self.lib.crp_batch_create(n, self._cfgs, self._bin, ctypes.byref(h))
+        if st:
+            raise CrpError(st, self.lib.crp_status_string(st).decode())
+        self.h = h
+        self.sims = [_BatchSim(self.lib, self.lib.crp_batch_sim(self.h, k), (cfgs[k], bubbles[k])) for k in range(n)]
+
+    def run(self, steps: list[int], threads: int = 0) -> list[int]:
+        n = len(self.sims)
+        st_arr = (c_int * n)()
+        st = self.lib.crp_batch_run(self.h, (c_int * n)(*steps), threads, st_arr)
+        per = list(st_arr)
+        if st:
+            bad = [k for k, v in enumerate(per) if v]
+            raise CrpError(st, f"simulations {bad} failed: {self.lib.crp_status_string(st).decode()}")
+        return per
+
+    def close(self):
+        if getattr(self, "h", None):
+            for s in self.sims:
+                s.close()
+            self.lib.crp_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -107,9 +107,10 @@ __device__ __forceinline__ bool source_value(const GridParams& g, bool pressure,
 }
 
 // Field storage.  FP64 path: one double per value.  Mixed path: an FP32 value
-// plus an FP32 compensation term holding its rounding error (hi + lo carries
-// about 48 significant bits); arithmetic is done in FP64 registers and each
-// store re-splits the result, so no rounding error accumulates step to step.
+// plus an FP32 compensation term holding its rounding error (value +
+// compensation carries about 48 significant bits), stored as one float2;
+// arithmetic is done in FP64 registers and each store re-splits the result,
+// so no rounding error accumulates step to step.
 struct F64 {
   double* p;
   __device__ __forceinline__ double get(long k) const { return p[k]; }
@@ -122,25 +123,23 @@ struct F64 {
   __device__ static __forceinline__ double staged(const void* src) { return *(const double*)src; }
 };
 struct F32c {
-  float* hi;
-  float* lo;
-  __device__ __forceinline__ double get(long k) const { return (double)hi[k] + (double)lo[k]; }
+  float2* p;  // (value, compensation) pairs, one 8-byte access per element
+  __device__ __forceinline__ double get(long k) const {
+    const float2 v = p[k];
+    return (double)v.x + (double)v.y;
+  }
   __device__ __forceinline__ void put(long k, double v) const {
     const float h = (float)v;
-    hi[k] = h;
-    lo[k] = (float)(v - (double)h);
+    p[k] = make_float2(h, (float)(v - (double)h));
   }
   __device__ static __forceinline__ double stored(double v) {
     const float h = (float)v;
     return (double)h + (double)(float)(v - (double)h);
   }
-  __device__ __forceinline__ void stage(void* dst, long k) const {
-    __pipeline_memcpy_async(dst, hi + k, 4);
-    __pipeline_memcpy_async((char*)dst + 4, lo + k, 4);
-  }
+  __device__ __forceinline__ void stage(void* dst, long k) const { __pipeline_memcpy_async(dst, p + k, 8); }
   __device__ static __forceinline__ double staged(const void* src) {
-    const float* v = (const float*)src;
-    return (double)v[0] + (double)v[1];
+    const float2 v = *(const float2*)src;
+    return (double)v.x + (double)v.y;
   }
 };
 // Void-fraction history of the mixed path: FP32 storage (sums are FP64).

@@ -1430,15 +1430,15 @@ struct Sim {
       CRP_CUDA(cudaStreamSynchronize(stream));
       return CRP_OK;
     }
-    std::vector<float> hi((size_t)w * h), lo(kind == 1 ? (size_t)w * h : 0);
+    // kind 1: (value, compensation) float pairs; kind 2: single floats.
+    const size_t per = kind == 1 ? 2 : 1;
+    std::vector<float> v((size_t)w * h * per);
     const float* fb = (const float*)buf;
-    CRP_CUDA(cudaMemcpy2DAsync(hi.data(), sizeof(float) * w, fb + off, sizeof(float) * f.pitch, sizeof(float) * w, h,
-                               cudaMemcpyDeviceToHost, stream));
-    if (kind == 1)
-      CRP_CUDA(cudaMemcpy2DAsync(lo.data(), sizeof(float) * w, fb + cells + off, sizeof(float) * f.pitch,
-                                 sizeof(float) * w, h, cudaMemcpyDeviceToHost, stream));
+    CRP_CUDA(cudaMemcpy2DAsync(v.data(), sizeof(float) * per * w, fb + per * off, sizeof(float) * per * f.pitch,
+                               sizeof(float) * per * w, h, cudaMemcpyDeviceToHost, stream));
     CRP_CUDA(cudaStreamSynchronize(stream));
-    for (size_t q = 0; q < hi.size(); q++) host[q] = (double)hi[q] + (kind == 1 ? (double)lo[q] : 0.0);
+    for (size_t q = 0; q < (size_t)w * h; q++)
+      host[q] = kind == 1 ? (double)v[2 * q] + (double)v[2 * q + 1] : (double)v[q];
     return CRP_OK;
   }
 
@@ -1633,7 +1633,7 @@ F64 Sim::view<F64>(void* b) const {
 }
 template <>
 F32c Sim::view<F32c>(void* b) const {
-  return F32c{(float*)b, (float*)b + cells};
+  return F32c{(float2*)b};
 }
 template <>
 F32 Sim::view<F32>(void* b) const {

@@ -262,6 +262,21 @@ size_t crp_void_fraction_noalloc_scratch(int32_t grid_x, int32_t grid_y, int32_t
 crp_status crp_void_fraction_noalloc(const crp_config* cfg, int32_t n, const double* x, const double* y,
                                      const double* r, const double* n_b, double* f_g, void* stream);
 
+/* Batched sweep: count independent simulations (cfgs[k], bubbles[k] or NULL /
+ * n = 0 for the configuration's own seeding), each with its own stream, run
+ * concurrently.  Replaces re-running `bubbles` over a list of configuration
+ * files (scripts/executor.sh:28-47).  crp_batch_run advances simulation k by
+ * steps[k] mixture steps from a pool of host threads (threads <= 0: up to 32),
+ * largest cells x steps first; per_sim (may be NULL) receives each status and
+ * the first non-OK status in index order is returned.  The simulations are
+ * crp_sim handles (crp_batch_sim) for reading fields, stats and rawdata. */
+typedef struct crp_batch crp_batch;
+crp_status crp_batch_create(int32_t count, const crp_config* cfgs, const crp_bubbles_in* bubbles, crp_batch** out);
+crp_status crp_batch_run(crp_batch* batch, const int32_t* steps, int32_t threads, crp_status* per_sim);
+int32_t crp_batch_count(const crp_batch* batch);
+crp_sim* crp_batch_sim(crp_batch* batch, int32_t k);
+void crp_batch_destroy(crp_batch* batch);
+
 const char* crp_last_error(const crp_sim* sim);
 const char* crp_status_string(crp_status s);
 void crp_destroy(crp_sim* sim);

@@ -50,6 +50,17 @@ def test_create_without_device_fails_cleanly():
     assert e.value.status == 10  # CRP_ERR_NO_DEVICE
 
 
+def test_batch_without_device_fails_cleanly():
+    """Without a GPU, crp_batch_create returns the first simulation's error."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(crp.CrpError) as e:
+        crp.Batch([B.small_config(), B.small_config()])
+    assert e.value.status == 10  # CRP_ERR_NO_DEVICE
+
+
 def test_struct_sizes_match_c():
     """ctypes mirrors have the C layout (offset of the last member + size)."""
     src = os.path.join(ROOT, "_work_sizes.c")
