@@ -158,37 +158,30 @@ int main(int argc, char** argv) {
     std::cerr << "error: " << crp_status_string(st) << std::endl;
     return 1;
   }
-  crp_stats stats;
-  int64_t nstep = 0;
-  double tstep = 0.0;
-  const int save = cfg.sim_save_interval > 0 ? cfg.sim_save_interval : 0;
-  while (((cfg.sim_n_step_max != 0) && (nstep < cfg.sim_n_step_max)) ||
-         ((cfg.sim_t_step_max != 0) && (tstep < cfg.sim_t_step_max))) {
-    st = crp_step(sim, 1);
-    if (st != CRP_OK) {
-      std::cerr << "\nerror at step " << nstep + 1 << ": " << crp_status_string(st) << ": " << crp_last_error(sim)
-                << std::endl;
-      crp_destroy(sim);
-      return 1;
-    }
+  // Progress line as the reference prints it at each save (src/bubbles.cpp:258-268).
+  struct Progress {
+    const crp_config* cfg;
+  } prog{&cfg};
+  crp_output_plan plan{};
+  plan.save_interval = cfg.sim_save_interval > 0 ? cfg.sim_save_interval : 0;
+  plan.dir = ascii ? target_dir.c_str() : nullptr;
+  plan.user = &prog;
+  plan.progress = [](int64_t step, double time, void* user) {
+    const crp_config* c = ((Progress*)user)->cfg;
+    if (c->sim_n_step_max != 0)
+      printf("\rRunning the simulation...\t\tnstep : %5lld / %i\t", (long long)step, c->sim_n_step_max);
+    else
+      printf("\rRunning the simulation...\t\ttstep : %4.2E / %4.2E\t", time, c->sim_t_step_max);
+    fflush(stdout);
+  };
+  st = crp_run(sim, &plan, &cfg);
+  if (st != CRP_OK) {
+    crp_stats stats;
     crp_get_stats(sim, &stats);
-    nstep = stats.steps;
-    tstep = stats.time;
-    if (save && nstep % save == 0) {
-      if (ascii) {
-        st = crp_write_rawdata(sim, target_dir.c_str());
-        if (st != CRP_OK) {
-          std::cerr << "\nerror writing rawdata: " << crp_status_string(st) << std::endl;
-          crp_destroy(sim);
-          return 1;
-        }
-      }
-      if (cfg.sim_n_step_max != 0)
-        printf("\rRunning the simulation...\t\tnstep : %5lld / %i\t", (long long)nstep, cfg.sim_n_step_max);
-      else
-        printf("\rRunning the simulation...\t\ttstep : %4.2E / %4.2E\t", tstep, cfg.sim_t_step_max);
-      fflush(stdout);
-    }
+    std::cerr << "\nerror at step " << stats.steps + 1 << ": " << crp_status_string(st) << ": " << crp_last_error(sim)
+              << std::endl;
+    crp_destroy(sim);
+    return 1;
   }
   printf("\rRunning the simulation...\t\tdone\n\n");
 

@@ -46,6 +46,7 @@ class Config(ctypes.Structure):
         ("ext_picard_cap", c_int), ("ext_rp_step_cap", c_int), ("ext_bubble_count", c_int),
         ("ext_bubble_seed", ctypes.c_uint64), ("ext_r0_sigma_ln", c_dbl), ("ext_cloud_shape", c_int),
         ("ext_cloud_r", c_dbl), ("ext_cloud_h", c_dbl), ("ext_n_b", c_dbl), ("ext_picard_tol", c_dbl),
+        ("ext_graphs", c_int),
     ]
 
 
@@ -61,6 +62,14 @@ class Stats(ctypes.Structure):
                 ("rp_launches", ctypes.c_int64), ("couple_launches", ctypes.c_int64),
                 ("ms_fdtd", c_dbl), ("ms_rp", c_dbl), ("ms_couple", c_dbl), ("ms_other", c_dbl),
                 ("picard_stalls", ctypes.c_int64)]
+
+
+PROGRESS = ctypes.CFUNCTYPE(None, ctypes.c_int64, c_dbl, ctypes.c_void_p)
+
+
+class OutputPlan(ctypes.Structure):
+    _fields_ = [("n_steps", ctypes.c_int64), ("t_max", c_dbl), ("save_interval", c_int),
+                ("dir", ctypes.c_char_p), ("progress", PROGRESS), ("user", ctypes.c_void_p)]
 
 
 class BubblesIn(ctypes.Structure):
@@ -130,6 +139,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "crp_destroy": (None, [vp]),
         "crp_void_fraction_noalloc_scratch": (ctypes.c_size_t, [c_int, c_int, c_int]),
         "crp_void_fraction_noalloc": (c_int, [P(Config), c_int, vp, vp, vp, vp, vp, vp]),
+        "crp_run": (c_int, [vp, P(OutputPlan), P(Config)]),
         "crp_batch_create": (c_int, [c_int, P(Config), P(BubblesIn), P(vp)]),
         "crp_batch_run": (c_int, [vp, P(c_int), c_int, P(c_int)]),
         "crp_batch_count": (c_int, [vp]),
@@ -228,6 +238,15 @@ class Sim:
         out = np.empty(self.dims.num_bubbles, dtype=np.float64)
         self._check(self.lib.crp_read_bubbles(self.h, BUBBLE_FIELDS[name], _ptr(out)))
         return out
+
+    def run(self, n_steps: int = 0, t_max: float = 0.0, save_interval: int = 0, directory: str | None = None,
+            progress=None):
+        """crp_run: step to the limits (config's n_step_max/t_step_max when both
+        are 0), writing rawdata every save_interval steps into directory."""
+        cb = PROGRESS(lambda step, t, user: progress(step, t)) if progress else PROGRESS()
+        plan = OutputPlan(n_steps, t_max, save_interval, directory.encode() if directory else None, cb, None)
+        cfg = self._keep[0]
+        self._check(self.lib.crp_run(self.h, ctypes.byref(plan), ctypes.byref(cfg) if cfg is not None else None))
 
     def write_rawdata(self, directory: str):
         self._check(self.lib.crp_write_rawdata(self.h, directory.encode()))

@@ -157,6 +157,7 @@ const Key kKeys[] = {
     K("ext.cloud_h", kDouble, ext_cloud_h),
     K("ext.n_b", kDouble, ext_n_b),
     K("ext.picard_tol", kDouble, ext_picard_tol),
+    K("ext.graphs", kBool, ext_graphs),
 };
 #undef K
 
@@ -292,6 +293,7 @@ crp_status crp_config_defaults(crp_config* cfg) {
   cfg->ext_p_inf = 0.1e6;
   cfg->ext_precision = CRP_PREC_FP64;
   cfg->ext_picard_cap = 1000;
+  cfg->ext_graphs = 1;
   cfg->ext_rp_step_cap = 1000000;
   cfg->ext_n_b = 1.0;
   return CRP_OK;

@@ -60,7 +60,7 @@ struct FdtdArgs {
   typename P::G fgA;       // f_g of the previous step (becomes f_gn)
   typename P::G fgB;       // f_gn of the previous step
   typename P::G fgC;       // f_gm of the previous step; receives the predicted f_g
-  double t_prev, t_cur;
+  const double* tdev;  // {t_prev, t_cur} of this step, in device memory
   int rho_const;           // first step: the mixture density is still rho_inf everywhere
   unsigned long long* residual;
 };
@@ -189,6 +189,7 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x;
   const int i = (blockIdx.x * kStripWarps + threadIdx.y) * kStripCells + lane;
+  const double t_prev = a.tdev[0], t_cur = a.tdev[1];
   const bool inwin = i <= X + 1;                                 // column inside the window [0, X+1]
   const bool cell = lane >= 1 && lane <= kStripCells && i <= X;  // updates cell (i, j)
   const bool face = lane <= kStripCells && i <= X;               // east face F(i) needed
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
   auto p0_of = [&](int r, double px_, double py_) -> double {
     if (!inwin) return 0.0;
     if (inner_col && r >= 1 && r <= Y && !(src_rows && r == g.source_row)) return px_ + py_;
-    return p0_edge(g, a.pnx, a.pny, i, r, a.t_prev);
+    return p0_edge(g, a.pnx, a.pny, i, r, t_prev);
   };
   auto rho_of = [&](double fa) -> double { return a.rho_const ? g.rho_inf : (1.0 - fa) * g.rho_inf; };
   auto predict = [&](long k, double fa) -> double {
@@ -256,7 +257,7 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
   double vyd = 0.0;
   if (cell) {
     double pre_d;
-    vyd = vy_face_value(g, j0 - 1, vyob, p0b, p0c, rhob, rhoc, xm, a.t_cur, pre_d);
+    vyd = vy_face_value(g, j0 - 1, vyob, p0b, p0c, rhob, rhoc, xm, t_cur, pre_d);
     if (j0 == 1) {
       a.vy_new.put(f.idx(i, 0), vyd);
       if (!g.pml_y0) a.vy_new.put(f.idx(i, -1), pre_d);
@@ -318,7 +319,7 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
       const double fw = __shfl_up_sync(full, fe, 1);
       if (cell) {
         double pre_u;
-        vyu = vy_face_value(g, j, vyo, p0c, p0n, rhoc, rhon, xm, a.t_cur, pre_u);
+        vyu = vy_face_value(g, j, vyo, p0c, p0n, rhoc, rhon, xm, t_cur, pre_u);
         const double s1x = g.cyl ? (-xu_w * fw + xu_e * fe) * g.rdx * rxp_c : (-fw + fe) * g.rdx;
         const double s1y = (-vyd + vyu) * g.rdy;
         const double h = void_rate_half(g, fgp, fac);
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
       a.px.put(k, qx);
       a.py.put(k, qy);
       double p0new = qx + qy;
-      if (src_rows && j == g.source_row) p0new = source_row_pressure(g, xm, a.t_cur);
+      if (src_rows && j == g.source_row) p0new = source_row_pressure(g, xm, t_cur);
       res = max(res, (unsigned long long)__double_as_longlong(fabs(p0c - p0new)));
       vyd = vyu;
     } else if (lane == 0 && i == 0) {
@@ -732,10 +733,12 @@ template <typename P>
 __global__ void __launch_bounds__(kRpThreads, kRpMinBlocks) bubble_rp(const __grid_constant__ GridParams g,
                                                         const __grid_constant__ BubbleParams bp, BubbleArrays b,
                                                         const typename P::S px, const typename P::S py,
-                                                        double t_cur, const int* __restrict__ order,
+                                                        const double* __restrict__ tdev,
+                                                        const int* __restrict__ order,
                                                         int* __restrict__ next, long long* __restrict__ substep_max,
                                                         int* __restrict__ err) {
   RpState s;
+  const double t_cur = tdev[1];
   int n = -1;
   bool drained = false;
   long long worst = 0;
@@ -858,9 +861,9 @@ struct CoupleArgs {
   const int* start;
   const int* idx;
   const double* contrib;
-  double t_cur;
   unsigned long long* residual;
   int i0, j0, i1, j1;  // cells to update (inclusive)
+  const int* dbox;     // if set: the box {i0, j0, i1, j1} in device memory instead
 };
 
 // calculate_void_fraction (memset, scatter, VoidFractionCylinderKernel fold:
@@ -870,10 +873,19 @@ template <typename P>
 __global__ void __launch_bounds__(256) couple_press(const __grid_constant__ GridParams g, const CoupleArgs<P> a) {
   const Frame& f = g.f;
   const int X = f.X, Y = f.Y;
-  const int i = a.i0 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = a.j0 + blockIdx.y * blockDim.y + threadIdx.y;
+  int i0 = a.i0, j0 = a.j0, i1 = a.i1, j1 = a.j1;
+  if (a.dbox) {
+    i0 = a.dbox[0];
+    j0 = a.dbox[1];
+    i1 = a.dbox[2];
+    j1 = a.dbox[3];
+    // Launched over the whole window: blocks past the box leave at once.
+    if (i0 + (int)(blockIdx.x * blockDim.x) > i1 || j0 + (int)(blockIdx.y * blockDim.y) > j1) return;
+  }
+  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = j0 + blockIdx.y * blockDim.y + threadIdx.y;
   double res = 0.0;
-  if (i <= a.i1 && j <= a.j1) {
+  if (i <= i1 && j <= j1) {
     double fgv;
     if (g.cyl && i <= 1)
       fgv = gather_fg(f, a.start, a.idx, a.contrib, 0, j) + gather_fg(f, a.start, a.idx, a.contrib, 1, j);
@@ -959,6 +971,184 @@ struct Profiler {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Device-resident step state.  The host path reads it after each residual
+// evaluation; the graph path (below) keeps the whole step's control on the
+// device and reads it back once per crp_step call.
+struct Scalars {
+  unsigned long long residual;  // max |dp0| as the bit pattern of a non-negative double
+  long long substep_max;        // largest RP sub-step count of one bubble
+  int err;                      // nonzero: a bubble hit the sub-step cap
+  int next;                     // work-queue head of the radius solve
+  int moved;                    // nonzero: a bubble changed cell bin this step
+  int bbox[4];                  // bins occupied this step, encoded (bubble_move)
+  double t[3];                  // t_prev, t (the step's time) and the Fast2Sum carry
+  // Graph path only: the Picard loop and the step's bookkeeping.
+  double res, prev, res_last;   // residual now, at the previous iteration, at the step's end
+  long long steps, picard_total, stalls;
+  int picard_last, picard_max;
+  int status;                   // crp_status of the first failure (0: none)
+  int loop;                     // Picard iterations of this step
+  int stale;                    // bins need a rebuild
+  int bnow[4], box[4];          // bubbles' cell box, coupling box
+  int supp[3][4];               // void-fraction supports of the last three steps
+  int entered, rebuilt;         // this step ran the Picard loop / rebuilt the bins
+  long long launches[4];        // kernels run by completed graph steps, per class
+};
+
+// Fast2Sum time step (src/bubble_CUDA.cu:208-212), written by the host path.
+__global__ void set_time(Scalars* s, double t_prev, double t, double carry) {
+  s->t[0] = t_prev;
+  s->t[1] = t;
+  s->t[2] = carry;
+}
+
+struct CtlParams {
+  double tol, P_inf, dt, stall;
+  int cap, nb, mixed, X, Y, cyl;
+  cudaGraphConditionalHandle h_step, h_picard, h_bins, h_loop;
+};
+
+__device__ __forceinline__ bool dbox_empty(const int* b) { return b[0] > b[2] || b[1] > b[3]; }
+__device__ __forceinline__ void dbox_union(int* o, const int* a, const int* b) {
+  if (dbox_empty(a)) {
+    for (int q = 0; q < 4; q++) o[q] = b[q];
+  } else if (dbox_empty(b)) {
+    for (int q = 0; q < 4; q++) o[q] = a[q];
+  } else {
+    o[0] = min(a[0], b[0]);
+    o[1] = min(a[1], b[1]);
+    o[2] = max(a[2], b[2]);
+    o[3] = max(a[3], b[3]);
+  }
+}
+__device__ __forceinline__ double residual_of(const Scalars* s, double P_inf) {
+  return __longlong_as_double((long long)s->residual) / P_inf;
+}
+
+// Start of a step: skip it after a failure; advance the time; clear the
+// per-step accumulators.
+__global__ void ctl_step_begin(Scalars* s, const CtlParams c) {
+  if (s->status) {
+    cudaGraphSetConditional(c.h_step, 0);
+    return;
+  }
+  const double tstep = s->t[1], tstepx = s->t[2];
+  const double s1 = tstep;
+  const double t = tstep + c.dt + tstepx;
+  const double s2 = t - s1;
+  s->t[0] = tstep;
+  s->t[1] = t;
+  s->t[2] = c.dt + tstepx - s2;
+  s->residual = 0ull;
+  s->moved = 0;
+  for (int q = 0; q < 4; q++) s->bbox[q] = 0;
+  s->loop = 0;
+  cudaGraphSetConditional(c.h_step, 1);
+}
+
+// After the FDTD pass and the bubble motion: the coupling box, the bin state,
+// and whether the Picard loop runs.
+__global__ void ctl_enter(Scalars* s, const CtlParams c, int box_off) {
+  const double r = residual_of(s, c.P_inf);
+  s->res = r;
+  s->prev = r;
+  s->stale |= s->moved;
+  int* bn = s->bnow;
+  const int* e = s->bbox;
+  if (c.nb > 0 && e[1] != 0) {
+    bn[0] = max(0, box_off - e[0]);
+    bn[1] = max(0, box_off - e[2]);
+    bn[2] = min(c.X + 1, e[1] - box_off + 1);
+    bn[3] = min(c.Y + 1, e[3] - box_off + 1);
+    if (!dbox_empty(bn) && c.cyl && bn[0] <= 1) {
+      bn[0] = 0;
+      bn[2] = max(bn[2], 1);
+    }
+  } else {
+    bn[0] = bn[1] = 1;
+    bn[2] = bn[3] = 0;
+  }
+  int u[4], w[4];
+  dbox_union(u, bn, s->supp[0]);
+  dbox_union(w, s->supp[1], s->supp[2]);
+  dbox_union(s->box, u, w);
+  bool enter = c.nb > 0 && r > c.tol;
+  if (enter && c.cap <= 0) {
+    s->status = CRP_ERR_PICARD;
+    enter = false;
+  }
+  s->entered = enter;
+  s->rebuilt = 0;
+  s->residual = 0ull;
+  s->next = 0;
+  cudaGraphSetConditional(c.h_picard, enter ? 1u : 0u);
+}
+
+__global__ void ctl_bins(Scalars* s, const CtlParams c) {
+  cudaGraphSetConditional(c.h_bins, s->stale ? 1u : 0u);
+  s->rebuilt = s->stale;
+  s->stale = 0;
+}
+
+// End of a Picard iteration: the loop continues while the residual is above
+// the threshold, up to the cap; the mixed path's stagnation rule as in the
+// host path.
+__global__ void ctl_iter(Scalars* s, const CtlParams c) {
+  const int loop = ++s->loop;
+  unsigned go = 0;
+  if (s->err) {
+    s->status = CRP_ERR_RP_STEPS;
+  } else {
+    const double r = residual_of(s, c.P_inf);
+    s->res = r;
+    if (c.mixed && loop >= 3 && r > c.tol && r > 0.5 * s->prev && r < c.stall) {
+      s->stalls++;
+    } else if (r > c.tol) {
+      if (loop >= c.cap)
+        s->status = CRP_ERR_PICARD;
+      else
+        go = 1;
+    }
+    s->prev = r;
+  }
+  s->residual = 0ull;
+  s->next = 0;
+  cudaGraphSetConditional(c.h_loop, go);
+}
+
+// End of a step: non-finite check, void-fraction support history, counters.
+__global__ void ctl_end(Scalars* s, const CtlParams c) {
+  if (s->status) return;
+  if (isnan(s->res)) {
+    s->status = CRP_ERR_NONFINITE;
+    return;
+  }
+  int snow[4];
+  if (s->loop > 0) {
+    for (int q = 0; q < 4; q++) snow[q] = s->bnow[q];
+  } else {
+    int u[4];
+    dbox_union(u, s->supp[0], s->supp[1]);
+    dbox_union(snow, u, s->supp[2]);
+  }
+  for (int q = 0; q < 4; q++) {
+    s->supp[2][q] = s->supp[1][q];
+    s->supp[1][q] = s->supp[0][q];
+    s->supp[0][q] = snow[q];
+  }
+  // Kernels of the step, per class (fdtd, rp, couple, other), as the host path counts them.
+  s->launches[0] += 1;
+  s->launches[1] += s->loop;
+  s->launches[2] += s->loop;
+  s->launches[3] += 4 + (c.nb > 0) + (s->entered ? 4 + s->loop + (s->rebuilt ? 6 : 0) : 0);
+  s->steps++;
+  s->picard_last = s->loop;
+  s->picard_total += s->loop;
+  s->picard_max = max(s->picard_max, s->loop);
+  s->res_last = s->res;
+}
+
 struct Sim {
   crp_config cfg{};
   Profiler prof;
@@ -988,14 +1178,6 @@ struct Sim {
   BubbleArrays bub{};
   Bins bins{};
   // Device scalars written by the kernels, read back once per pressure evaluation.
-  struct Scalars {
-    unsigned long long residual;  // max |dp0| as the bit pattern of a non-negative double
-    long long substep_max;        // largest RP sub-step count of one bubble
-    int err;                      // nonzero: a bubble hit the sub-step cap
-    int next;                     // work-queue head of the radius solve
-    int moved;                    // nonzero: a bubble changed cell bin this step
-    int bbox[4];                  // bins occupied this step, encoded (bubble_move)
-  };
   Scalars* d_scalars = nullptr;
   unsigned long long* d_residual = nullptr;
   long long* d_substep_max = nullptr;
@@ -1015,6 +1197,14 @@ struct Sim {
   Box supp[3];
   Box couple_box;
   bool bins_stale = false;  // a bubble changed cell since the bins were built
+  // Graph path: one executable graph per buffer phase (velocity/pressure
+  // ping-pong x f_g ring = 6), built on first use by stream capture.
+  cudaStream_t cap_stream = nullptr;
+  cudaGraph_t step_graph[6] = {};
+  cudaGraphExec_t step_exec[6] = {};
+  bool capturing = false;    // launches go into a graph (device-decided coupling box)
+  bool graphs_on = true;     // ext: off runs every step from the host
+  Scalars* h_push = nullptr;  // pinned staging of the host state for the graph path
   bool debug_picard = std::getenv("CRP_DEBUG_PICARD") != nullptr;  // residual of every Picard iteration to stderr
   struct Lpt {
     int* hist;    // kLptBuckets
@@ -1114,6 +1304,7 @@ struct Sim {
       return fail(CRP_ERR_INVALID, "ext.precision must be fp64 or mixed");
     mixed = cfg.ext_precision == CRP_PREC_MIXED;
     picard_tol = cfg.ext_picard_tol > 0.0 ? cfg.ext_picard_tol : (mixed ? 1.0e-5 : (double)1.0e-7f);
+    graphs_on = cfg.ext_graphs != 0;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CRP_ERR_NO_DEVICE, "no CUDA device");
     if (user_stream) {
@@ -1334,6 +1525,7 @@ struct Sim {
     tstep = tstep + gp.dt + tstepx;
     double s2 = tstep - s1;
     tstepx = gp.dt + tstepx - s2;
+    CRP_CUDA(launch(kClassOther, [&] { set_time<<<1, 1, 0, stream>>>(d_scalars, t_prev, tstep, tstepx); }));
 
     const int nv = cur_v ^ 1, np = cur_p ^ 1;
     // Ring rotation of store_variables: the predicted f_g goes to the f_gm buffer.
@@ -1442,6 +1634,266 @@ struct Sim {
     return CRP_OK;
   }
 
+  // ---- Graph path --------------------------------------------------------
+  // One mixture step as a CUDA graph whose control flow runs on the device:
+  //   ctl_step_begin -> IF(step ok) {
+  //     fdtd_strip, vghost, bubble_move, ctl_enter -> IF(Picard needed) {
+  //       ctl_bins -> IF(bins stale) { counting sort } -> solve order ->
+  //       WHILE(residual > threshold) { bubble_rp, couple_press, ctl_iter } }
+  //     -> ctl_end }
+  // so a crp_step call of n steps is n graph launches and one read-back,
+  // instead of two host round trips per step.  The arithmetic is the host
+  // path's, kernel for kernel.
+  int phase() const { return cur_v * 3 + fg_a; }
+
+  void rotate_once() {
+    cur_v ^= 1;
+    cur_p ^= 1;
+    const int a = fg_a, b = fg_b, c = fg_c;
+    fg_a = c;
+    fg_b = a;
+    fg_c = b;
+  }
+
+  // Appends what fn enqueues on `stream` to graph g after the nodes deps and
+  // returns the capture's last nodes in sinks.
+  template <typename F>
+  cudaError_t capture(cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, std::vector<cudaGraphNode_t>& sinks,
+                      F&& fn) {
+    cudaError_t e = cudaStreamBeginCaptureToGraph(cap_stream, g, deps.empty() ? nullptr : deps.data(), nullptr,
+                                                  deps.size(), cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    const cudaStream_t saved = stream;
+    int64_t saved_launches[4];
+    std::memcpy(saved_launches, launches, sizeof(launches));
+    stream = cap_stream;
+    capturing = true;
+    const cudaError_t fe = fn();
+    capturing = false;
+    stream = saved;
+    std::memcpy(launches, saved_launches, sizeof(launches));
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t* d = nullptr;
+    size_t nd = 0;
+    const cudaError_t ie = cudaStreamGetCaptureInfo(cap_stream, &cs, nullptr, nullptr, &d, &nd);
+    if (ie == cudaSuccess) sinks.assign(d, d + nd);
+    cudaGraph_t out = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(cap_stream, &out);
+    return fe != cudaSuccess ? fe : ie != cudaSuccess ? ie : ee;
+  }
+
+  static cudaError_t add_cond(cudaGraph_t g, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                              cudaGraphNode_t* node, cudaGraph_t* body) {
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = type;
+    p.conditional.size = 1;
+    const cudaError_t e = cudaGraphAddNode(node, g, nullptr, 0, &p);
+    if (e == cudaSuccess) *body = p.conditional.phGraph_out[0];
+    return e;
+  }
+
+  static cudaError_t link(cudaGraph_t g, const std::vector<cudaGraphNode_t>& from, cudaGraphNode_t to) {
+    for (cudaGraphNode_t f : from) {
+      const cudaError_t e = cudaGraphAddDependencies(g, &f, &to, 1);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+
+  cudaError_t build_step_graph(int ph) {
+    if (!cap_stream) {
+      cudaError_t e = cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking);
+      if (e != cudaSuccess) return e;
+    }
+    cudaGraph_t top = nullptr;
+    cudaError_t e = cudaGraphCreate(&top, 0);
+    if (e != cudaSuccess) return e;
+    step_graph[ph] = top;
+    CtlParams c{};
+    c.tol = picard_tol;
+    c.P_inf = gp.P_inf;
+    c.dt = gp.dt;
+    c.stall = CRP_MIXED_STALL_RESIDUAL;
+    c.cap = cfg.ext_picard_cap;
+    c.nb = hs.nb;
+    c.mixed = mixed ? 1 : 0;
+    c.X = gp.f.X;
+    c.Y = gp.f.Y;
+    c.cyl = gp.cyl;
+    cudaGraphNode_t n_step, n_picard, n_bins, n_loop;
+    cudaGraph_t body1, body2, body3, body4;
+    std::vector<cudaGraphNode_t> sinks;
+#define CRP_G(x)                       \
+  do {                                 \
+    cudaError_t ge_ = (x);             \
+    if (ge_ != cudaSuccess) return ge_; \
+  } while (0)
+    CRP_G(cudaGraphConditionalHandleCreate(&c.h_step, top, 0, cudaGraphCondAssignDefault));
+    CRP_G(add_cond(top, c.h_step, cudaGraphCondTypeIf, &n_step, &body1));
+    CRP_G(cudaGraphConditionalHandleCreate(&c.h_picard, body1, 0, cudaGraphCondAssignDefault));
+    CRP_G(add_cond(body1, c.h_picard, cudaGraphCondTypeIf, &n_picard, &body2));
+    CRP_G(cudaGraphConditionalHandleCreate(&c.h_bins, body2, 0, cudaGraphCondAssignDefault));
+    CRP_G(cudaGraphConditionalHandleCreate(&c.h_loop, body2, 1, cudaGraphCondAssignDefault));
+    CRP_G(add_cond(body2, c.h_bins, cudaGraphCondTypeIf, &n_bins, &body3));
+    CRP_G(add_cond(body2, c.h_loop, cudaGraphCondTypeWhile, &n_loop, &body4));
+    Scalars* ds = d_scalars;
+    // Top level.
+    CRP_G(capture(top, {}, sinks, [&] {
+      return launch(kClassOther, [&] { ctl_step_begin<<<1, 1, 0, stream>>>(ds, c); });
+    }));
+    CRP_G(link(top, sinks, n_step));
+    // The step body, with the buffers of this phase.
+    const int sv = cur_v, sp = cur_p, sa = fg_a, sb = fg_b, sc = fg_c;
+    cudaError_t be = capture(body1, {}, sinks, [&]() -> cudaError_t {
+      const int nv = cur_v ^ 1, np = cur_p ^ 1;
+      cudaError_t x = mixed ? launch_fdtd<PrecMixed>(nv, np, fg_a, fg_b, fg_c)
+                            : launch_fdtd<PrecFP64>(nv, np, fg_a, fg_b, fg_c);
+      if (x != cudaSuccess) return x;
+      rotate_once();
+      if (hs.nb > 0) {
+        x = mixed ? launch_move<PrecMixed>() : launch_move<PrecFP64>();
+        if (x != cudaSuccess) return x;
+      }
+      return launch(kClassOther, [&] { ctl_enter<<<1, 1, 0, stream>>>(ds, c, kBoxOff); });
+    });
+    if (be == cudaSuccess) be = link(body1, sinks, n_picard);
+    if (be == cudaSuccess)
+      be = capture(body1, {n_picard}, sinks,
+                   [&] { return launch(kClassOther, [&] { ctl_end<<<1, 1, 0, stream>>>(ds, c); }); });
+    // Picard body: bins, order, loop (buffers as after the rotation).
+    if (be == cudaSuccess)
+      be = capture(body2, {}, sinks,
+                   [&] { return launch(kClassOther, [&] { ctl_bins<<<1, 1, 0, stream>>>(ds, c); }); });
+    if (be == cudaSuccess) be = link(body2, sinks, n_bins);
+    if (be == cudaSuccess) be = capture(body2, {n_bins}, sinks, [&] { return build_order(); });
+    if (be == cudaSuccess) be = link(body2, sinks, n_loop);
+    if (be == cudaSuccess) be = capture(body3, {}, sinks, [&] { return build_bins(); });
+    if (be == cudaSuccess)
+      be = capture(body4, {}, sinks, [&]() -> cudaError_t {
+        cudaError_t x = mixed ? launch_rp<PrecMixed>() : launch_rp<PrecFP64>();
+        if (x != cudaSuccess) return x;
+        x = launch_couple(true);
+        if (x != cudaSuccess) return x;
+        return launch(kClassOther, [&] { ctl_iter<<<1, 1, 0, stream>>>(ds, c); });
+      });
+    cur_v = sv;
+    cur_p = sp;
+    fg_a = sa;
+    fg_b = sb;
+    fg_c = sc;
+    CRP_G(be);
+    CRP_G(cudaGraphInstantiate(&step_exec[ph], top, 0));
+#undef CRP_G
+    return cudaSuccess;
+  }
+
+  // Host state into the device block before graph steps.
+  cudaError_t push_ctl() {
+    Scalars& h = *h_push;
+    std::memset(&h, 0, sizeof(Scalars));
+    h.substep_max = h_scalars->substep_max;
+    h.t[0] = t_prev;
+    h.t[1] = tstep;
+    h.t[2] = tstepx;
+    h.steps = stats.steps;
+    h.picard_total = stats.picard_total;
+    h.stalls = stats.picard_stalls;
+    h.picard_last = stats.picard_last;
+    h.picard_max = stats.picard_max;
+    h.res_last = stats.residual_last;
+    h.stale = bins_stale ? 1 : 0;
+    for (int q = 0; q < 3; q++) {
+      h.supp[q][0] = supp[q].i0;
+      h.supp[q][1] = supp[q].j0;
+      h.supp[q][2] = supp[q].i1;
+      h.supp[q][3] = supp[q].j1;
+    }
+    return cudaMemcpyAsync(d_scalars, h_push, sizeof(Scalars), cudaMemcpyHostToDevice, stream);
+  }
+
+  // n steps through the graph path; one read-back at the end.
+  crp_status step_graphs(int n) {
+    if (!h_push) CRP_CUDA(cudaMallocHost(&h_push, sizeof(Scalars)));
+    for (int k = 0; k < 6; k++)
+      if (!step_exec[k]) {
+        // Build all phases up front so that the launches below do not interleave with captures.
+        const int sv = cur_v, sp = cur_p, sa = fg_a, sb = fg_b, sc = fg_c;
+        for (int r = 0; r < 6; r++) {
+          const int ph = phase();
+          if (!step_exec[ph]) {
+            const cudaError_t e = build_step_graph(ph);
+            if (e != cudaSuccess) {
+              graphs_on = false;
+              cur_v = sv, cur_p = sp, fg_a = sa, fg_b = sb, fg_c = sc;
+              return CRP_ERR_UNSUPPORTED;
+            }
+          }
+          rotate_once();
+        }
+        cur_v = sv, cur_p = sp, fg_a = sa, fg_b = sb, fg_c = sc;
+        break;
+      }
+    const int64_t steps0 = stats.steps;
+    const int sv = cur_v, sp = cur_p, sa = fg_a, sb = fg_b, sc = fg_c;
+    CRP_CUDA(push_ctl());
+    for (int k = 0; k < n; k++) {
+      CRP_CUDA(cudaGraphLaunch(step_exec[phase()], stream));
+      rotate_once();
+    }
+    CRP_CUDA(cudaMemcpyAsync(h_scalars, d_scalars, sizeof(Scalars), cudaMemcpyDeviceToHost, stream));
+    CRP_CUDA(cudaStreamSynchronize(stream));
+    const Scalars& d = *h_scalars;
+    t_prev = d.t[0];
+    tstep = d.t[1];
+    tstepx = d.t[2];
+    const int64_t done = d.steps - steps0;
+    stats.steps = d.steps;
+    stats.time = tstep;
+    stats.picard_total = d.picard_total;
+    stats.picard_stalls = d.stalls;
+    stats.picard_last = d.picard_last;
+    stats.picard_max = d.picard_max;
+    stats.residual_last = d.res_last;
+    stats.rp_substeps_max = d.substep_max;
+    bins_stale = d.stale != 0;
+    for (int q = 0; q < 3; q++) supp[q] = Box{d.supp[q][0], d.supp[q][1], d.supp[q][2], d.supp[q][3]};
+    for (int q = 0; q < 4; q++) launches[q] += d.launches[q];
+    fill_launch_stats();
+    if (d.status) {
+      // The failed step ran up to its failure (its buffers rotated); later launches did nothing.
+      cur_v = sv, cur_p = sp, fg_a = sa, fg_b = sb, fg_c = sc;
+      for (int64_t r = 0; r < done + 1; r++) rotate_once();
+      const crp_status st = (crp_status)d.status;
+      return fail(st, st == CRP_ERR_PICARD      ? "Picard iteration cap reached"
+                      : st == CRP_ERR_RP_STEPS ? "Rayleigh-Plesset sub-step cap reached"
+                                               : "non-finite pressure");
+    }
+    return CRP_OK;
+  }
+
+  // crp_step: the first step (initial mixture density), profiled steps and
+  // simulations without bubbles run from the host; the rest as graphs.
+  crp_status step_n(int n) {
+    int k = 0;
+    while (k < n && (stats.steps == 0 || prof.on || !graphs_on || hs.nb == 0 || debug_picard)) {
+      const crp_status st = step_once();
+      if (st != CRP_OK) return st;
+      k++;
+    }
+    if (k >= n) return CRP_OK;
+    const crp_status st = step_graphs(n - k);
+    if (st == CRP_ERR_UNSUPPORTED && !graphs_on) {
+      for (; k < n; k++) {
+        const crp_status s2 = step_once();
+        if (s2 != CRP_OK) return s2;
+      }
+      return CRP_OK;
+    }
+    return st;
+  }
+
   crp_status read_field(crp_field which, double* host) {
     const int X = gp.f.X, Y = gp.f.Y;
     const int kv = mixed ? 1 : 0, kg = mixed ? 2 : 0;
@@ -1490,8 +1942,7 @@ struct Sim {
     fa.fgA = view<G>(fg[a]);
     fa.fgB = view<G>(fg[b]);
     fa.fgC = view<G>(fg[c]);
-    fa.t_prev = t_prev;
-    fa.t_cur = tstep;
+    fa.tdev = d_scalars->t;
     fa.rho_const = stats.steps == 0 ? 1 : 0;
     fa.residual = d_residual;
     const int strips = (gp.f.X + kStripCells - 1) / kStripCells;
@@ -1518,10 +1969,9 @@ struct Sim {
   cudaError_t launch_rp() {
     using S = typename P::S;
     const S pxc = view<S>(px[cur_p]), pyc = view<S>(py[cur_p]);
-    const double tc = tstep;
     return launch(kClassRp, [&] {
-      bubble_rp<P><<<rp_grid, kRpThreads, 0, stream>>>(gp, bp, bub, pxc, pyc, tc, lpt.order, d_next, d_substep_max,
-                                                        d_err);
+      bubble_rp<P><<<rp_grid, kRpThreads, 0, stream>>>(gp, bp, bub, pxc, pyc, d_scalars->t, lpt.order, d_next,
+                                                        d_substep_max, d_err);
     });
   }
 
@@ -1580,6 +2030,12 @@ struct Sim {
   }
 
   ~Sim() {
+    for (int k = 0; k < 6; k++) {
+      if (step_exec[k]) cudaGraphExecDestroy(step_exec[k]);
+      if (step_graph[k]) cudaGraphDestroy(step_graph[k]);
+    }
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+    if (h_push) cudaFreeHost(h_push);
     if (pool) cudaFree(pool);
     if (h_scalars) cudaFreeHost(h_scalars);
     if (own_stream && stream) cudaStreamDestroy(stream);
@@ -1657,9 +2113,18 @@ cudaError_t Sim::launch_couple_t(bool pressure) {
   ca.start = bins.start;
   ca.idx = bins.idx;
   ca.contrib = bub.contrib;
-  ca.t_cur = tstep;
+  ca.dbox = nullptr;
   ca.residual = d_residual;
   dim3 blk(32, 8);
+  if (pressure && capturing) {
+    // Graph step: the box is decided on the device each step.
+    ca.i0 = ca.j0 = 0;
+    ca.i1 = gp.f.X + 1;
+    ca.j1 = gp.f.Y + 1;
+    ca.dbox = d_scalars->box;
+    dim3 grd((gp.f.X + 2 + 31) / 32, (gp.f.Y + 2 + 7) / 8);
+    return launch(kClassCouple, [&] { couple_press<P><<<grd, blk, 0, stream>>>(gp, ca); });
+  }
   if (pressure) {
     const Box& b = couple_box;
     if (box_empty(b)) return cudaSuccess;
@@ -1704,11 +2169,7 @@ crp_status crp_create(const crp_config* cfg, const crp_bubbles_in* bubbles, void
 
 crp_status crp_step(crp_sim* h, int32_t n) {
   if (!h || n < 0) return CRP_ERR_INVALID;
-  for (int k = 0; k < n; k++) {
-    crp_status st = h->s.step_once();
-    if (st != CRP_OK) return st;
-  }
-  return CRP_OK;
+  return h->s.step_n(n);
 }
 
 crp_status crp_get_dims(const crp_sim* h, crp_dims* d) {

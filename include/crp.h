@@ -115,6 +115,8 @@ typedef struct crp_config {
   double ext_n_b;            /* weight n_B of each seeded bubble, default 1 */
   double ext_picard_tol;     /* Picard residual threshold, max|dp0|/P_inf; 0 selects the reference's
                                 1e-7 (FP64) or 1e-5 (mixed: FP32 storage has a higher noise floor) */
+  int32_t ext_graphs;        /* 1 (default): steps after the first run as CUDA graphs with the Picard
+                                loop decided on the device; 0: every step driven from the host */
 } crp_config;
 
 /* Dense host layouts of the readable fields, in the reference's index order:
@@ -261,6 +263,22 @@ void* crp_stream(crp_sim* sim);
 size_t crp_void_fraction_noalloc_scratch(int32_t grid_x, int32_t grid_y, int32_t n);
 crp_status crp_void_fraction_noalloc(const crp_config* cfg, int32_t n, const double* x, const double* y,
                                      const double* r, const double* n_b, double* f_g, void* stream);
+
+/* Main loop with saves (src/bubble_CUDA.cu:203-438): step while
+ * (n_steps != 0 && steps < n_steps) || (t_max != 0 && time < t_max); after
+ * every save_interval-th step write rawdata to dir (if not NULL) and call
+ * progress (if not NULL).  With n_steps = t_max = 0 the limits come from cfg
+ * (sim_n_step_max, sim_t_step_max); cfg may be NULL otherwise.  Steps already
+ * taken count towards the limits. */
+typedef struct crp_output_plan {
+  int64_t n_steps;
+  double t_max;
+  int32_t save_interval;
+  const char* dir;
+  void (*progress)(int64_t step, double time, void* user);
+  void* user;
+} crp_output_plan;
+crp_status crp_run(crp_sim* sim, const crp_output_plan* plan, const crp_config* cfg);
 
 /* Batched sweep: count independent simulations (cfgs[k], bubbles[k] or NULL /
  * n = 0 for the configuration's own seeding), each with its own stream, run

@@ -116,3 +116,45 @@ def test_void_fraction_conservation_gpu():
         lhs = fg.sum() * d.dx * d.dy
         rhs = (4.0 / 3.0 * np.pi * nb * R ** 3).sum()
         assert abs(lhs - rhs) <= 1e-12 * rhs
+
+
+def _snapshot(sim):
+    st = sim.stats()
+    arrays = [sim.field(k) for k in ("p0", "vx", "vy", "f_g")]
+    if sim.dims.num_bubbles:
+        arrays += [sim.bubbles(k) for k in ("R_t", "PG_p", "x")]
+    return arrays, (st.steps, st.picard_total, st.picard_max, st.picard_stalls, st.rp_substeps_max, st.time)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("name", ["focus_p", "strong_drive", "plane_p_all_cells", "ext_source_row_ramp"])
+def test_graph_steps_match_host_steps(name, prec):
+    """Steps run as CUDA graphs with device-side Picard control give the host
+    path's results bit for bit, across several crp_step calls."""
+    over, steps = CASES[name]
+    snaps = []
+    for graphs in (0, 1):
+        cfg = B.small_config(ext_precision=prec, ext_graphs=graphs, **over)
+        with crp.Sim(cfg) as gpu:
+            gpu.step(1)
+            gpu.step(steps // 3)
+            gpu.step(steps - 1 - steps // 3)
+            snaps.append(_snapshot(gpu))
+    (a_arr, a_st), (b_arr, b_st) = snaps
+    assert a_st == b_st
+    for a, b in zip(a_arr, b_arr):
+        assert np.array_equal(a, b)
+
+
+def test_graph_steps_report_the_picard_cap_like_host_steps():
+    over, steps = CASES["strong_drive"]
+    seen = []
+    for graphs in (0, 1):
+        cfg = B.small_config(ext_graphs=graphs, ext_picard_cap=2, **over)
+        with crp.Sim(cfg) as gpu:
+            with pytest.raises(crp.CrpError) as e:
+                gpu.step(steps)
+            seen.append((e.value.status, gpu.stats().steps))
+            gpu_p0 = gpu.field("p0")
+            assert np.all(np.isfinite(gpu_p0))
+    assert seen[0] == seen[1] and seen[0][0] == 6

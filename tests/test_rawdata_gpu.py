@@ -97,3 +97,24 @@ def test_bubbles_program(tmp_path):
     assert (out / "runtime.txt").read_text().startswith("Finished in ")
     lo, hi = [float(v) for v in (out / "p0_minmax.txt").read_text().split()]
     assert lo <= hi
+
+
+def test_run_writes_what_a_step_loop_writes(tmp_path):
+    """crp_run with a save interval writes the files a manual step loop writes."""
+    cfg, steps = _mrg.case_config("tiny")
+    a, b = tmp_path / "run", tmp_path / "loop"
+    a.mkdir()
+    b.mkdir()
+    seen = []
+    with crp.Sim(cfg) as sim:
+        sim.run(n_steps=steps, save_interval=20, directory=str(a), progress=lambda s, t: seen.append(s))
+        assert sim.stats().steps == steps
+    with crp.Sim(cfg) as sim:
+        for k in range(steps // 20):
+            sim.step(20)
+            sim.write_rawdata(str(b))
+    assert seen == [20, 40, 60][: steps // 20]
+    names = sorted(os.listdir(b))
+    assert names and sorted(os.listdir(a)) == names
+    for name in names:
+        assert open(a / name).read() == open(b / name).read(), name
