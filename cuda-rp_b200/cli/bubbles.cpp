@@ -189,6 +189,13 @@ int main(int argc, char** argv) {
   double fg_min = 1e10, fg_max = -1e10, p0_min = 1e10, p0_max = -1e10;
   crp_minmax(sim, &fg_min, &fg_max, &p0_min, &p0_max);
   double v;
+  if (cfg.dbg_T) {
+    double T_min = 1e10, T_max = -1e10;
+    crp_minmax_T(sim, &T_min, &T_max);
+    if (lookup_key(in_file, "debug.T_min", &v)) T_min = v;
+    if (lookup_key(in_file, "debug.T_max", &v)) T_max = v;
+    write_minmax(target_dir + "T_minmax.txt", T_min, T_max);
+  }
   if (cfg.dbg_p) {
     if (lookup_key(in_file, "debug.p_max", &v)) p0_max = v;
     write_minmax(target_dir + "p0_minmax.txt", p0_min, p0_max);

@@ -77,7 +77,7 @@ class BubblesIn(ctypes.Structure):
                 ("n_b", ctypes.c_void_p)]
 
 
-FIELDS = {"p0": 0, "px": 1, "py": 2, "pnx": 3, "pny": 4, "vx": 5, "vy": 6, "f_g": 7, "f_gn": 8,
+FIELDS = {"p0": 0, "px": 1, "py": 2, "pnx": 3, "pny": 4, "vx": 5, "vy": 6, "f_g": 7, "f_gn": 8, "T": 11,
           "f_gm": 9, "rho_m": 10}
 BUBBLE_FIELDS = {"x": 0, "y": 1, "R_t": 2, "R_p": 3, "R_n": 4, "d1_R_p": 5, "PG_p": 6, "PL_p": 7,
                  "PL_n": 8, "PL_m": 9, "dt": 10, "re": 11, "Q_B": 12, "n_B": 13, "R0": 14, "v_x": 15,

@@ -293,7 +293,7 @@ crp_status crp_config_defaults(crp_config* cfg) {
   cfg->ext_p_inf = 0.1e6;
   cfg->ext_precision = CRP_PREC_FP64;
   cfg->ext_picard_cap = 1000;
-  cfg->ext_graphs = 1;
+  cfg->ext_graphs = 0;
   cfg->ext_rp_step_cap = 1000000;
   cfg->ext_n_b = 1.0;
   return CRP_OK;

@@ -45,7 +45,7 @@ int64_t sim_step_count(const crp_sim* h);
 // Running min/max of the values written to rawdata files (the globals of
 // src/bubbles.cpp:11-13 that save_ascii updates), per simulation.
 struct MinMax {
-  double fg_min = 1e10, fg_max = -1e10, p0_min = 1e10, p0_max = -1e10;
+  double fg_min = 1e10, fg_max = -1e10, p0_min = 1e10, p0_max = -1e10, T_min = 1e10, T_max = -1e10;
 };
 MinMax& sim_minmax(crp_sim* h);
 

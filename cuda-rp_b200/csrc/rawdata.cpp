@@ -1,12 +1,11 @@
 // Plain-text rawdata writer: the file names, column order, number formatting
 // and row separators of save_ascii (src/output_styles.cpp:139-341).
 //
-//   fg_step_%05d.txt, p0_step_%05d.txt, vx_step_%05d.txt, vy_step_%05d.txt:
+//   fg_step_%05d.txt, T_step_%05d.txt, p0_step_%05d.txt, vx_step_%05d.txt, vy_step_%05d.txt:
 //     one line "x<TAB>y<TAB>value" per point for j = 0..Y and i = 0..X (or
 //     i = -X..X mirrored when axisymmetric), a blank line after each row j;
 //   bubble_radii_%05d.txt, bubble_PG_%05d.txt: "x<TAB>y<TAB>R" / "x<TAB>y<TAB>PG".
 // Numbers use the default ostream conversion (%g, 6 significant digits).
-// T_step files are not written: the temperature field is outside this path.
 #include <sys/stat.h>
 
 #include <cerrno>
@@ -92,6 +91,12 @@ crp_status write_rawdata(crp_sim* sim, const char* dir_c) {
     buf.resize((size_t)d.i2m * d.j2m);
     if ((st = sim_read_field(sim, CRP_FIELD_FG, buf.data())) != CRP_OK) return st;
     st = write_grid(step_name(dir, "fg_step_", step), c, d.dx, d.dy, buf, 0, 0, d.i2m, &mm.fg_min, &mm.fg_max);
+    if (st != CRP_OK) return st;
+  }
+  if (c.dbg_T) {
+    buf.resize((size_t)d.i2m * d.j2m);
+    if ((st = sim_read_field(sim, CRP_FIELD_T, buf.data())) != CRP_OK) return st;
+    st = write_grid(step_name(dir, "T_step_", step), c, d.dx, d.dy, buf, 0, 0, d.i2m, &mm.T_min, &mm.T_max);
     if (st != CRP_OK) return st;
   }
   if (c.dbg_p) {

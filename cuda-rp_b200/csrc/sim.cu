@@ -168,13 +168,13 @@ __device__ __noinline__ double source_row_pressure(const GridParams& g, double x
 // shuffle, the row below stays in registers, so every array element is read
 // once per step (the two edge columns of a strip and the row under a chunk
 // once more, from L2), with 256-byte coalesced rows per warp load.  Rows are
-// staged through a per-warp ring in shared memory by asynchronous copies
-// issued kStripStages - 2 rows ahead, so each warp keeps several rows of all
-// seven input arrays in flight instead of one dependent round trip per row.
+// staged through a per-warp ring of kStripStages rows in shared memory by
+// asynchronous copies issued kStripStages - 2 rows ahead, so each warp keeps
+// the next rows of all seven input arrays in flight while it computes.
 constexpr int kStripCells = 30;
 constexpr int kStripWarps = 4;
-constexpr int kStripRows = 8;    // rows per chunk; the grid is a few waves of 148 SMs at 1024 x 2048
-constexpr int kStripStages = 6;  // ring slots (rows) per warp
+constexpr int kStripRows = 6;    // rows per chunk (measured best of 4-16 at 1024 x 2048)
+constexpr int kStripStages = 4;  // ring slots (rows) per warp; a smaller ring leaves more L1 (measured)
 constexpr int kStripFields = 7;  // pnx, pny, fgA, vx_old, vy_old, fgB, fgC
 
 template <typename P>
@@ -347,7 +347,10 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
     issue(j + kStripStages);  // reuses the slot of row j
   }
   if (j1 == Y && own) predict(f.idx(i, Y + 1), fac);
-  block_max_to(__longlong_as_double((long long)res), a.residual);
+  // Warp maximum, one atomic per warp with a nonzero residual (no block
+  // barrier: the warps of a block finish their strips at different times).
+  for (int o = 16; o > 0; o >>= 1) res = max(res, __shfl_xor_sync(0xffffffffu, res, o));
+  if (lane == 0 && res) atomicMax(a.residual, res);
 }
 
 // Velocity ghost cells (VelocityBoundaryKernel, inc/bubble_CUDA_kernel.cuh:701-811,
@@ -932,6 +935,122 @@ __global__ void materialize_p0(const __grid_constant__ GridParams g, const S px,
 // Kernel classes for launch counting and optional per-class device timing.
 enum KernelClass { kClassFdtd = 0, kClassRp = 1, kClassCouple = 2, kClassOther = 3 };
 
+// ---------------------------------------------------------------------------
+// Temperature branch (calculate_temperature, inc/bubble_CUDA_kernel.cuh:1347-1376):
+// bubble heat scattered to cells, mixture conductivity, energy fluxes, the
+// temperature update with acoustic absorption, and the non-PML mirrors.  Run
+// after the Picard loop when the temperature is requested (debug.T); nothing
+// on the pressure/bubble path reads it.
+
+// Water properties (:176-193); the float literals are the reference's.
+__host__ __device__ __forceinline__ double conductivity_water(double T) {
+  return 0.76760 + ((double)7.5390e-3f * T) - (double)9.8250e-6f * (T * T);
+}
+__host__ __device__ __forceinline__ double heat_capacity_water(double T) {
+  const double H2O = (double)18.0e-3f;
+  return (917.5 - (double)10.1016f * T + (double)0.0454134f * (T * T) - 9.07517e-5 * (T * T * T) +
+          (double)6.80700e-8f * (T * T * T * T)) /
+         H2O;
+}
+
+// Heat of each bubble to the four cells of its stencil (BubbleHeatKernel,
+// :972-1007): n_B Q_B / (dx dy [x]) delta_x delta_y, laid out like the
+// void-fraction contributions so the same bin gather sums them.
+__global__ void heat_contrib(const __grid_constant__ GridParams g, const __grid_constant__ BubbleParams bp,
+                             BubbleArrays b, double* __restrict__ hc) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= b.n) return;
+  const double x = b.x[n], y = b.y[n];
+  const int inx = b.ibnx[n], iny = b.ibny[n];
+  const double q = g.cyl ? b.n_B[n] * b.Q_B[n] * g.rdx * g.rdy / x : b.n_B[n] * b.Q_B[n] * g.rdx * g.rdy;
+  const double dx0 = delta_x(bp, g, inx, x), dx1 = delta_x(bp, g, inx + 1, x);
+  const double dy0 = delta_y(bp, g, iny, y), dy1 = delta_y(bp, g, iny + 1, y);
+  double* c = hc + 4 * (long)n;
+  c[0] = q * dx0 * dy0;
+  c[1] = q * dx0 * dy1;
+  c[2] = q * dx1 * dy0;
+  c[3] = q * dx1 * dy1;
+}
+
+struct TempArgs {
+  F64 T_old, T_new;
+  const int* start;
+  const int* idx;
+  const double* hc;     // heat contributions (heat_contrib)
+  double coef_abs;      // 2 (0.22) 0.115129255 / (rho c omega^2) of MixtureTemperatureKernel
+  double T_inf;
+  int rho_const;
+  int bubbles;
+};
+
+// MixtureKMKernel, MixtureEnergyKernel and MixtureTemperatureKernel
+// (:955-1062) fused: each interior cell forms its conductivities, the four
+// face fluxes and its new temperature from the old field.
+template <typename P>
+__global__ void __launch_bounds__(256) temperature_step(const __grid_constant__ GridParams g, const TempArgs t,
+                                                         const typename P::G fg, const typename P::G fgn,
+                                                         const typename P::S px, const typename P::S py,
+                                                         const typename P::S pnx, const typename P::S pny) {
+  const Frame& f = g.f;
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  if (i > f.X || j > f.Y) return;
+  auto km = [&](int a, int b) -> double {
+    const long k = f.idx(a, b);
+    const double fv = fg.get(k);
+    return conductivity_water(t.T_old.get(k) + t.T_inf) * (1.0 - 3.0 * fv / (2.0 + fv));
+  };
+  const long k = f.idx(i, j);
+  const double Tc = t.T_old.get(k);
+  const double kc = km(i, j), kl = km(i - 1, j), kr = km(i + 1, j), kd = km(i, j - 1), ku = km(i, j + 1);
+  const double exr = 2.0 * kc * kr / (kc + kr) * ((-Tc + t.T_old.get(f.idx(i + 1, j))) * g.rdx);
+  const double exl = 2.0 * kl * kc / (kl + kc) * ((-t.T_old.get(f.idx(i - 1, j)) + Tc) * g.rdx);
+  const double eyu = 2.0 * kc * ku / (kc + ku) * ((-Tc + t.T_old.get(f.idx(i, j + 1))) * g.rdy);
+  const double eyd = 2.0 * kd * kc / (kd + kc) * ((-t.T_old.get(f.idx(i, j - 1)) + Tc) * g.rdy);
+  double s0 = (px.get(k) + py.get(k) - pnx.get(k) - pny.get(k)) / g.dt;
+  s0 = t.coef_abs * s0 * s0;
+  const double work = t.bubbles ? gather_fg(f, t.start, t.idx, t.hc, i, j) : 0.0;
+  const double Q = work + s0;
+  const double s1 = (exr - exl) * g.rdx;
+  const double s2 = (eyu - eyd) * g.rdy;
+  const double rho_m = t.rho_const ? g.rho_inf : (1.0 - fgn.get(k)) * g.rho_inf;
+  const double cpm = heat_capacity_water(Tc + t.T_inf);
+  t.T_new.put(k, Tc + g.dt * (s1 + s2 + Q) / (rho_m * cpm));
+}
+
+// MixtureBoundaryTemperatureKernel (:1065-1102) as one block: the old ghost
+// ring is carried over, then the sections run in the reference's order, each
+// over all its indices before the next (X0, X1, Y0, Y1; the Y1 loop starts at
+// row Y, so row Y takes the ghost row's value and the ghost row keeps it).
+__global__ void __launch_bounds__(1024) temperature_bc(const __grid_constant__ GridParams g, const F64 T_old,
+                                                        const F64 T_new) {
+  const Frame& f = g.f;
+  const int X = f.X, Y = f.Y;
+  for (int q = threadIdx.x; q <= X + 1; q += blockDim.x) {
+    T_new.put(f.idx(q, 0), T_old.get(f.idx(q, 0)));
+    T_new.put(f.idx(q, Y + 1), T_old.get(f.idx(q, Y + 1)));
+  }
+  for (int q = threadIdx.x; q <= Y + 1; q += blockDim.x) {
+    T_new.put(f.idx(0, q), T_old.get(f.idx(0, q)));
+    T_new.put(f.idx(X + 1, q), T_old.get(f.idx(X + 1, q)));
+  }
+  __syncthreads();
+  if (!g.pml_x0)
+    for (int q = 1 + threadIdx.x; q <= Y; q += blockDim.x) T_new.put(f.idx(0, q), T_new.get(f.idx(1, q)));
+  __syncthreads();
+  if (!g.pml_x1)
+    for (int q = threadIdx.x; q <= Y + 1; q += blockDim.x) T_new.put(f.idx(X + 1, q), T_new.get(f.idx(X, q)));
+  __syncthreads();
+  if (!g.pml_y0)
+    for (int q = threadIdx.x; q <= X + 1; q += blockDim.x) T_new.put(f.idx(q, 0), T_new.get(f.idx(q, 1)));
+  __syncthreads();
+  if (!g.pml_y1)
+    for (int q = threadIdx.x; q <= X + 1; q += blockDim.x) {
+      T_new.put(f.idx(q, Y), T_new.get(f.idx(q, Y + 1)));
+      T_new.put(f.idx(q, Y + 1), T_new.get(f.idx(q, Y)));
+    }
+}
+
 struct Profiler {
   bool on = false;
   std::vector<cudaEvent_t> ev;  // pairs
@@ -1203,6 +1322,12 @@ struct Sim {
   cudaGraph_t step_graph[6] = {};
   cudaGraphExec_t step_exec[6] = {};
   bool capturing = false;    // launches go into a graph (device-decided coupling box)
+  // Temperature branch (debug.T): two temperature buffers and the bubbles'
+  // heat contributions.
+  bool temperature_on = false;
+  void* Tbuf[2] = {nullptr, nullptr};
+  int cur_t = 0;
+  double* heat = nullptr;
   bool graphs_on = true;     // ext: off runs every step from the host
   Scalars* h_push = nullptr;  // pinned staging of the host state for the graph path
   bool debug_picard = std::getenv("CRP_DEBUG_PICARD") != nullptr;  // residual of every Picard iteration to stderr
@@ -1245,6 +1370,8 @@ struct Sim {
       py[k] = carve<double>(cells, off, dry);
     }
     for (int k = 0; k < 3; k++) fg[k] = carve<double>(cells, off, dry);
+    if (temperature_on)
+      for (int k = 0; k < 2; k++) Tbuf[k] = carve<double>(cells, off, dry);
     scratch = carve<double>((size_t)(f.X + 2) * (f.Y + 2), off, dry);
     d_sigma = carve<double>(hs.sigma_block.size(), off, dry);
     d_scalars = carve<Scalars>(1, off, dry);
@@ -1262,6 +1389,7 @@ struct Sim {
                      &bub.re, &bub.re_n, &bub.vbx, &bub.vby, &bub.R0};
     for (double** p : dp) *p = carve<double>(std::max(n, 1), off, dry);
     bub.contrib = carve<double>(4 * (size_t)std::max(n, 1), off, dry);
+    heat = temperature_on ? carve<double>(4 * (size_t)std::max(n, 1), off, dry) : nullptr;
     int** ip[] = {&bub.ibmx, &bub.ibmy, &bub.ibnx, &bub.ibny, &bub.bin, &bub.nsub};
     for (int** p : ip) *p = carve<int>(std::max(n, 1), off, dry);
     bins.nbx = f.X + 3;
@@ -1305,6 +1433,7 @@ struct Sim {
     mixed = cfg.ext_precision == CRP_PREC_MIXED;
     picard_tol = cfg.ext_picard_tol > 0.0 ? cfg.ext_picard_tol : (mixed ? 1.0e-5 : (double)1.0e-7f);
     graphs_on = cfg.ext_graphs != 0;
+    temperature_on = cfg.dbg_T != 0;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CRP_ERR_NO_DEVICE, "no CUDA device");
     if (user_stream) {
@@ -1576,6 +1705,7 @@ struct Sim {
       }
     }
     if (std::isnan(resimax)) return fail(CRP_ERR_NONFINITE, "non-finite pressure");
+    if (temperature_on) CRP_CUDA(mixed ? launch_temperature<PrecMixed>() : launch_temperature<PrecFP64>());
     // Support of this step's void fraction: the gather's when it ran, else the
     // prediction's.
     const Box snow = loop > 0 ? bnow : box_union(supp[0], box_union(supp[1], supp[2]));
@@ -1877,7 +2007,7 @@ struct Sim {
   // simulations without bubbles run from the host; the rest as graphs.
   crp_status step_n(int n) {
     int k = 0;
-    while (k < n && (stats.steps == 0 || prof.on || !graphs_on || hs.nb == 0 || debug_picard)) {
+    while (k < n && (stats.steps == 0 || prof.on || !graphs_on || hs.nb == 0 || debug_picard || temperature_on)) {
       const crp_status st = step_once();
       if (st != CRP_OK) return st;
       k++;
@@ -1913,6 +2043,9 @@ struct Sim {
       case CRP_FIELD_FG: return copy_window(fg[fg_a], kg, 0, X + 1, 0, Y + 1, host);
       case CRP_FIELD_FGN: return copy_window(fg[fg_b], kg, 0, X + 1, 0, Y + 1, host);
       case CRP_FIELD_FGM: return copy_window(fg[fg_c], kg, 0, X + 1, 0, Y + 1, host);
+      case CRP_FIELD_T:
+        if (!temperature_on) return fail(CRP_ERR_UNSUPPORTED, "the temperature is computed only with debug.T = 1");
+        return copy_window(Tbuf[cur_t], 0, 0, X + 1, 0, Y + 1, host);
       case CRP_FIELD_RHO_M: {
         crp_status st = copy_window(fg[fg_a], kg, 0, X + 1, 0, Y + 1, host);
         if (st != CRP_OK) return st;
@@ -1954,6 +2087,49 @@ struct Sim {
     const int ng = std::max(gp.f.X, gp.f.Y) + 3;
     const V vxn = view<V>(vx[nv]), vyn = view<V>(vy[nv]);
     return launch(kClassOther, [&] { vghost<V><<<(ng + 255) / 256, 256, 0, stream>>>(gp, vxn, vyn); });
+  }
+
+  // calculate_temperature after the Picard loop: the bins must follow the
+  // bubbles' current cells for the heat gather.
+  template <typename P>
+  cudaError_t launch_temperature() {
+    using S = typename P::S;
+    using G = typename P::G;
+    cudaError_t e;
+    const bool bubbles = hs.nb > 0 && cfg.bub_enable;
+    if (bubbles) {
+      if (bins_stale) {
+        if ((e = build_bins()) != cudaSuccess) return e;
+        bins_stale = false;
+      }
+      if ((e = launch(kClassOther, [&] {
+             heat_contrib<<<(bub.n + 255) / 256, 256, 0, stream>>>(gp, bp, bub, heat);
+           })) != cudaSuccess)
+        return e;
+    }
+    TempArgs ta;
+    ta.T_old = F64{(double*)Tbuf[cur_t]};
+    ta.T_new = F64{(double*)Tbuf[cur_t ^ 1]};
+    ta.start = bins.start;
+    ta.idx = bins.idx;
+    ta.hc = heat;
+    ta.coef_abs = 2.0 * (0.22) * 0.115129255 / (gp.rho_inf * gp.c_inf * gp.omega * gp.omega);
+    ta.T_inf = hs.d.T_inf;
+    ta.rho_const = stats.steps == 0 ? 1 : 0;
+    ta.bubbles = bubbles ? 1 : 0;
+    const G fgc = view<G>(fg[fg_a]), fgp = view<G>(fg[fg_b]);
+    const S pxc = view<S>(px[cur_p]), pyc = view<S>(py[cur_p]), pxn = view<S>(px[cur_p ^ 1]),
+            pyn = view<S>(py[cur_p ^ 1]);
+    dim3 blk(32, 8), grd((gp.f.X + 31) / 32, (gp.f.Y + 7) / 8);
+    if ((e = launch(kClassOther, [&] {
+           temperature_step<P><<<grd, blk, 0, stream>>>(gp, ta, fgc, fgp, pxc, pyc, pxn, pyn);
+         })) != cudaSuccess)
+      return e;
+    if ((e = launch(kClassOther, [&] { temperature_bc<<<1, 1024, 0, stream>>>(gp, ta.T_old, ta.T_new); })) !=
+        cudaSuccess)
+      return e;
+    cur_t ^= 1;
+    return cudaSuccess;
   }
 
   template <typename P>
@@ -2211,6 +2387,13 @@ crp_status crp_read_field(crp_sim* h, crp_field f, double* host) {
 crp_status crp_read_bubbles(crp_sim* h, crp_bubble_field w, double* host) {
   if (!h || !host) return CRP_ERR_INVALID;
   return h->s.read_bubbles(w, host);
+}
+
+crp_status crp_minmax_T(const crp_sim* h, double* T_min, double* T_max) {
+  if (!h || !T_min || !T_max) return CRP_ERR_INVALID;
+  *T_min = h->s.mm.T_min;
+  *T_max = h->s.mm.T_max;
+  return CRP_OK;
 }
 
 crp_status crp_minmax(const crp_sim* h, double* fg_min, double* fg_max, double* p0_min, double* p0_max) {

@@ -227,6 +227,15 @@ struct Field {
   bool in(int i, int j) const { return i >= i0 && i < i0 + w && j >= j0 && j < j0 + h; }
 };
 
+// Water properties, inc/bubble_CUDA_kernel.cuh:176-193 (float literals as written there).
+double conductivity_water(double T) { return 0.76760 + ((double)7.5390e-3f * T) - (double)9.8250e-6f * (T * T); }
+double heat_capacity_water(double T) {
+  const double H2O = (double)18.0e-3f;
+  return (917.5 - (double)10.1016f * T + (double)0.0454134f * (T * T) - 9.07517e-5 * (T * T * T) +
+          (double)6.80700e-8f * (T * T * T * T)) /
+         H2O;
+}
+
 struct Derived {
   double dx, dy, rdx, rdy;
   double fpx, fpy, omega, dt;
@@ -360,6 +369,10 @@ struct crpo_sim {
   bool cyl, bubbles_on;
   std::vector<double> mx, my, nx, ny, xu, rxp;
   Field p0, px, py, pnx, pny, vx, vy, fg, fgn, fgm, rho_m, work;
+  // Temperature branch (debug.T): T and k_m on the 2m window, C_pm on the 1m
+  // window, the energy fluxes Ex / Ey, and the reference's Work array.
+  bool temperature_on = false;
+  Field T, k_m, C_pm, Ex, Ey, twork;
   // Bubble state, bubble_t (inc/bubble_CUDA.h:172-189), structure of arrays.
   int nb = 0;
   std::vector<BubConst> bc;
@@ -443,6 +456,15 @@ struct crpo_sim {
     fgn = fg;
     fgm = fg;
     work = fg;
+    temperature_on = c.dbg_T != 0;
+    if (temperature_on) {
+      T.init(a.ista2m, a.iend2m, a.jsta2m, a.jend2m, 0.0);
+      k_m = T;
+      twork = T;
+      C_pm.init(a.ista1m, a.iend1m, a.jsta1m, a.jend1m, heat_capacity_water(d.T_inf));
+      Ex.init(a.ista1n, a.iend1n, a.jsta1m, a.jend1m, 0.0);
+      Ey.init(a.ista1m, a.iend1m, a.jsta1n, a.jend1n, 0.0);
+    }
     if (bubbles_on) {
       crp_status st = init_bubbles(bin);
       if (st != CRP_OK) return st;
@@ -827,11 +849,73 @@ struct crpo_sim {
     return capped ? -1 : worst;
   }
 
-  // MixturePropertiesKernel, density part (inc/bubble_CUDA_kernel.cuh:1110-1125).
+  // MixturePropertiesKernel (inc/bubble_CUDA_kernel.cuh:1110-1125): density,
+  // and the heat capacity when the temperature is computed.
   void properties() {
 #pragma omp parallel for schedule(static)
     for (int j = a.jsta1m; j <= a.jend1m; j++)
-      for (int i = a.ista1m; i <= a.iend1m; i++) rho_m.at(i, j) = (1.0 - fg.at(i, j)) * d.rho_inf;
+      for (int i = a.ista1m; i <= a.iend1m; i++) {
+        rho_m.at(i, j) = (1.0 - fg.at(i, j)) * d.rho_inf;
+        if (temperature_on) C_pm.at(i, j) = heat_capacity_water(T.at(i, j) + d.T_inf);
+      }
+  }
+
+  // calculate_temperature (inc/bubble_CUDA_kernel.cuh:1347-1376).
+  void temperature() {
+    // Work cleared, then BubbleHeatKernel (:972-1007), bubble by bubble.
+    std::fill(twork.v.begin(), twork.v.end(), 0.0);
+    if (bubbles_on) {
+      for (int b = 0; b < nb; b++) {
+        const double q = cyl ? n_B[b] * Q_B[b] * d.rdx * d.rdy / x[b] : n_B[b] * Q_B[b] * d.rdx * d.rdy;
+        for (int i = ibnx[b] + d.mbs; i <= ibnx[b] + d.mbe; i++) {
+          const double dxw = delta_x(i, x[b]);
+          for (int j = ibny[b] + d.mbs; j <= ibny[b] + d.mbe; j++) {
+            const double dyw = delta_y(j, y[b]);
+            if (i >= a.ista2m && i <= a.iend2m && j >= a.jsta2m && j <= a.jend2m) twork.at(i, j) += q * dxw * dyw;
+          }
+        }
+      }
+    }
+    // MixtureKMKernel (:955-969).
+    for (int j = a.jsta2m; j <= a.jend2m; j++)
+      for (int i = a.ista2m; i <= a.iend2m; i++)
+        k_m.at(i, j) = conductivity_water(T.at(i, j) + d.T_inf) * (1.0 - 3.0 * fg.at(i, j) / (2.0 + fg.at(i, j)));
+    // MixtureEnergyKernel (:1010-1035).
+    for (int j = a.jsta1m; j <= a.jend1m; j++)
+      for (int i = a.ista1n; i <= a.iend1n; i++) {
+        const double s0 = 2.0 * k_m.at(i, j) * k_m.at(i + 1, j) / (k_m.at(i, j) + k_m.at(i + 1, j));
+        const double s1 = (-T.at(i, j) + T.at(i + 1, j)) * d.rdx;
+        Ex.at(i, j) = s0 * s1;
+      }
+    for (int j = a.jsta1n; j <= a.jend1n; j++)
+      for (int i = a.ista1m; i <= a.iend1m; i++) {
+        const double s0 = 2.0 * k_m.at(i, j) * k_m.at(i, j + 1) / (k_m.at(i, j) + k_m.at(i, j + 1));
+        const double s1 = (-T.at(i, j) + T.at(i, j + 1)) * d.rdy;
+        Ey.at(i, j) = s0 * s1;
+      }
+    // MixtureTemperatureKernel (:1038-1062).
+    for (int j = a.jstam; j <= a.jendm; j++)
+      for (int i = a.istam; i <= a.iendm; i++) {
+        double s0 = (px.at(i, j) + py.at(i, j) - pnx.at(i, j) - pny.at(i, j)) / d.dt;
+        s0 = 2.0 * (0.22) * 0.115129255 / (d.rho_inf * d.cs_inf * d.omega * d.omega) * s0 * s0;
+        const double Q = twork.at(i, j) + s0;
+        const double s1 = (Ex.at(i, j) - Ex.at(i - 1, j)) * d.rdx;
+        const double s2 = (Ey.at(i, j) - Ey.at(i, j - 1)) * d.rdy;
+        T.at(i, j) += twork.at(i, j) = d.dt * (s1 + s2 + Q) / (rho_m.at(i, j) * C_pm.at(i, j));
+      }
+    // MixtureBoundaryTemperatureKernel (:1065-1102), sections in order.
+    if (!cfg.pml_x0)
+      for (int j = a.jstam; j <= a.jendm; j++)
+        for (int i = 1 + a.ns + a.ms; i <= 0; i++) T.at(i, j) = T.at(1 - i, j);
+    if (!cfg.pml_x1)
+      for (int j = a.jsta1m; j <= a.jend1m; j++)
+        for (int i = X + 1; i <= X + a.ne + a.me; i++) T.at(i, j) = T.at(X - (i - X - 1), j);
+    if (!cfg.pml_y0)
+      for (int i = a.ista2m; i <= a.iend2m; i++)
+        for (int j = 1 + a.ns + a.ms; j <= 0; j++) T.at(i, j) = T.at(i, 1 - j);
+    if (!cfg.pml_y1)
+      for (int i = a.ista2m; i <= a.iend2m; i++)
+        for (int j = Y; j <= Y + a.ne + a.me; j++) T.at(i, j) = T.at(i, Y - (j - Y - 1));
   }
 
   // One pass of solve_bubbles' main loop, src/bubble_CUDA.cu:206-285.
@@ -859,6 +943,7 @@ struct crpo_sim {
         resimax = pressure();
       }
     }
+    if (temperature_on) temperature();
     properties();
     stats.steps = nstep;
     stats.time = tstep;
@@ -936,6 +1021,10 @@ crp_status crpo_read_field(crpo_sim* s, crp_field f, double* host) {
     case CRP_FIELD_FGN: src = &s->fgn; break;
     case CRP_FIELD_FGM: src = &s->fgm; break;
     case CRP_FIELD_RHO_M: src = &s->rho_m; break;
+    case CRP_FIELD_T:
+      if (!s->temperature_on) return CRP_ERR_UNSUPPORTED;
+      src = &s->T;
+      break;
     default: return CRP_ERR_INVALID;
   }
   std::memcpy(host, src->v.data(), sizeof(double) * src->v.size());

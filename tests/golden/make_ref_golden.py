@@ -57,7 +57,7 @@ RUN_CASES = {
                  tr_focal_dist=3.0e-3, tr_box_size=1.0e-3, sim_save_interval=60),
 }
 
-FIELDS = ["p0", "p", "pn", "vx", "vy", "f_g", "f_gn", "f_gm", "rho_m"]
+FIELDS = ["p0", "p", "pn", "vx", "vy", "f_g", "f_gn", "f_gm", "rho_m", "T"]
 BUBBLE_FIELDS = ["pos", "R_t", "R_p", "R_n", "d1_R_p", "PG_p", "PL_p", "PL_n", "dt", "re", "Q_B", "n_B", "ibm",
                  "ibn"]
 
@@ -157,7 +157,7 @@ def run_case(name: str, outdir: str) -> None:
     rc = r.crp_ref_run(steps, 1000, _p(picard))
     assert rc == 0, rc
     shapes = {"p0": (j1m, i1m), "p": (j1m, 2 * i1m), "pn": (j1m, 2 * i1m), "vx": (j2m, i2n), "vy": (j2n, i2m),
-              "f_g": (j2m, i2m), "f_gn": (j2m, i2m), "f_gm": (j2m, i2m), "rho_m": (j1m, i1m)}
+              "f_g": (j2m, i2m), "f_gn": (j2m, i2m), "f_gm": (j2m, i2m), "rho_m": (j1m, i1m), "T": (j2m, i2m)}
     out = {"steps": np.int64(steps), "picard": picard, "time": np.float64(r.crp_ref_time())}
     for fname in FIELDS:
         a = np.zeros(shapes[fname])

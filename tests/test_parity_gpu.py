@@ -19,7 +19,7 @@ TOL_FP64 = 1e-9  # max |gpu - oracle| / max(max |oracle|, floor) per field
 FLOOR = {"p0": 1e-3, "px": 1e-3, "py": 1e-3, "pnx": 1e-3, "pny": 1e-3, "vx": 1e-9, "vy": 1e-9, "f_g": 1e-12,
          "f_gn": 1e-12, "f_gm": 1e-12, "rho_m": 1.0, "bub_x": 1e-9, "bub_y": 1e-9, "bub_R_t": 1e-9,
          "bub_R_p": 1e-9, "bub_R_n": 1e-9, "bub_d1_R_p": 1e-6, "bub_PG_p": 1e-3, "bub_PL_p": 1e-3, "bub_PL_n": 1e-3,
-         "bub_dt": 1e-15, "bub_Q_B": 1e-12, "bub_v_x": 1e-9, "bub_v_y": 1e-9}
+         "bub_dt": 1e-15, "bub_Q_B": 1e-12, "bub_v_x": 1e-9, "bub_v_y": 1e-9, "T": 1e-30}
 
 FIELDS = ["p0", "px", "py", "pnx", "pny", "vx", "vy", "f_g", "f_gn", "f_gm", "rho_m"]
 BUBBLE = ["x", "y", "R_t", "R_p", "R_n", "d1_R_p", "PG_p", "PL_p", "PL_n", "dt", "Q_B", "v_x", "v_y"]
@@ -47,7 +47,8 @@ def rel_err(a, b, floor):
 
 def _compare(gpu, cpu, tol):
     worst = {}
-    for k in FIELDS:
+    fields = FIELDS + (["T"] if gpu._keep[0].dbg_T else [])
+    for k in fields:
         a, b = gpu.field(k), cpu.field(k)
         assert a.shape == b.shape, k
         worst[k] = rel_err(a, b, FLOOR[k])

@@ -21,8 +21,8 @@ _mrg = importlib.util.module_from_spec(_spec)
 _spec.loader.exec_module(_mrg)
 
 _, STEPS = _mrg.case_config("tiny")
-FILES = [f"{stem}{STEPS:05d}.txt" for stem in ("fg_step_", "p0_step_", "vx_step_", "vy_step_", "bubble_radii_",
-                                               "bubble_PG_")]
+FILES = [f"{stem}{STEPS:05d}.txt" for stem in ("fg_step_", "T_step_", "p0_step_", "vx_step_", "vy_step_",
+                                               "bubble_radii_", "bubble_PG_")]
 
 # crp.Config field -> (section, key) of the configuration file, for the keys the
 # tiny case overrides.

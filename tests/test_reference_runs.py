@@ -48,6 +48,8 @@ def ref_fields(g):
     out = {"p0": g["p0"], "px": g["p"][:, 0::2], "py": g["p"][:, 1::2], "pnx": g["pn"][:, 0::2],
            "pny": g["pn"][:, 1::2], "vx": g["vx"], "vy": g["vy"], "f_g": g["f_g"], "f_gn": g["f_gn"],
            "f_gm": g["f_gm"], "rho_m": g["rho_m"]}
+    if "T" in g:
+        out["T"] = g["T"]
     return out
 
 
