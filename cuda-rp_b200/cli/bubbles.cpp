@@ -142,7 +142,6 @@ int main(int argc, char** argv) {
   std::cout << "Saving results to " << target_dir << std::endl;
   std::cout << "Save format is " << (sph && !ascii ? "sph" : "ASCII plaintext");
   std::cout << std::endl << std::endl;
-  if (sph) std::cout << "note: SPH output is not produced by this build; ASCII is written when -a is given" << std::endl;
   if (cfg.tr_pid) std::cout << "note: the PID focal controller is not part of this build; the focus stays fixed" << std::endl;
 
   std::error_code ec;
@@ -164,7 +163,10 @@ int main(int argc, char** argv) {
   } prog{&cfg};
   crp_output_plan plan{};
   plan.save_interval = cfg.sim_save_interval > 0 ? cfg.sim_save_interval : 0;
-  plan.dir = ascii ? target_dir.c_str() : nullptr;
+  // As solve_bubbles: SPH when -s is given, else text rawdata when -a is
+  // (src/bubble_CUDA.cu:398-411).
+  plan.dir = (sph || ascii) ? target_dir.c_str() : nullptr;
+  plan.sph = sph ? 1 : 0;
   plan.user = &prog;
   plan.progress = [](int64_t step, double time, void* user) {
     const crp_config* c = ((Progress*)user)->cfg;

@@ -69,7 +69,7 @@ PROGRESS = ctypes.CFUNCTYPE(None, ctypes.c_int64, c_dbl, ctypes.c_void_p)
 
 class OutputPlan(ctypes.Structure):
     _fields_ = [("n_steps", ctypes.c_int64), ("t_max", c_dbl), ("save_interval", c_int),
-                ("dir", ctypes.c_char_p), ("progress", PROGRESS), ("user", ctypes.c_void_p)]
+                ("dir", ctypes.c_char_p), ("sph", c_int), ("progress", PROGRESS), ("user", ctypes.c_void_p)]
 
 
 class BubblesIn(ctypes.Structure):
@@ -131,6 +131,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "crp_read_field": (c_int, [vp, c_int, vp]),
         "crp_read_bubbles": (c_int, [vp, c_int, vp]),
         "crp_write_rawdata": (c_int, [vp, ctypes.c_char_p]),
+        "crp_write_sph": (c_int, [vp, ctypes.c_char_p]),
         "crp_stream": (vp, [vp]),
         "crp_set_profiling": (c_int, [vp, c_int]),
         "crp_minmax": (c_int, [vp, P(c_dbl), P(c_dbl), P(c_dbl), P(c_dbl)]),
@@ -244,9 +245,12 @@ class Sim:
         """crp_run: step to the limits (config's n_step_max/t_step_max when both
         are 0), writing rawdata every save_interval steps into directory."""
         cb = PROGRESS(lambda step, t, user: progress(step, t)) if progress else PROGRESS()
-        plan = OutputPlan(n_steps, t_max, save_interval, directory.encode() if directory else None, cb, None)
+        plan = OutputPlan(n_steps, t_max, save_interval, directory.encode() if directory else None, 0, cb, None)
         cfg = self._keep[0]
         self._check(self.lib.crp_run(self.h, ctypes.byref(plan), ctypes.byref(cfg) if cfg is not None else None))
+
+    def write_sph(self, directory: str):
+        self._check(self.lib.crp_write_sph(self.h, directory.encode()))
 
     def write_rawdata(self, directory: str):
         self._check(self.lib.crp_write_rawdata(self.h, directory.encode()))

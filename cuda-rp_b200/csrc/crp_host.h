@@ -37,10 +37,12 @@ crp_status host_setup(const crp_config& cfg, const crp_bubbles_in* bubbles, Host
 
 // Rawdata writer (rawdata.cpp) and the accessors it uses (sim.cu).
 crp_status write_rawdata(crp_sim* sim, const char* dir);
+crp_status write_sph(crp_sim* sim, const char* dir);
 crp_status sim_read_field(crp_sim* h, crp_field f, double* host);
 crp_status sim_read_bubbles(crp_sim* h, crp_bubble_field w, double* host);
 const crp_config& sim_config(const crp_sim* h);
 int64_t sim_step_count(const crp_sim* h);
+double sim_time(const crp_sim* h);
 
 // Running min/max of the values written to rawdata files (the globals of
 // src/bubbles.cpp:11-13 that save_ascii updates), per simulation.

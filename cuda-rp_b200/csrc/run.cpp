@@ -21,7 +21,7 @@ extern "C" crp_status crp_run(crp_sim* sim, const crp_output_plan* plan, const c
     crp_get_stats(sim, &st);
     if (plan->save_interval > 0 && st.steps % plan->save_interval == 0) {
       if (plan->dir) {
-        s = crp_write_rawdata(sim, plan->dir);
+        s = plan->sph ? crp_write_sph(sim, plan->dir) : crp_write_rawdata(sim, plan->dir);
         if (s != CRP_OK) return s;
       }
       if (plan->progress) plan->progress(st.steps, st.time, plan->user);

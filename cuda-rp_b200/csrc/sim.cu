@@ -2416,6 +2416,11 @@ crp_status crp_write_rawdata(crp_sim* h, const char* dir) {
   return crp::write_rawdata(h, dir);
 }
 
+crp_status crp_write_sph(crp_sim* h, const char* dir) {
+  if (!h || !dir) return CRP_ERR_INVALID;
+  return crp::write_sph(h, dir);
+}
+
 }  // extern "C"
 
 namespace crp {
@@ -2424,5 +2429,6 @@ crp_status sim_read_field(crp_sim* h, crp_field f, double* host) { return h->s.r
 crp_status sim_read_bubbles(crp_sim* h, crp_bubble_field w, double* host) { return h->s.read_bubbles(w, host); }
 const crp_config& sim_config(const crp_sim* h) { return h->s.cfg; }
 int64_t sim_step_count(const crp_sim* h) { return h->s.stats.steps; }
+double sim_time(const crp_sim* h) { return h->s.tstep; }
 MinMax& sim_minmax(crp_sim* h) { return h->s.mm; }
 }  // namespace crp

@@ -229,6 +229,12 @@ crp_status crp_read_bubbles(crp_sim* sim, crp_bubble_field what, double* host);
  * bubble_radii_/bubble_PG_%05d.txt as selected by the debug keys. */
 crp_status crp_write_rawdata(crp_sim* sim, const char* dir);
 
+/* Write the reference's binary SPH files for the current step into dir
+ * (save_sph, src/output_styles.cpp:36-137; record layout of SphData::SaveSph,
+ * src/SphDataType.cpp:142-192): fg/p0/T_step_%05d.sph as selected by the
+ * debug keys; updates the same min/max as crp_write_rawdata. */
+crp_status crp_write_sph(crp_sim* sim, const char* dir);
+
 /* Running min/max of the f_g and p0 values written by crp_write_rawdata so far
  * (what save_ascii accumulates for *_minmax.txt, src/output_styles.cpp:200-224). */
 crp_status crp_minmax(const crp_sim* sim, double* fg_min, double* fg_max, double* p0_min, double* p0_max);
@@ -281,6 +287,7 @@ typedef struct crp_output_plan {
   double t_max;
   int32_t save_interval;
   const char* dir;
+  int32_t sph;  /* nonzero: write SPH files instead of text rawdata (the reference's -s) */
   void (*progress)(int64_t step, double time, void* user);
   void* user;
 } crp_output_plan;

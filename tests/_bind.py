@@ -158,6 +158,7 @@ def ref_lib():
             "crp_ref_read_field": (ctypes.c_int, [ctypes.c_char_p, vp]),
             "crp_ref_read_bubbles": (ctypes.c_int, [ctypes.c_char_p, vp]),
             "crp_ref_save_ascii": (ctypes.c_int, [ctypes.c_char_p]),
+            "crp_ref_save_sph": (ctypes.c_int, [ctypes.c_char_p]),
             "crp_ref_time": (ctypes.c_double, []),
             "crp_ref_teardown": (ctypes.c_int, []),
         }

@@ -177,6 +177,9 @@ def run_case(name: str, outdir: str) -> None:
         d = os.path.join(outdir, "ref_rawdata_tiny") + "/"
         os.makedirs(d, exist_ok=True)
         assert r.crp_ref_save_ascii(d.encode()) == 0
+        d = os.path.join(outdir, "ref_sph_tiny") + "/"
+        os.makedirs(d, exist_ok=True)
+        assert r.crp_ref_save_sph(d.encode()) == 0
     r.crp_ref_teardown()
     np.savez_compressed(os.path.join(outdir, f"ref_run_{name}.npz"), **out)
     print(f"{name}: steps={steps} picard total={int(picard.sum())} max={int(picard.max())} bubbles={nb}")

@@ -118,3 +118,39 @@ def test_run_writes_what_a_step_loop_writes(tmp_path):
     assert names and sorted(os.listdir(a)) == names
     for name in names:
         assert open(a / name).read() == open(b / name).read(), name
+
+
+SPH = os.path.join(HERE, "golden", "ref_sph_tiny")
+
+
+def _read_sph(path):
+    """Records of an SPH file: each is (int length, bytes, int length)."""
+    raw = open(path, "rb").read()
+    recs, k = [], 0
+    while k < len(raw):
+        n = int(np.frombuffer(raw[k:k + 4], np.int32)[0])
+        recs.append(raw[k + 4:k + 4 + n])
+        assert raw[k + 4 + n:k + 8 + n] == raw[k:k + 4]
+        k += 8 + n
+    return recs
+
+
+@pytest.mark.skipif(not os.path.isdir(SPH), reason="no SPH fixture")
+def test_sph_matches_reference_save_sph(tmp_path):
+    """SPH files against the reference's own save_sph output for the tiny case:
+    identical headers; values as floats within one float rounding."""
+    cfg, steps = _mrg.case_config("tiny")
+    with crp.Sim(cfg) as sim:
+        sim.step(steps)
+        sim.write_sph(str(tmp_path))
+    names = sorted(os.listdir(SPH))
+    assert names == sorted(f"{s}{steps:05d}.sph" for s in ("fg_step_", "p0_step_", "T_step_"))
+    for name in names:
+        ours, ref = _read_sph(os.path.join(tmp_path, name)), _read_sph(os.path.join(SPH, name))
+        assert len(ours) == len(ref) == 6
+        for a, b in zip(ours[:5], ref[:5]):
+            assert a == b, name
+        va, vb = np.frombuffer(ours[5], np.float32), np.frombuffer(ref[5], np.float32)
+        assert va.shape == vb.shape
+        scale = max(float(np.abs(vb).max()), 1e-30)
+        assert float(np.abs(va.astype(np.float64) - vb).max()) <= 2.4e-7 * scale, name
