@@ -394,6 +394,10 @@ struct BubbleArrays {
   double *x, *y, *R_t, *R_p, *R_pn, *R_n, *R_nn, *d1_R_p, *d1_R_n, *PG_p, *PG_n, *PL_p, *PL_n, *PL_m, *Q_B, *n_B,
       *dt, *dt_n, *re, *re_n, *vbx, *vby, *R0, *contrib;
   int *ibmx, *ibmy, *ibnx, *ibny, *bin, *nsub;
+  // Position of each bubble in the sorted bins (-1: outside every bin).  A
+  // bubble's four stencil contributions are stored at 4 * pos, so that each
+  // cell gathers contiguous runs.
+  int* pos;
   int n;
 };
 
@@ -587,6 +591,12 @@ __global__ void bin_fill(const int* __restrict__ bin, int n, const int* __restri
   idx[slot] = b;
 }
 
+// Position of every binned bubble in the sorted order (pos was set to -1 first).
+__global__ void bin_pos(const int* __restrict__ idx, const int* __restrict__ total, int* __restrict__ pos, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n && k < *total) pos[idx[k]] = k;
+}
+
 // Bubbles of a cell in ascending index order, so every sum over a cell has a
 // fixed order run to run.
 __global__ void bin_sort(const int* __restrict__ start, int* __restrict__ idx, int nbins) {
@@ -712,7 +722,9 @@ __device__ __forceinline__ void rp_end(const GridParams& g, const BubbleParams& 
   const double Rt = s.Rt;
   const double vol = g.cyl ? bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy / x
                            : bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy;
-  double* c = b.contrib + 4 * (long)n;
+  const int p = b.pos[n];
+  if (p < 0) return;
+  double* c = b.contrib + 4 * (long)p;
   c[0] = vol * dx0 * dy0;
   c[1] = vol * dx0 * dy1;
   c[2] = vol * dx1 * dy0;
@@ -840,15 +852,16 @@ __global__ void __launch_bounds__(kLptScatterThreads)
 }
 
 // Void fraction of one cell from the bubbles of the four bins whose stencils
-// cover it (bins (i-1..i) x (j-1..j), each in ascending bubble order).
-__device__ __forceinline__ double gather_fg(const Frame& f, const int* __restrict__ start, const int* __restrict__ idx,
+// cover it (bins (i-1..i) x (j-1..j), each in ascending bubble order): their
+// contributions sit contiguously at 4 * (position in the sorted bins).
+__device__ __forceinline__ double gather_fg(const Frame& f, const int* __restrict__ start,
                                             const double* __restrict__ contrib, int i, int j) {
   double s = 0.0;
   for (int by = j - 1; by <= j; by++) {
     for (int bx = i - 1; bx <= i; bx++) {
-      int c = (by + 1) * (f.X + 3) + (bx + 1);
-      int slot = (i - bx) * 2 + (j - by);
-      for (int k = start[c]; k < start[c + 1]; k++) s += contrib[4 * (long)idx[k] + slot];
+      const int c = (by + 1) * (f.X + 3) + (bx + 1);
+      const int slot = (i - bx) * 2 + (j - by);
+      for (int k = start[c]; k < start[c + 1]; k++) s += contrib[4 * (long)k + slot];
     }
   }
   return s;
@@ -891,9 +904,9 @@ __global__ void __launch_bounds__(256) couple_press(const __grid_constant__ Grid
   if (i <= i1 && j <= j1) {
     double fgv;
     if (g.cyl && i <= 1)
-      fgv = gather_fg(f, a.start, a.idx, a.contrib, 0, j) + gather_fg(f, a.start, a.idx, a.contrib, 1, j);
+      fgv = gather_fg(f, a.start, a.contrib, 0, j) + gather_fg(f, a.start, a.contrib, 1, j);
     else
-      fgv = gather_fg(f, a.start, a.idx, a.contrib, i, j);
+      fgv = gather_fg(f, a.start, a.contrib, i, j);
     long k = f.idx(i, j);
     a.fg.put(k, fgv);
     fgv = a.fg.get(k);  // the stored value (FP32 in the mixed path) is what the step uses
@@ -965,7 +978,9 @@ __global__ void heat_contrib(const __grid_constant__ GridParams g, const __grid_
   const double q = g.cyl ? b.n_B[n] * b.Q_B[n] * g.rdx * g.rdy / x : b.n_B[n] * b.Q_B[n] * g.rdx * g.rdy;
   const double dx0 = delta_x(bp, g, inx, x), dx1 = delta_x(bp, g, inx + 1, x);
   const double dy0 = delta_y(bp, g, iny, y), dy1 = delta_y(bp, g, iny + 1, y);
-  double* c = hc + 4 * (long)n;
+  const int p = b.pos[n];
+  if (p < 0) return;
+  double* c = hc + 4 * (long)p;
   c[0] = q * dx0 * dy0;
   c[1] = q * dx0 * dy1;
   c[2] = q * dx1 * dy0;
@@ -1009,7 +1024,7 @@ __global__ void __launch_bounds__(256) temperature_step(const __grid_constant__ 
   const double eyd = 2.0 * kd * kc / (kd + kc) * ((-t.T_old.get(f.idx(i, j - 1)) + Tc) * g.rdy);
   double s0 = (px.get(k) + py.get(k) - pnx.get(k) - pny.get(k)) / g.dt;
   s0 = t.coef_abs * s0 * s0;
-  const double work = t.bubbles ? gather_fg(f, t.start, t.idx, t.hc, i, j) : 0.0;
+  const double work = t.bubbles ? gather_fg(f, t.start, t.hc, i, j) : 0.0;
   const double Q = work + s0;
   const double s1 = (exr - exl) * g.rdx;
   const double s2 = (eyu - eyd) * g.rdy;
@@ -1390,7 +1405,7 @@ struct Sim {
     for (double** p : dp) *p = carve<double>(std::max(n, 1), off, dry);
     bub.contrib = carve<double>(4 * (size_t)std::max(n, 1), off, dry);
     heat = temperature_on ? carve<double>(4 * (size_t)std::max(n, 1), off, dry) : nullptr;
-    int** ip[] = {&bub.ibmx, &bub.ibmy, &bub.ibnx, &bub.ibny, &bub.bin, &bub.nsub};
+    int** ip[] = {&bub.ibmx, &bub.ibmy, &bub.ibnx, &bub.ibny, &bub.bin, &bub.nsub, &bub.pos};
     for (int** p : ip) *p = carve<int>(std::max(n, 1), off, dry);
     bins.nbx = f.X + 3;
     bins.nby = f.Y + 3;
@@ -1593,7 +1608,14 @@ struct Sim {
            bin_fill<<<(bub.n + 255) / 256, 256, 0, stream>>>(bub.bin, bub.n, bins.start, bins.count, bins.idx);
          })) != cudaSuccess)
       return e;
-    return launch(kClassOther, [&] { bin_sort<<<(nbins + 255) / 256, 256, 0, stream>>>(bins.start, bins.idx, nbins); });
+    if ((e = launch(kClassOther, [&] {
+           bin_sort<<<(nbins + 255) / 256, 256, 0, stream>>>(bins.start, bins.idx, nbins);
+         })) != cudaSuccess)
+      return e;
+    if ((e = cudaMemsetAsync(bub.pos, 0xff, sizeof(int) * bub.n, stream)) != cudaSuccess) return e;
+    return launch(kClassOther, [&] {
+      bin_pos<<<(bub.n + 255) / 256, 256, 0, stream>>>(bins.idx, bins.start + nbins, bub.pos, bub.n);
+    });
   }
 
   // Radius-solve order from the last sub-step counts (heaviest first).
@@ -2233,7 +2255,9 @@ __global__ void bubble_contrib(const __grid_constant__ GridParams g, const __gri
   const double Rt = b.R_t[n];
   const double vol = g.cyl ? bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy / x
                            : bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy;
-  double* c = b.contrib + 4 * (long)n;
+  const int p = b.pos[n];
+  if (p < 0) return;
+  double* c = b.contrib + 4 * (long)p;
   c[0] = vol * dxw[0] * dyw[0];
   c[1] = vol * dxw[0] * dyw[1];
   c[2] = vol * dxw[1] * dyw[0];
@@ -2249,9 +2273,9 @@ __global__ void __launch_bounds__(256) couple_fg_only(const __grid_constant__ Gr
   if (i > f.X + 1 || j > f.Y + 1) return;
   double fgv;
   if (g.cyl && i <= 1)
-    fgv = gather_fg(f, a.start, a.idx, a.contrib, 0, j) + gather_fg(f, a.start, a.idx, a.contrib, 1, j);
+    fgv = gather_fg(f, a.start, a.contrib, 0, j) + gather_fg(f, a.start, a.contrib, 1, j);
   else
-    fgv = gather_fg(f, a.start, a.idx, a.contrib, i, j);
+    fgv = gather_fg(f, a.start, a.contrib, i, j);
   a.fg.put(f.idx(i, j), fgv);
 }
 
