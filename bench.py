@@ -265,10 +265,7 @@ def timed_run(cfg, bub, args, preroll, dist, dev):
         e1.synchronize()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     return ms, s0, sim.stats(), sim, clk.summary()
 
 
@@ -315,6 +312,24 @@ def driven_sample(sim, args, cells, nb):
     return out
 
 
+def max_over_ranks(x, dist):
+    """The largest of every rank's x (the job's time is its slowest rank's);
+    x itself without a process group.  NCCL reduces a CUDA tensor, gloo a CPU one."""
+    if not dist:
+        return x
+    import torch
+
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, ms):
+    """Whole-job throughput in units/s: every rank's units over the slowest rank's time."""
+    return units_per_rank * world / (ms * 1e-3)
+
+
 def focal_mask(sim, cfg, radius=2e-3):
     d = sim.dims
     fy = cfg.tr_focal_dist * 0.5 * np.sqrt(3.0)
@@ -355,7 +370,7 @@ def run_ours(args, rank, world, dist):
     cfg.ext_precision = 1 if primary == "mixed" else 0
     nb = sim.dims.num_bubbles
     ms, s0, s1 = run["ms"], run["s0"], run["s1"]
-    value = cells * mix_steps * world / (ms * 1e-3) / 1e6
+    value = job_rate(cells * mix_steps, world, ms) / 1e6
     launches = s1.kernel_launches - s0.kernel_launches
     picard = s1.picard_total - s0.picard_total
 

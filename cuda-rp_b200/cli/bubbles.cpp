@@ -8,6 +8,7 @@
 // simulated path: the output directory is created if missing and never cleared
 // (the reference runs `rm -rf` on it); SPH files, T_step files, the focal-point
 // tracker files and the PID passes are not produced (the run uses a fixed focus).
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -92,7 +93,7 @@ void write_minmax(const std::string& path, double lo, double hi) {
 int main(int argc, char** argv) {
   time_t start_time = time(nullptr);
   std::string in_file, target_dir = "./rawdata/";
-  bool ascii = false, sph = false;
+  bool ascii = false, sph = false, dir_given = false;
   for (int k = 1; k < argc; k++) {
     std::string a = argv[k];
     if (a == "-h" || a == "--help") {
@@ -113,8 +114,10 @@ int main(int argc, char** argv) {
         return 1;
       }
       target_dir = argv[++k];
+      dir_given = true;
     } else if (a.rfind("--directory=", 0) == 0) {
       target_dir = a.substr(12);
+      dir_given = true;
     } else if (!a.empty() && a[0] == '-') {
       // unregistered options are ignored (allow_unregistered)
     } else if (in_file.empty()) {
@@ -142,74 +145,104 @@ int main(int argc, char** argv) {
   std::cout << "Saving results to " << target_dir << std::endl;
   std::cout << "Save format is " << (sph && !ascii ? "sph" : "ASCII plaintext");
   std::cout << std::endl << std::endl;
-  if (cfg.tr_pid) std::cout << "note: the PID focal controller is not part of this build; the focus stays fixed" << std::endl;
 
-  std::error_code ec;
-  std::filesystem::create_directories(target_dir, ec);
-  if (ec) {
-    std::cerr << "error: cannot create " << target_dir << ": " << ec.message() << std::endl;
-    return 1;
-  }
+  // transducer.pid_iterate passes (src/bubbles.cpp:218-306): with -d each pass
+  // writes to <dir>_I/, <dir>_II/, ...; the focus control state and the
+  // running min/max carry over from pass to pass.
+  const int num_iters = cfg.tr_pid_iterate > 0 ? cfg.tr_pid_iterate : 1;
+  std::string base_dir = target_dir;
+  if (!base_dir.empty() && base_dir.back() == '/') base_dir.pop_back();
+  double fg_min = 1e10, fg_max = -1e10, p0_min = 1e10, p0_max = -1e10, T_min = 1e10, T_max = -1e10;
+  crp_focus_state carry{};
+  for (int pass = 0; pass < num_iters; pass++) {
+    if (num_iters > 1 && dir_given) target_dir = base_dir + "_" + std::string(pass + 1, 'I') + "/";
+    std::error_code ec;
+    std::filesystem::create_directories(target_dir, ec);
+    if (ec) {
+      std::cerr << "error: cannot create " << target_dir << ": " << ec.message() << std::endl;
+      return 1;
+    }
+    crp_sim* sim = nullptr;
+    st = crp_create(&cfg, nullptr, nullptr, &sim);
+    if (st != CRP_OK) {
+      std::cerr << "error: " << crp_status_string(st) << std::endl;
+      return 1;
+    }
+    if (pass > 0) crp_set_focus_state(sim, &carry);
+    // Progress line as the reference prints it at each save (src/bubbles.cpp:258-268).
+    struct Progress {
+      const crp_config* cfg;
+    } prog{&cfg};
+    crp_output_plan plan{};
+    plan.save_interval = cfg.sim_save_interval > 0 ? cfg.sim_save_interval : 0;
+    // As solve_bubbles: SPH when -s is given, else text rawdata when -a is
+    // (src/bubble_CUDA.cu:398-411).
+    plan.dir = (sph || ascii) ? target_dir.c_str() : nullptr;
+    plan.sph = sph ? 1 : 0;
+    plan.user = &prog;
+    plan.progress = [](int64_t step, double time, void* user) {
+      const crp_config* c = ((Progress*)user)->cfg;
+      if (c->sim_n_step_max != 0)
+        printf("\rRunning the simulation...\t\tnstep : %5lld / %i\t", (long long)step, c->sim_n_step_max);
+      else
+        printf("\rRunning the simulation...\t\ttstep : %4.2E / %4.2E\t", time, c->sim_t_step_max);
+      fflush(stdout);
+    };
+    st = crp_run(sim, &plan, &cfg);
+    if (st != CRP_OK) {
+      crp_stats stats;
+      crp_get_stats(sim, &stats);
+      std::cerr << "\nerror at step " << stats.steps + 1 << ": " << crp_status_string(st) << ": "
+                << crp_last_error(sim) << std::endl;
+      crp_destroy(sim);
+      return 1;
+    }
+    printf("\rRunning the simulation...\t\tdone\n\n");
 
-  crp_sim* sim = nullptr;
-  st = crp_create(&cfg, nullptr, nullptr, &sim);
-  if (st != CRP_OK) {
-    std::cerr << "error: " << crp_status_string(st) << std::endl;
-    return 1;
-  }
-  // Progress line as the reference prints it at each save (src/bubbles.cpp:258-268).
-  struct Progress {
-    const crp_config* cfg;
-  } prog{&cfg};
-  crp_output_plan plan{};
-  plan.save_interval = cfg.sim_save_interval > 0 ? cfg.sim_save_interval : 0;
-  // As solve_bubbles: SPH when -s is given, else text rawdata when -a is
-  // (src/bubble_CUDA.cu:398-411).
-  plan.dir = (sph || ascii) ? target_dir.c_str() : nullptr;
-  plan.sph = sph ? 1 : 0;
-  plan.user = &prog;
-  plan.progress = [](int64_t step, double time, void* user) {
-    const crp_config* c = ((Progress*)user)->cfg;
-    if (c->sim_n_step_max != 0)
-      printf("\rRunning the simulation...\t\tnstep : %5lld / %i\t", (long long)step, c->sim_n_step_max);
-    else
-      printf("\rRunning the simulation...\t\ttstep : %4.2E / %4.2E\t", time, c->sim_t_step_max);
-    fflush(stdout);
-  };
-  st = crp_run(sim, &plan, &cfg);
-  if (st != CRP_OK) {
-    crp_stats stats;
-    crp_get_stats(sim, &stats);
-    std::cerr << "\nerror at step " << stats.steps + 1 << ": " << crp_status_string(st) << ": " << crp_last_error(sim)
-              << std::endl;
+    // focalpoint_actual_T.txt and focalpoint_controller_T.txt (src/bubbles.cpp:258-270),
+    // written when the tracker ran (debug.T or transducer.pid).
+    const int64_t nf = crp_focus_history(sim, 0, nullptr, 0), nc = crp_focus_history(sim, 1, nullptr, 0);
+    if (nf > 0) {
+      std::vector<double> f((size_t)nf), c((size_t)nc);
+      crp_focus_history(sim, 0, f.data(), nf);
+      crp_focus_history(sim, 1, c.data(), nc);
+      std::ofstream fa((target_dir + "focalpoint_actual_T.txt").c_str());
+      for (int64_t k = 0; k < nf; k++) fa << k << "\t" << f[(size_t)k] << std::endl;
+      std::ofstream fc((target_dir + "focalpoint_controller_T.txt").c_str());
+      for (int64_t k = 0; k < nc; k++) fc << k + cfg.tr_pid_start_step << "\t" << c[(size_t)k] << std::endl;
+    }
+    crp_get_focus_state(sim, &carry);
+
+    // *_minmax.txt (src/bubbles.cpp:273-296), running over the passes.
+    double a0, a1, b0, b1;
+    crp_minmax(sim, &a0, &a1, &b0, &b1);
+    fg_min = std::min(fg_min, a0), fg_max = std::max(fg_max, a1), p0_min = std::min(p0_min, b0),
+    p0_max = std::max(p0_max, b1);
+    crp_minmax_T(sim, &a0, &a1);
+    T_min = std::min(T_min, a0), T_max = std::max(T_max, a1);
+    double v;
+    if (cfg.dbg_T) {
+      if (lookup_key(in_file, "debug.T_min", &v)) T_min = v;
+      if (lookup_key(in_file, "debug.T_max", &v)) T_max = v;
+      write_minmax(target_dir + "T_minmax.txt", T_min, T_max);
+    }
+    if (cfg.dbg_p) {
+      if (lookup_key(in_file, "debug.p_max", &v)) p0_max = v;
+      write_minmax(target_dir + "p0_minmax.txt", p0_min, p0_max);
+    }
+    if (cfg.dbg_fg) {
+      if (lookup_key(in_file, "debug.fg_min", &v)) fg_min = v;
+      if (lookup_key(in_file, "debug.fg_max", &v)) fg_max = v;
+      write_minmax(target_dir + "fg_minmax.txt", fg_min, fg_max);
+    }
     crp_destroy(sim);
-    return 1;
+    if (num_iters == 1)
+      std::cout << "The program took ";
+    else
+      std::cout << pass << " pass took ";
+    std::cout << time(nullptr) - start_time << " seconds to run" << std::endl;
+    std::ofstream runtime((target_dir + "runtime.txt").c_str());
+    runtime << "Finished in " << time(nullptr) - start_time << " seconds" << std::endl;
   }
-  printf("\rRunning the simulation...\t\tdone\n\n");
-
-  // *_minmax.txt (src/bubbles.cpp:273-296) for the fields written above.
-  double fg_min = 1e10, fg_max = -1e10, p0_min = 1e10, p0_max = -1e10;
-  crp_minmax(sim, &fg_min, &fg_max, &p0_min, &p0_max);
-  double v;
-  if (cfg.dbg_T) {
-    double T_min = 1e10, T_max = -1e10;
-    crp_minmax_T(sim, &T_min, &T_max);
-    if (lookup_key(in_file, "debug.T_min", &v)) T_min = v;
-    if (lookup_key(in_file, "debug.T_max", &v)) T_max = v;
-    write_minmax(target_dir + "T_minmax.txt", T_min, T_max);
-  }
-  if (cfg.dbg_p) {
-    if (lookup_key(in_file, "debug.p_max", &v)) p0_max = v;
-    write_minmax(target_dir + "p0_minmax.txt", p0_min, p0_max);
-  }
-  if (cfg.dbg_fg) {
-    if (lookup_key(in_file, "debug.fg_min", &v)) fg_min = v;
-    if (lookup_key(in_file, "debug.fg_max", &v)) fg_max = v;
-    write_minmax(target_dir + "fg_minmax.txt", fg_min, fg_max);
-  }
-  crp_destroy(sim);
-  std::cout << "The program took " << time(nullptr) - start_time << " seconds to run" << std::endl;
-  std::ofstream runtime((target_dir + "runtime.txt").c_str());
-  runtime << "Finished in " << time(nullptr) - start_time << " seconds" << std::endl;
   return 0;
 }

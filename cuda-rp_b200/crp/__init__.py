@@ -67,6 +67,11 @@ class Stats(ctypes.Structure):
 PROGRESS = ctypes.CFUNCTYPE(None, ctypes.c_int64, c_dbl, ctypes.c_void_p)
 
 
+class FocusState(ctypes.Structure):
+    _fields_ = [("control_x", c_dbl), ("control_y", c_dbl), ("err_total_x", c_dbl), ("err_total_y", c_dbl),
+                ("d_err_x", c_dbl), ("d_err_y", c_dbl), ("filter_in", c_dbl * 5), ("filter_out", c_dbl * 5)]
+
+
 class OutputPlan(ctypes.Structure):
     _fields_ = [("n_steps", ctypes.c_int64), ("t_max", c_dbl), ("save_interval", c_int),
                 ("dir", ctypes.c_char_p), ("sph", c_int), ("progress", PROGRESS), ("user", ctypes.c_void_p)]
@@ -141,6 +146,9 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "crp_void_fraction_noalloc_scratch": (ctypes.c_size_t, [c_int, c_int, c_int]),
         "crp_void_fraction_noalloc": (c_int, [P(Config), c_int, vp, vp, vp, vp, vp, vp]),
         "crp_run": (c_int, [vp, P(OutputPlan), P(Config)]),
+        "crp_focus_history": (ctypes.c_int64, [vp, c_int, vp, ctypes.c_int64]),
+        "crp_get_focus_state": (c_int, [vp, P(FocusState)]),
+        "crp_set_focus_state": (c_int, [vp, P(FocusState)]),
         "crp_batch_create": (c_int, [c_int, P(Config), P(BubblesIn), P(vp)]),
         "crp_batch_run": (c_int, [vp, P(c_int), c_int, P(c_int)]),
         "crp_batch_count": (c_int, [vp]),
@@ -248,6 +256,23 @@ class Sim:
         plan = OutputPlan(n_steps, t_max, save_interval, directory.encode() if directory else None, 0, cb, None)
         cfg = self._keep[0]
         self._check(self.lib.crp_run(self.h, ctypes.byref(plan), ctypes.byref(cfg) if cfg is not None else None))
+
+    def focus_history(self, which: str = "actual") -> np.ndarray:
+        """Tracked focal depths ("actual") or control depths ("control")."""
+        w = 0 if which == "actual" else 1
+        n = self.lib.crp_focus_history(self.h, w, None, 0)
+        out = np.zeros(max(n, 0))
+        if n > 0:
+            self.lib.crp_focus_history(self.h, w, _ptr(out), n)
+        return out
+
+    def focus_state(self) -> FocusState:
+        st = FocusState()
+        self._check(self.lib.crp_get_focus_state(self.h, ctypes.byref(st)))
+        return st
+
+    def set_focus_state(self, st: FocusState):
+        self._check(self.lib.crp_set_focus_state(self.h, ctypes.byref(st)))
 
     def write_sph(self, directory: str):
         self._check(self.lib.crp_write_sph(self.h, directory.encode()))

@@ -796,6 +796,7 @@ __global__ void __launch_bounds__(kRpThreads, kRpMinBlocks) bubble_rp(const __gr
 // Work order for the next radius solves: bubbles bucketed by the binary
 // logarithm of their last sub-step count, heaviest bucket first.
 constexpr int kLptBuckets = 32;
+constexpr long long kLptMinSubsteps = 12;  // the quiet phase takes 10 (dt0 = dt / 10)
 
 __device__ __forceinline__ int lpt_bucket(int nsub) {
   return kLptBuckets - 1 - min(kLptBuckets - 1, 31 - __clz(max(nsub, 1)));
@@ -989,6 +990,7 @@ __global__ void heat_contrib(const __grid_constant__ GridParams g, const __grid_
 
 struct TempArgs {
   F64 T_old, T_new;
+  double* dT;           // if set: the step's temperature increment (the focal tracker's input)
   const int* start;
   const int* idx;
   const double* hc;     // heat contributions (heat_contrib)
@@ -1030,7 +1032,9 @@ __global__ void __launch_bounds__(256) temperature_step(const __grid_constant__ 
   const double s2 = (eyu - eyd) * g.rdy;
   const double rho_m = t.rho_const ? g.rho_inf : (1.0 - fgn.get(k)) * g.rho_inf;
   const double cpm = heat_capacity_water(Tc + t.T_inf);
-  t.T_new.put(k, Tc + g.dt * (s1 + s2 + Q) / (rho_m * cpm));
+  const double dT = g.dt * (s1 + s2 + Q) / (rho_m * cpm);
+  t.T_new.put(k, Tc + dT);
+  if (t.dT) t.dT[k] = dT;
 }
 
 // MixtureBoundaryTemperatureKernel (:1065-1102) as one block: the old ghost
@@ -1104,6 +1108,86 @@ struct Profiler {
     for (cudaEvent_t e : ev) cudaEventDestroy(e);
   }
 };
+
+// ---------------------------------------------------------------------------
+// Focal tracker (determine_focal_point, inc/bubble_CUDA_kernel.cuh:1132-1166).
+// The reference reduces the Work array (the step's temperature increment) with
+// functors of a header that its source tree does not contain, so their exact
+// weighting is unknown; here the focal depth is the centroid, over the
+// interior cells, of the increment's excess over half of its maximum:
+//   y_f = sum(w (j - 1/2) dy) / sum(w),  w = max(dT - max(dT) / 2, 0),
+// a weight that goes to zero continuously at the half maximum, so rounding
+// differences move y_f by rounding amounts (a hard cut would flip cells in
+// and out of the region),
+// and y_f = 0 while max(dT) <= kFocalFloor: increments of rounding size (the
+// prediction's multiply-adds leave ~1e-40 K where nothing heats) define no focus.
+// Three launches, each in a fixed order, so the result is the same run to run.
+constexpr int kFocalBlocks = 148, kFocalThreads = 256;
+constexpr double kFocalFloor = 1.0e-30;  // K per step
+
+__device__ __forceinline__ double block_sum_fixed(double v, double* sh) {
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kFocalThreads) focal_max(const double* __restrict__ dT, const Frame f,
+                                                            double* __restrict__ part) {
+  __shared__ double sh[kFocalThreads];
+  double m = -1.0e300;
+  for (int j = 1 + blockIdx.x; j <= f.Y; j += gridDim.x)
+    for (int i = 1 + threadIdx.x; i <= f.X; i += blockDim.x) m = fmax(m, dT[f.idx(i, j)]);
+  sh[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void __launch_bounds__(kFocalThreads) focal_sums(const double* __restrict__ dT, const Frame f, double dy,
+                                                             const double* __restrict__ pmax, int nparts,
+                                                             double* __restrict__ part2) {
+  __shared__ double sh[kFocalThreads];
+  double mx = -1.0e300;
+  for (int k = 0; k < nparts; k++) mx = fmax(mx, pmax[k]);
+  const double thr = 0.5 * mx;
+  double sw = 0.0, swy = 0.0;
+  if (mx > kFocalFloor)
+    for (int j = 1 + blockIdx.x; j <= f.Y; j += gridDim.x) {
+      const double y = ((double)j - 0.5) * dy;
+      for (int i = 1 + threadIdx.x; i <= f.X; i += blockDim.x) {
+        const double v = dT[f.idx(i, j)] - thr;
+        if (v > 0.0) {
+          sw += v;
+          swy += v * y;
+        }
+      }
+    }
+  sw = block_sum_fixed(sw, sh);
+  swy = block_sum_fixed(swy, sh);
+  if (threadIdx.x == 0) {
+    part2[2 * blockIdx.x] = sw;
+    part2[2 * blockIdx.x + 1] = swy;
+  }
+}
+
+__global__ void focal_final(const double* __restrict__ part2, int nparts, double* __restrict__ out) {
+  double sw = 0.0, swy = 0.0;
+  for (int k = 0; k < nparts; k++) {
+    sw += part2[2 * k];
+    swy += part2[2 * k + 1];
+  }
+  out[0] = sw;
+  out[1] = swy;
+}
 
 // ---------------------------------------------------------------------------
 // Device-resident step state.  The host path reads it after each residual
@@ -1343,6 +1427,15 @@ struct Sim {
   void* Tbuf[2] = {nullptr, nullptr};
   int cur_t = 0;
   double* heat = nullptr;
+  // Focal tracker and PID focus control (src/bubble_CUDA.cu:123-153, 310-352),
+  // run with the temperature branch: the step's temperature increment, the
+  // reduction partials, the tracked and controlled focal depths, the
+  // Butterworth filter's state and the PID accumulators.
+  double* dTbuf = nullptr;
+  double* focal_part = nullptr;
+  double* h_focal = nullptr;  // pinned {sum w, sum w y}
+  std::vector<double> focal_hist, control_hist;
+  crp_focus_state focus{};
   bool graphs_on = true;     // ext: off runs every step from the host
   Scalars* h_push = nullptr;  // pinned staging of the host state for the graph path
   bool debug_picard = std::getenv("CRP_DEBUG_PICARD") != nullptr;  // residual of every Picard iteration to stderr
@@ -1385,8 +1478,11 @@ struct Sim {
       py[k] = carve<double>(cells, off, dry);
     }
     for (int k = 0; k < 3; k++) fg[k] = carve<double>(cells, off, dry);
-    if (temperature_on)
+    if (temperature_on) {
       for (int k = 0; k < 2; k++) Tbuf[k] = carve<double>(cells, off, dry);
+      dTbuf = carve<double>(cells, off, dry);
+      focal_part = carve<double>(3 * kFocalBlocks + 2, off, dry);
+    }
     scratch = carve<double>((size_t)(f.X + 2) * (f.Y + 2), off, dry);
     d_sigma = carve<double>(hs.sigma_block.size(), off, dry);
     d_scalars = carve<Scalars>(1, off, dry);
@@ -1448,7 +1544,9 @@ struct Sim {
     mixed = cfg.ext_precision == CRP_PREC_MIXED;
     picard_tol = cfg.ext_picard_tol > 0.0 ? cfg.ext_picard_tol : (mixed ? 1.0e-5 : (double)1.0e-7f);
     graphs_on = cfg.ext_graphs != 0;
-    temperature_on = cfg.dbg_T != 0;
+    // The focal tracker reads the temperature increment, so the PID controller
+    // turns the temperature branch on (its output stays governed by debug.T).
+    temperature_on = cfg.dbg_T != 0 || cfg.tr_pid != 0;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CRP_ERR_NO_DEVICE, "no CUDA device");
     if (user_stream) {
@@ -1465,6 +1563,13 @@ struct Sim {
     layout(false);
     CRP_CUDA(cudaMemsetAsync(pool, 0, pool_bytes, stream));
     CRP_CUDA(cudaMallocHost(&h_scalars, sizeof(Scalars)));
+    CRP_CUDA(cudaMallocHost(&h_focal, 2 * sizeof(double)));
+    // Control system start (src/bubble_CUDA.cu:123-153): the first tracked
+    // point is (0, 0); the first control point is the focus the source uses.
+    focal_hist.assign(1, 0.0);
+    control_hist.assign(1, gp.ctl_y);
+    focus.control_x = gp.ctl_x;
+    focus.control_y = gp.ctl_y;
     {
       int dev = 0, sms = 0, per_sm = 0;
       CRP_CUDA(cudaGetDevice(&dev));
@@ -1487,6 +1592,12 @@ struct Sim {
       auto up = [&](double* d, const std::vector<double>& h) {
         return cudaMemcpyAsync(d, h.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream);
       };
+      {
+        std::vector<int> ident(n);
+        for (int k = 0; k < n; k++) ident[k] = k;
+        CRP_CUDA(cudaMemcpyAsync(lpt.order, ident.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
+        CRP_CUDA(cudaStreamSynchronize(stream));
+      }
       CRP_CUDA(up(bub.x, hs.bx));
       CRP_CUDA(up(bub.y, hs.by));
       CRP_CUDA(up(bub.R0, hs.r0));
@@ -1699,10 +1810,12 @@ struct Sim {
     couple_box = box_union(box_union(bnow, supp[0]), box_union(supp[1], supp[2]));
     if (hs.nb > 0 && resimax > picard_tol) {
       // Bins change only when a bubble crosses into another cell; the solve
-      // order follows the latest sub-step counts.
+      // order follows the latest sub-step counts, and is left as it is while
+      // no bubble has needed more than kLptMinSubsteps sub-steps (all equal:
+      // the order cannot shorten the launch).
       if (bins_stale) CRP_CUDA(build_bins());
       bins_stale = false;
-      CRP_CUDA(build_order());
+      if (h_scalars->substep_max > kLptMinSubsteps) CRP_CUDA(build_order());
     }
     if (hs.nb > 0) {
       double prev = resimax;
@@ -1727,7 +1840,11 @@ struct Sim {
       }
     }
     if (std::isnan(resimax)) return fail(CRP_ERR_NONFINITE, "non-finite pressure");
-    if (temperature_on) CRP_CUDA(mixed ? launch_temperature<PrecMixed>() : launch_temperature<PrecFP64>());
+    if (temperature_on) {
+      CRP_CUDA(mixed ? launch_temperature<PrecMixed>() : launch_temperature<PrecFP64>());
+      const crp_status fs = track_focus(stats.steps + 1);
+      if (fs != CRP_OK) return fs;
+    }
     // Support of this step's void fraction: the gather's when it ran, else the
     // prediction's.
     const Box snow = loop > 0 ? bnow : box_union(supp[0], box_union(supp[1], supp[2]));
@@ -2111,6 +2228,71 @@ struct Sim {
     return launch(kClassOther, [&] { vghost<V><<<(ng + 255) / 256, 256, 0, stream>>>(gp, vxn, vyn); });
   }
 
+  // Fourth-order Butterworth low-pass of the tracked depth (filter_loop,
+  // inc/bubble_CUDA_kernel.cuh:117-129), with this simulation's state.
+  double filter_depth(double input) {
+    double* xv = focus.filter_in;
+    double* yv = focus.filter_out;
+    const double gain = 6.522112693e+08;
+    xv[0] = xv[1];
+    xv[1] = xv[2];
+    xv[2] = xv[3];
+    xv[3] = xv[4];
+    xv[4] = input / gain;
+    yv[0] = yv[1];
+    yv[1] = yv[2];
+    yv[2] = yv[3];
+    yv[3] = yv[4];
+    yv[4] = (xv[0] + xv[4]) + 4 * (xv[1] + xv[3]) + 6 * xv[2] + (-0.9676955438 * yv[0]) + (3.9025587848 * yv[1]) +
+            (-5.9020258615 * yv[2]) + (3.9671625959 * yv[3]);
+    return yv[4];
+  }
+
+  // After the temperature step: the focal depth, its filtered value and, with
+  // transducer.pid, the next focus of the source (focal_PID and the clamp of
+  // src/bubble_CUDA.cu:328-347, inc/bubble_CUDA_kernel.cuh:1168-1184).
+  crp_status track_focus(int64_t nstep) {
+    double* part = focal_part;
+    CRP_CUDA(launch(kClassOther, [&] {
+      focal_max<<<kFocalBlocks, kFocalThreads, 0, stream>>>(dTbuf, gp.f, part);
+    }));
+    CRP_CUDA(launch(kClassOther, [&] {
+      focal_sums<<<kFocalBlocks, kFocalThreads, 0, stream>>>(dTbuf, gp.f, gp.dy, part, kFocalBlocks,
+                                                              part + kFocalBlocks);
+    }));
+    CRP_CUDA(launch(kClassOther, [&] {
+      focal_final<<<1, 1, 0, stream>>>(part + kFocalBlocks, kFocalBlocks, part + 3 * kFocalBlocks);
+    }));
+    CRP_CUDA(cudaMemcpyAsync(h_focal, part + 3 * kFocalBlocks, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CRP_CUDA(cudaStreamSynchronize(stream));
+    const double depth = h_focal[0] > 0.0 ? h_focal[1] / h_focal[0] : 0.0;
+    focal_hist.push_back(filter_depth(depth));
+    if (cfg.tr_pid && nstep > cfg.tr_pid_start_step) {
+      const double K = 0.2 * 0.60, Pc = 1000.0, D = K * 0.125 * Pc, I = K / (0.5 * Pc);
+      const double tx = hs.d.fpx, ty = hs.d.fpy;
+      const double ax = 0.0, ay = focal_hist[focal_hist.size() - 1];
+      const double px_ = 0.0, py_ = focal_hist[focal_hist.size() - 2];
+      const double ex = tx - ax, ey = ty - ay;
+      focus.err_total_x += ex;
+      focus.err_total_y += ey;
+      focus.d_err_x = px_ - ax;
+      focus.d_err_y = py_ - ay;
+      double cy = ty + (K * ey + D * focus.d_err_y + I * focus.err_total_y);
+      cy = cy < ty ? ty : (cy > cfg.grid_ly ? cfg.grid_ly : cy);
+      control_hist.push_back(cy);
+      set_control(0.0, cy);
+    }
+    return CRP_OK;
+  }
+
+  void set_control(double cx, double cy) {
+    focus.control_x = cx;
+    focus.control_y = cy;
+    gp.ctl_x = cx;
+    gp.ctl_y = cy;
+    gp.focal_dist = cy / 0.5 / std::sqrt(3.0);
+  }
+
   // calculate_temperature after the Picard loop: the bins must follow the
   // bubbles' current cells for the heat gather.
   template <typename P>
@@ -2132,6 +2314,7 @@ struct Sim {
     TempArgs ta;
     ta.T_old = F64{(double*)Tbuf[cur_t]};
     ta.T_new = F64{(double*)Tbuf[cur_t ^ 1]};
+    ta.dT = dTbuf;
     ta.start = bins.start;
     ta.idx = bins.idx;
     ta.hc = heat;
@@ -2236,6 +2419,7 @@ struct Sim {
     if (h_push) cudaFreeHost(h_push);
     if (pool) cudaFree(pool);
     if (h_scalars) cudaFreeHost(h_scalars);
+    if (h_focal) cudaFreeHost(h_focal);
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
 };
@@ -2411,6 +2595,32 @@ crp_status crp_read_field(crp_sim* h, crp_field f, double* host) {
 crp_status crp_read_bubbles(crp_sim* h, crp_bubble_field w, double* host) {
   if (!h || !host) return CRP_ERR_INVALID;
   return h->s.read_bubbles(w, host);
+}
+
+int64_t crp_focus_history(const crp_sim* h, int32_t which, double* out, int64_t capacity) {
+  if (!h || (which != 0 && which != 1)) return -1;
+  const std::vector<double>& v = which == 0 ? h->s.focal_hist : h->s.control_hist;
+  if (!h->s.temperature_on) return 0;
+  for (int64_t k = 0; out && k < capacity && k < (int64_t)v.size(); k++) out[k] = v[k];
+  return (int64_t)v.size();
+}
+
+crp_status crp_get_focus_state(const crp_sim* h, crp_focus_state* st) {
+  if (!h || !st) return CRP_ERR_INVALID;
+  *st = h->s.focus;
+  return CRP_OK;
+}
+
+crp_status crp_set_focus_state(crp_sim* h, const crp_focus_state* st) {
+  if (!h || !st) return CRP_ERR_INVALID;
+  if (h->s.stats.steps != 0) return CRP_ERR_INVALID;
+  h->s.focus = *st;
+  if (h->s.cfg.tr_pid) {
+    // A carried-over control point replaces the initial one (pid_init).
+    h->s.set_control(st->control_x, st->control_y);
+    h->s.control_hist.assign(1, st->control_y);
+  }
+  return CRP_OK;
 }
 
 crp_status crp_minmax_T(const crp_sim* h, double* T_min, double* T_max) {

@@ -276,6 +276,34 @@ size_t crp_void_fraction_noalloc_scratch(int32_t grid_x, int32_t grid_y, int32_t
 crp_status crp_void_fraction_noalloc(const crp_config* cfg, int32_t n, const double* x, const double* y,
                                      const double* r, const double* n_b, double* f_g, void* stream);
 
+/* Focal tracker and PID focus control (src/bubble_CUDA.cu:123-153, 310-352;
+ * inc/bubble_CUDA_kernel.cuh:117-129, 1132-1184).  They run with the
+ * temperature branch (debug.T = 1, or transducer.pid = 1, which turns the
+ * branch on).  After every step the focal depth is tracked from the step's
+ * temperature increment dT: the reference's reduction functors are missing
+ * from its source tree, so the depth is defined here as the mean of the
+ * cell-centre depths (j - 1/2) dy over the interior cells weighted by
+ * max(dT - max(dT) / 2, 0) (0 while max(dT) <= 1e-30 K: increments of
+ * rounding size define no focus).  It passes through the
+ * reference's fourth-order Butterworth low-pass.  With transducer.pid, after
+ * step pid_start_step the PID of focal_PID moves the focus the source aims at
+ * (clamped to [focal depth, LY]).
+ * crp_focus_history copies the tracked depths (which = 0, the reference's
+ * focalpoint[].y, starting with 0) or the control depths (which = 1, its
+ * control[].y, starting with the initial focus) and returns how many there are
+ * (at most capacity are copied).  crp_get/set_focus_state carry the control
+ * point, the PID accumulators and the filter state from one simulation to the
+ * next (transducer.pid_iterate passes); set it before the first step. */
+typedef struct crp_focus_state {
+  double control_x, control_y;        /* focus the source aims at (focal_point_c) */
+  double err_total_x, err_total_y;    /* PID accumulated error */
+  double d_err_x, d_err_y;            /* PID last derivative term */
+  double filter_in[5], filter_out[5]; /* Butterworth filter history */
+} crp_focus_state;
+int64_t crp_focus_history(const crp_sim* sim, int32_t which, double* out, int64_t capacity);
+crp_status crp_get_focus_state(const crp_sim* sim, crp_focus_state* state);
+crp_status crp_set_focus_state(crp_sim* sim, const crp_focus_state* state);
+
 /* Main loop with saves (src/bubble_CUDA.cu:203-438): step while
  * (n_steps != 0 && steps < n_steps) || (t_max != 0 && time < t_max); after
  * every save_interval-th step write rawdata to dir (if not NULL) and call

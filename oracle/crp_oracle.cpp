@@ -373,6 +373,11 @@ struct crpo_sim {
   // window, the energy fluxes Ex / Ey, and the reference's Work array.
   bool temperature_on = false;
   Field T, k_m, C_pm, Ex, Ey, twork;
+  // Focal tracker and PID (src/bubble_CUDA.cu:123-153, 310-352): tracked and
+  // controlled focal depths, Butterworth state, PID accumulators.
+  std::vector<double> focal_hist, control_hist;
+  double filt_in[5] = {0, 0, 0, 0, 0}, filt_out[5] = {0, 0, 0, 0, 0};
+  double pid_cum_y = 0.0, pid_der_y = 0.0;
   // Bubble state, bubble_t (inc/bubble_CUDA.h:172-189), structure of arrays.
   int nb = 0;
   std::vector<BubConst> bc;
@@ -456,7 +461,9 @@ struct crpo_sim {
     fgn = fg;
     fgm = fg;
     work = fg;
-    temperature_on = c.dbg_T != 0;
+    temperature_on = c.dbg_T != 0 || c.tr_pid != 0;
+    focal_hist.assign(1, 0.0);
+    control_hist.assign(1, d.ctly);
     if (temperature_on) {
       T.init(a.ista2m, a.iend2m, a.jsta2m, a.jend2m, 0.0);
       k_m = T;
@@ -860,6 +867,57 @@ struct crpo_sim {
       }
   }
 
+  // Focal depth of the step (determine_focal_point, inc/bubble_CUDA_kernel.cuh:
+  // 1132-1166, whose reduction functors are not in the reference's tree): the
+  // mean of the cell-centre depths weighted by the temperature increment's
+  // excess over half its maximum, over the interior cells (0 while the maximum
+  // is at most 1e-30 K, rounding size); then filter_loop
+  // (:117-129) and, with transducer.pid, focal_PID and the clamp
+  // (src/bubble_CUDA.cu:328-347, inc/bubble_CUDA_kernel.cuh:1168-1184).
+  void track_focus() {
+    double mx = -1.0e300;
+    for (int j = a.jstam; j <= a.jendm; j++)
+      for (int i = a.istam; i <= a.iendm; i++) mx = std::max(mx, twork.at(i, j));
+    double sw = 0.0, swy = 0.0;
+    if (mx > 1.0e-30) {  // rounding-size increments define no focus
+      const double thr = 0.5 * mx;
+      for (int j = a.jstam; j <= a.jendm; j++) {
+        const double y = ((double)j - 0.5) * d.dy;
+        for (int i = a.istam; i <= a.iendm; i++) {
+          const double v = twork.at(i, j) - thr;
+          if (v > 0.0) {
+            sw += v;
+            swy += v * y;
+          }
+        }
+      }
+    }
+    const double depth = sw > 0.0 ? swy / sw : 0.0;
+    double* xv = filt_in;
+    double* yv = filt_out;
+    const double gain = 6.522112693e+08;
+    for (int k = 0; k < 4; k++) xv[k] = xv[k + 1];
+    xv[4] = depth / gain;
+    for (int k = 0; k < 4; k++) yv[k] = yv[k + 1];
+    yv[4] = (xv[0] + xv[4]) + 4 * (xv[1] + xv[3]) + 6 * xv[2] + (-0.9676955438 * yv[0]) + (3.9025587848 * yv[1]) +
+            (-5.9020258615 * yv[2]) + (3.9671625959 * yv[3]);
+    focal_hist.push_back(yv[4]);
+    if (cfg.tr_pid && nstep > cfg.tr_pid_start_step) {
+      const double K = 0.2 * 0.60, Pc = 1000.0, D = K * 0.125 * Pc, I = K / (0.5 * Pc);
+      const double ty = d.fpy;
+      const double ay = focal_hist[focal_hist.size() - 1], py = focal_hist[focal_hist.size() - 2];
+      const double ey = ty - ay;
+      pid_cum_y += ey;
+      pid_der_y = py - ay;
+      double cy = ty + (K * ey + D * pid_der_y + I * pid_cum_y);
+      cy = cy < ty ? ty : (cy > cfg.grid_ly ? cfg.grid_ly : cy);
+      control_hist.push_back(cy);
+      d.ctlx = 0.0;
+      d.ctly = cy;
+      d.focal_dist = cy / 0.5 / std::sqrt(3.0);
+    }
+  }
+
   // calculate_temperature (inc/bubble_CUDA_kernel.cuh:1347-1376).
   void temperature() {
     // Work cleared, then BubbleHeatKernel (:972-1007), bubble by bubble.
@@ -943,7 +1001,10 @@ struct crpo_sim {
         resimax = pressure();
       }
     }
-    if (temperature_on) temperature();
+    if (temperature_on) {
+      temperature();
+      track_focus();
+    }
     properties();
     stats.steps = nstep;
     stats.time = tstep;
@@ -1004,6 +1065,14 @@ crp_status crpo_get_stats(const crpo_sim* s, crp_stats* st) {
   if (!s || !st) return CRP_ERR_INVALID;
   *st = s->stats;
   return CRP_OK;
+}
+
+int64_t crpo_focus_history(const crpo_sim* s, int32_t which, double* out, int64_t capacity) {
+  if (!s || (which != 0 && which != 1)) return -1;
+  if (!s->temperature_on) return 0;
+  const std::vector<double>& v = which == 0 ? s->focal_hist : s->control_hist;
+  for (int64_t k = 0; out && k < capacity && k < (int64_t)v.size(); k++) out[k] = v[k];
+  return (int64_t)v.size();
 }
 
 crp_status crpo_read_field(crpo_sim* s, crp_field f, double* host) {

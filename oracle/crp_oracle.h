@@ -30,6 +30,7 @@ crp_status crpo_step(crpo_sim* sim, int32_t n);
 crp_status crpo_get_dims(const crpo_sim* sim, crp_dims* dims);
 crp_status crpo_get_stats(const crpo_sim* sim, crp_stats* stats);
 crp_status crpo_read_field(crpo_sim* sim, crp_field field, double* host);
+int64_t crpo_focus_history(const crpo_sim* sim, int32_t which, double* out, int64_t capacity);
 crp_status crpo_read_bubbles(crpo_sim* sim, crp_bubble_field what, double* host);
 /* Number of OpenMP threads the oracle uses (0 = library default). */
 void crpo_set_threads(int32_t n);

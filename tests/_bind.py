@@ -37,6 +37,7 @@ def oracle_lib():
             "crpo_get_dims": (ctypes.c_int32, [vp, P(crp.Dims)]),
             "crpo_get_stats": (ctypes.c_int32, [vp, P(crp.Stats)]),
             "crpo_read_field": (ctypes.c_int32, [vp, ctypes.c_int32, vp]),
+            "crpo_focus_history": (ctypes.c_int64, [vp, ctypes.c_int32, vp, ctypes.c_int64]),
             "crpo_read_bubbles": (ctypes.c_int32, [vp, ctypes.c_int32, vp]),
             "crpo_set_threads": (None, [ctypes.c_int32]),
             "crpo_get_threads": (ctypes.c_int32, []),
@@ -87,6 +88,14 @@ class OracleSim:
         out = np.empty(crp.field_shape(self.dims, name))
         st = self.lib.crpo_read_field(self.h, crp.FIELDS[name], _ptr(out))
         assert st == 0
+        return out
+
+    def focus_history(self, which="actual"):
+        w = 0 if which == "actual" else 1
+        n = self.lib.crpo_focus_history(self.h, w, None, 0)
+        out = np.zeros(max(n, 0))
+        if n > 0:
+            self.lib.crpo_focus_history(self.h, w, _ptr(out), n)
         return out
 
     def bubbles(self, name):

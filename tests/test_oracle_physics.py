@@ -129,3 +129,45 @@ def test_pml_absorbs():
     r_wall = reflected(0)
     assert r_wall > 0.5
     assert r_pml < 0.05 * r_wall, (r_pml, r_wall)
+
+
+def test_focus_tracker_and_pid_histories():
+    """Focal tracker and PID (src/bubble_CUDA.cu:123-153, 310-352) in the oracle:
+    one tracked depth per step after the initial 0; one control depth per step
+    after transducer.pid_start_step, each clamped to [focus depth, LY]; the
+    source's focus follows the last control depth."""
+    import math
+
+    cfg = B.small_config(tr_pid=1, tr_pid_start_step=10)
+    o = B.OracleSim(cfg)
+    o.step(40)
+    a, c = o.focus_history("actual"), o.focus_history("control")
+    fpy = cfg.tr_focal_dist * math.sqrt(3.0) / 2
+    assert len(a) == 41 and a[0] == 0.0
+    assert len(c) == 1 + 30
+    assert abs(c[0] - fpy) < 1e-15
+    assert np.all(c >= fpy - 1e-15) and np.all(c <= cfg.grid_ly)
+    assert c[-1] != c[0]
+    # Without the controller the focus stays where the source aims it.
+    o2 = B.OracleSim(B.small_config())
+    o2.step(20)
+    assert len(o2.focus_history("actual")) == 21 and len(o2.focus_history("control")) == 1
+
+
+def test_butterworth_filter_settles_to_its_dc_gain():
+    """filter_loop's coefficients (inc/bubble_CUDA_kernel.cuh:117-129): a
+    constant input settles to 16 / gain / (1 - sum of the feedback
+    coefficients) = 0.99723 of itself (the coefficients are rounded) within a
+    few thousand steps."""
+    xv, yv = [0.0] * 5, [0.0] * 5
+    gain = 6.522112693e+08
+    out = 0.0
+    for _ in range(20000):
+        xv = xv[1:] + [1.0 / gain]
+        yv = yv[1:] + [0.0]
+        yv[4] = ((xv[0] + xv[4]) + 4 * (xv[1] + xv[3]) + 6 * xv[2] + (-0.9676955438 * yv[0]) + (3.9025587848 * yv[1])
+                 + (-5.9020258615 * yv[2]) + (3.9671625959 * yv[3]))
+        out = yv[4]
+    dc = 16.0 / gain / (1.0 - (-0.9676955438 + 3.9025587848 - 5.9020258615 + 3.9671625959))
+    assert abs(dc - 0.99723) < 1e-5
+    assert abs(out - dc) < 1e-8

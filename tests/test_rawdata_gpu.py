@@ -97,6 +97,29 @@ def test_bubbles_program(tmp_path):
     assert (out / "runtime.txt").read_text().startswith("Finished in ")
     lo, hi = [float(v) for v in (out / "p0_minmax.txt").read_text().split()]
     assert lo <= hi
+    # The tracker ran with debug.T: one line per step plus the initial 0.
+    lines = (out / "focalpoint_actual_T.txt").read_text().splitlines()
+    assert len(lines) == steps + 1 and lines[0] == "0\t0"
+    assert (out / "focalpoint_controller_T.txt").read_text().splitlines() == [f"1\t{cfg.tr_focal_dist * 3 ** 0.5 / 2:g}"]
+
+
+def test_bubbles_program_pid_passes(tmp_path):
+    """transducer.pid_iterate = 2 with -d: two passes into <dir>_I/ and
+    <dir>_II/, the second starting from the first one's last control point."""
+    conf = tmp_path / "pid.conf"
+    text = tiny_conf_text().replace("[transducer]", "[transducer]\npid\t=\t1\npid_start_step\t=\t10\npid_iterate\t=\t2")
+    conf.write_text(text)
+    exe = os.path.join(ROOT, "cuda-rp_b200", "build", "bubbles")
+    r = subprocess.run([exe, "-d", str(tmp_path / "out"), str(conf)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert "0 pass took" in r.stdout and "1 pass took" in r.stdout
+    ctl = []
+    for d in ("out_I", "out_II"):
+        rows = [ln.split("\t") for ln in (tmp_path / d / "focalpoint_controller_T.txt").read_text().splitlines()]
+        assert rows[0][0] == "10"
+        ctl.append([float(v) for _, v in rows])
+    assert len(ctl[0]) == 1 + STEPS - 10
+    assert abs(ctl[1][0] - ctl[0][-1]) <= 1e-5 * abs(ctl[0][-1])
 
 
 def test_run_writes_what_a_step_loop_writes(tmp_path):
