@@ -4,10 +4,10 @@
 //   bubbles [-h|--help] [--help-all] [-a|--ascii] [-s|--sph] [-d|--directory DIR] <input-file>
 //
 // Same options, configuration keys, defaults, output directory (./rawdata/),
-// rawdata files and *_minmax.txt / runtime.txt.  Differences, all outside the
-// simulated path: the output directory is created if missing and never cleared
-// (the reference runs `rm -rf` on it); SPH files, T_step files, the focal-point
-// tracker files and the PID passes are not produced (the run uses a fixed focus).
+// rawdata files (text or SPH, fg/p0/T/vx/vy), focal-point tracker files,
+// transducer.pid_iterate passes and *_minmax.txt / runtime.txt.  One difference,
+// outside the simulated path: the output directory is created if missing and
+// never cleared (the reference runs `rm -rf` on it, src/output_styles.cpp:20).
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
