@@ -49,6 +49,17 @@ struct GridParams {
   const double* ny;
   const double* xu;
   const double* rxp;
+  // PML update factors, 1 - s and 1 / (1 + s) (exactly 1 and 1 outside the
+  // PML): velocity faces vax/vbx[i+1], vay/vby[j+1] (s = dt c sigma / 2 of the
+  // face), pressure components pax/pbx[i], pay/pby[j] (s = dt c sigma_m / 2).
+  const double* vax;
+  const double* vbx;
+  const double* vay;
+  const double* vby;
+  const double* pax;
+  const double* pbx;
+  const double* pay;
+  const double* pby;
 };
 
 // bub_params_t scalars shared by every bubble (inc/bubble_CUDA.h:135-154); the
@@ -113,22 +124,33 @@ __device__ __forceinline__ bool source_value(const GridParams& g, bool pressure,
 // so no rounding error accumulates step to step.
 struct F64 {
   double* p;
-  __device__ __forceinline__ double get(long k) const { return p[k]; }
-  __device__ __forceinline__ void put(long k, double v) const { p[k] = v; }
+  template <typename K>
+  __device__ __forceinline__ double get(K k) const {
+    return p[k];
+  }
+  template <typename K>
+  __device__ __forceinline__ void put(K k, double v) const {
+    p[k] = v;
+  }
   // The value get() returns after put(v).
   __device__ static __forceinline__ double stored(double v) { return v; }
   // Asynchronous copy of element k into an 8-byte shared-memory slot, and the
   // value of a slot once the copy has landed.
-  __device__ __forceinline__ void stage(void* dst, long k) const { __pipeline_memcpy_async(dst, p + k, 8); }
+  template <typename K>
+  __device__ __forceinline__ void stage(void* dst, K k) const {
+    __pipeline_memcpy_async(dst, p + k, 8);
+  }
   __device__ static __forceinline__ double staged(const void* src) { return *(const double*)src; }
 };
 struct F32c {
   float2* p;  // (value, compensation) pairs, one 8-byte access per element
-  __device__ __forceinline__ double get(long k) const {
+  template <typename K>
+  __device__ __forceinline__ double get(K k) const {
     const float2 v = p[k];
     return (double)v.x + (double)v.y;
   }
-  __device__ __forceinline__ void put(long k, double v) const {
+  template <typename K>
+  __device__ __forceinline__ void put(K k, double v) const {
     const float h = (float)v;
     p[k] = make_float2(h, (float)(v - (double)h));
   }
@@ -136,7 +158,10 @@ struct F32c {
     const float h = (float)v;
     return (double)h + (double)(float)(v - (double)h);
   }
-  __device__ __forceinline__ void stage(void* dst, long k) const { __pipeline_memcpy_async(dst, p + k, 8); }
+  template <typename K>
+  __device__ __forceinline__ void stage(void* dst, K k) const {
+    __pipeline_memcpy_async(dst, p + k, 8);
+  }
   __device__ static __forceinline__ double staged(const void* src) {
     const float2 v = *(const float2*)src;
     return (double)v.x + (double)v.y;
@@ -145,10 +170,19 @@ struct F32c {
 // Void-fraction history of the mixed path: FP32 storage (sums are FP64).
 struct F32 {
   float* p;
-  __device__ __forceinline__ double get(long k) const { return (double)p[k]; }
-  __device__ __forceinline__ void put(long k, double v) const { p[k] = (float)v; }
+  template <typename K>
+  __device__ __forceinline__ double get(K k) const {
+    return (double)p[k];
+  }
+  template <typename K>
+  __device__ __forceinline__ void put(K k, double v) const {
+    p[k] = (float)v;
+  }
   __device__ static __forceinline__ double stored(double v) { return (double)(float)v; }
-  __device__ __forceinline__ void stage(void* dst, long k) const { __pipeline_memcpy_async(dst, p + k, 4); }
+  template <typename K>
+  __device__ __forceinline__ void stage(void* dst, K k) const {
+    __pipeline_memcpy_async(dst, p + k, 4);
+  }
   __device__ static __forceinline__ double staged(const void* src) { return (double)*(const float*)src; }
 };
 

@@ -25,9 +25,11 @@ struct Derived {
 
 struct HostSetup {
   Derived d{};
-  // mx, my, nx, ny, xu, rxp concatenated; offsets in elements.
+  // mx, my, nx, ny, xu, rxp and the PML update factors concatenated; offsets
+  // in elements.
   std::vector<double> sigma_block;
   size_t off_mx = 0, off_my = 0, off_nx = 0, off_ny = 0, off_xu = 0, off_rxp = 0;
+  size_t off_vax = 0, off_vbx = 0, off_vay = 0, off_vby = 0, off_pax = 0, off_pbx = 0, off_pay = 0, off_pby = 0;
   int nb = 0;
   std::vector<double> bx, by, r0, nb_w;
 };

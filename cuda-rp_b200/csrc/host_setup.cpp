@@ -129,6 +129,27 @@ crp_status host_setup(const crp_config& c, const crp_bubbles_in* bin, HostSetup*
   put(ny, &h.off_ny);
   put(xu, &h.off_xu);
   put(rxp, &h.off_rxp);
+  // PML factors (1 - s) and 1 / (1 + s) of every velocity face (s3 = dt c
+  // sigma / 2 of VelocityKernel, inc/bubble_CUDA_kernel.cuh:664-665, 674-675) and
+  // of every pressure component (s2 of MixturePressureKernel, :853), so that
+  // the grid kernels multiply where the reference divides.  Both are exactly 1
+  // outside the PML.
+  auto factors = [&](const std::vector<double>& sigma, double per_sigma, size_t* off_a, size_t* off_b) {
+    std::vector<double> fa(sigma.size()), fb(sigma.size());
+    for (size_t k = 0; k < sigma.size(); k++) {
+      const double sk = per_sigma * sigma[k];
+      fa[k] = 1.0 - sk;
+      fb[k] = 1.0 / (1.0 + sk);
+    }
+    put(fa, off_a);
+    put(fb, off_b);
+  };
+  const double v_per_sigma = (d.c_inf + d.c_inf) * 0.5 * 0.5 * d.dt;
+  const double p_per_sigma = 0.5 * d.dt * d.c_inf;
+  factors(nx, v_per_sigma, &h.off_vax, &h.off_vbx);
+  factors(ny, v_per_sigma, &h.off_vay, &h.off_vby);
+  factors(mx, p_per_sigma, &h.off_pax, &h.off_pbx);
+  factors(my, p_per_sigma, &h.off_pay, &h.off_pby);
 
   h.bx.clear();
   h.by.clear();

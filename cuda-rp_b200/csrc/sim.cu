@@ -83,27 +83,25 @@ __device__ __forceinline__ void block_max_to(double v, unsigned long long* out) 
 }
 
 // Velocity update of VelocityKernel (inc/bubble_CUDA_kernel.cuh:658-676) for one
-// face, with the coefficients of the reference.
-// Outside the PML (sigma = 0) and where both densities are rho_inf the same
-// value is computed without its divisions: x / 1.0, v * 1.0 and
-// dt / ((rho + rho) * 0.5) = dt / rho are exact.
+// face: (v_old (1 - s3) - q s2) / (1 + s3), with the face's PML factors
+// fa = 1 - s3 and fb = 1 / (1 + s3) precomputed on the host.  Outside the PML
+// both are exactly 1 and the value is the reference's v_old - q s2; inside,
+// the multiplication by fb in place of the division changes it by at most one
+// rounding.  q = dt / mean(rho) is dt / rho_inf, without its division, where
+// both densities are rho_inf.
 __device__ __forceinline__ double velocity_face(const GridParams& g, double v_old, double p0a, double p0b, double rhoa,
-                                                double rhob, double sigma) {
+                                                double rhob, double fa, double fb) {
   const double s2 = (-p0a + p0b) * g.rdx;  // rdx on both faces, as :661 and :671
   const double q = (rhoa == g.rho_inf && rhob == g.rho_inf) ? g.dt_rho : g.dt / ((rhoa + rhob) * 0.5);
-  if (sigma == 0.0) return v_old - q * s2;
-  double s3 = (g.c_inf + g.c_inf) * 0.5;
-  s3 = s3 * 0.5 * g.dt * sigma;
-  return (v_old * (1.0 - s3) - q * s2) / (1.0 + s3);
+  return (v_old * fa - q * s2) * fb;
 }
 
 // Split-pressure update of MixturePressureKernel (:856-859) for one component:
-// pn (1 - s2) - s3 (s1 + s5/2) / (1 + s2), with s2 = dt c sigma / 2.
-__device__ __forceinline__ double pressure_component(const GridParams& g, double pn, double sigma, double s1,
+// pn (1 - s2) - s3 (s1 + s5/2) / (1 + s2), with s2 = dt c sigma / 2 and the
+// component's PML factors fa = 1 - s2, fb = 1 / (1 + s2) (as velocity_face).
+__device__ __forceinline__ double pressure_component(const GridParams& g, double pn, double fa, double fb, double s1,
                                                      double h) {
-  if (sigma == 0.0) return pn - g.s3p * (s1 + h);
-  const double s2 = g.s4p * sigma;
-  return pn * (1.0 - s2) - g.s3p * (s1 + h) / (1.0 + s2);
+  return pn * fa - g.s3p * (s1 + h) * fb;
 }
 
 // s5 / 2 of :854: the void-fraction rate term; zero where f_g stays zero.
@@ -138,7 +136,7 @@ __device__ __noinline__ double vy_face_special(const GridParams& g, int jf, doub
 // VelocityBoundaryKernel): y0 wall or source, [ext] source row, y1 wall.
 __device__ __forceinline__ double vy_face_value(const GridParams& g, int jf, double v_old, double p0a, double p0b,
                                                 double ra, double rb, double xm, double t_cur, double& pre) {
-  double v = velocity_face(g, v_old, p0a, p0b, ra, rb, g.ny[jf + 1]);
+  double v = velocity_face(g, v_old, p0a, p0b, ra, rb, g.vay[jf + 1], g.vby[jf + 1]);
   pre = v;
   if ((jf == 0 && !g.pml_y0) || (g.source_row > 0 && jf == g.source_row)) v = vy_face_special(g, jf, v, xm, t_cur, &pre);
   if (jf == g.f.Y && !g.pml_y1) v = 0.0;
@@ -163,14 +161,21 @@ __device__ __noinline__ double source_row_pressure(const GridParams& g, double x
 // predicted void fraction (:816-867) and the residual of calculate_pressure_field.
 // The work is organised as column strips.  A warp holds the
 // 32 adjacent columns i = 30 s + lane of strip s and marches up a chunk of
-// rows: lanes 1..30 update their cells, lanes 0 and 31 only provide the values
-// across the strip's edges.  Left/right neighbour values arrive by warp
-// shuffle, the row below stays in registers, so every array element is read
-// once per step (the two edge columns of a strip and the row under a chunk
-// once more, from L2), with 256-byte coalesced rows per warp load.  Rows are
-// staged through a per-warp ring of kStripStages rows in shared memory by
+// kStripRows rows: lanes 1..30 update their cells, lanes 0 and 31 only provide
+// the values across the strip's edges.  Left/right neighbour values arrive by
+// warp shuffle, the row below stays in registers, so every array element is
+// read once per step (the two edge columns of a strip and the row under a
+// chunk once more, from L2), with 256-byte coalesced rows per warp load.  Rows
+// are staged through a per-warp ring of kStripStages rows in shared memory by
 // asynchronous copies issued kStripStages - 2 rows ahead, so each warp keeps
 // the next rows of all seven input arrays in flight while it computes.
+//
+// The kernel is bound by the latency of each row's dependent chain rather than
+// by bytes, so its instruction stream is kept short: element offsets are 32-bit
+// (the host rejects frames of 2^32 elements or more), one add per row; lanes
+// past the window stage a copy of column X+1 instead of branching around
+// their copies; only the stores are predicated.  The row loop stays rolled (an
+// unrolled chunk measured slower).
 constexpr int kStripCells = 30;
 constexpr int kStripWarps = 4;
 constexpr int kStripRows = 6;    // rows per chunk (measured best of 4-16 at 1024 x 2048)
@@ -179,7 +184,7 @@ constexpr int kStripFields = 7;  // pnx, pny, fgA, vx_old, vy_old, fgB, fgC
 
 template <typename P>
 __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_constant__ GridParams g,
-                                                               const FdtdArgs<P> a, int rows) {
+                                                               const FdtdArgs<P> a) {
   using G = typename P::G;
   using S = typename P::S;
   using V = typename P::V;
@@ -196,14 +201,21 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
   // Owner of the f_g prediction of this column.
   const bool own = inwin && ((lane >= 1 && lane <= kStripCells) || (lane == 0 && i == 0) ||
                              (lane == 31 && i == X + 1));
-  const int j0 = 1 + blockIdx.y * rows;
-  const int j1 = min(Y, j0 + rows - 1);
+  // Chunks are taken alternately from the bottom and the top of the grid, so
+  // that the PML bands at both y ends (the slowest chunks: general updates
+  // with divisions) start first and the cheap interior chunks fill the tail.
+  const int by = blockIdx.y, cy = (by & 1) ? (int)gridDim.y - 1 - (by >> 1) : (by >> 1);
+  const int j0 = 1 + cy * kStripRows;
+  const int j1 = min(Y, j0 + kStripRows - 1);
   const double xm = ((double)i - 0.5) * g.dx;
   const bool inner_col = i >= 1 && i <= X;
   const bool src_rows = g.source_row > 0 && src_pressure(g);
+  // Offset of element (min(i, X+1), j0 - 1 + rr) is kb + rr * pitch.
+  const unsigned pitch = (unsigned)f.pitch;
+  const unsigned kb = (unsigned)j0 * pitch + (unsigned)(min(i, X + 1) + 1);
   auto p0_of = [&](int r, double px_, double py_) -> double {
-    if (!inwin) return 0.0;
     if (inner_col && r >= 1 && r <= Y && !(src_rows && r == g.source_row)) return px_ + py_;
+    if (!inwin) return 0.0;
     return p0_edge(g, a.pnx, a.pny, i, r, t_prev);
   };
   auto rho_of = [&](double fa) -> double { return a.rho_const ? g.rho_inf : (1.0 - fa) * g.rho_inf; };
@@ -212,47 +224,49 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
     a.fgC.put(k, v);
     return v;
   };
-  // Ring slot of field fld of row r (each lane only touches its own column).
-  auto slot = [&](int r, int fld) -> double* { return &ring[threadIdx.y][r % kStripStages][fld][lane]; };
-  // Queue the copies of row r: pnx, pny, fgA for rows j0-1..j1+1, vy_old for
-  // j0-1..j1, vx_old, fgB, fgC for j0..j1.  One commit group per row, empty
-  // past the chunk, so that a fixed wait count always means "row j+1 landed".
-  auto issue = [&](int r) {
-    if (inwin && r <= j1 + 1) {
-      const long k = f.idx(i, r);
-      a.pnx.stage(slot(r, 0), k);
-      a.pny.stage(slot(r, 1), k);
-      a.fgA.stage(slot(r, 2), k);
+  // Ring slot of field fld of chunk row rr (row j0 - 1 + rr); each lane only
+  // touches its own column.
+  auto slot = [&](int rr, int fld) -> double* { return &ring[threadIdx.y][rr % kStripStages][fld][lane]; };
+  // Queue the copies of chunk row rr: pnx, pny, fgA for rows j0-1..j1+1,
+  // vy_old for j0-1..j1, vx_old, fgB, fgC for j0..j1.  One commit group per
+  // row, empty past the chunk, so that a fixed wait count always means "the
+  // next row landed".
+  auto issue = [&](int rr) {
+    const int r = j0 - 1 + rr;
+    if (rr <= kStripRows + 1 && r <= j1 + 1) {
+      const unsigned k = kb + (unsigned)rr * pitch;
+      a.pnx.stage(slot(rr, 0), k);
+      a.pny.stage(slot(rr, 1), k);
+      a.fgA.stage(slot(rr, 2), k);
       if (r <= j1) {
-        a.vy_old.stage(slot(r, 4), k);
-        if (r >= j0) {
-          a.vx_old.stage(slot(r, 3), k);
-          if (own) {
-            a.fgB.stage(slot(r, 5), k);
-            a.fgC.stage(slot(r, 6), k);
-          }
+        a.vy_old.stage(slot(rr, 4), k);
+        if (rr >= 1) {
+          a.vx_old.stage(slot(rr, 3), k);
+          a.fgB.stage(slot(rr, 5), k);
+          a.fgC.stage(slot(rr, 6), k);
         }
       }
     }
     __pipeline_commit();
   };
-  for (int r = j0 - 1; r < j0 - 1 + kStripStages; r++) issue(r);
+#pragma unroll
+  for (int rr = 0; rr < kStripStages; rr++) issue(rr);
   __pipeline_wait_prior(kStripStages - 2);  // rows j0-1 and j0 have landed
 
   // Row below the chunk and the chunk's first row.
-  double pxc = 0.0, pyc = 0.0, fac = 0.0, p0b = 0.0, rhob = 0.0, vyob = 0.0;
-  if (inwin) {
-    const double pxb = S::staged(slot(j0 - 1, 0)), pyb = S::staged(slot(j0 - 1, 1));
-    const double fab = G::staged(slot(j0 - 1, 2));
-    vyob = V::staged(slot(j0 - 1, 4));
-    pxc = S::staged(slot(j0, 0));
-    pyc = S::staged(slot(j0, 1));
-    fac = G::staged(slot(j0, 2));
+  double pxc, pyc, fac, p0b, rhob, vyob;
+  {
+    const double pxb = S::staged(slot(0, 0)), pyb = S::staged(slot(0, 1));
+    const double fab = G::staged(slot(0, 2));
+    vyob = V::staged(slot(0, 4));
+    pxc = S::staged(slot(1, 0));
+    pyc = S::staged(slot(1, 1));
+    fac = G::staged(slot(1, 2));
     p0b = p0_of(j0 - 1, pxb, pyb);
     rhob = rho_of(fab);
     if (j0 == 1 && own) predict(f.idx(i, 0), fab);
   }
-  issue(j0 - 1 + kStripStages);  // reuses the slot of row j0-1
+  issue(kStripStages);  // reuses the slot of row j0-1
   double p0c = p0_of(j0, pxc, pyc), rhoc = rho_of(fac);
   double vyd = 0.0;
   if (cell) {
@@ -264,69 +278,44 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
     }
   }
 
-  // Per-column coefficients: PML profiles of the east face and the cell, and
-  // the cylindrical metrics.
-  const double nx_e = face ? g.nx[i + 1] : 0.0;
-  const double mx_c = cell ? g.mx[i] : 0.0;
+  // Per-column coefficients: PML factors of the east face and of the cell's x
+  // component, and the cylindrical metrics.
+  const double vax_e = face ? g.vax[i + 1] : 1.0, vbx_e = face ? g.vbx[i + 1] : 1.0;
+  const double pax_c = cell ? g.pax[i] : 1.0, pbx_c = cell ? g.pbx[i] : 1.0;
   const double xu_w = cell && g.cyl ? g.xu[i] : 0.0, xu_e = cell && g.cyl ? g.xu[i + 1] : 0.0;
   const double rxp_c = cell && g.cyl ? g.rxp[i] : 0.0;
   const bool zero_e = (i == 0 && !g.pml_x0) || (i == X && !g.pml_x1);
 
+  // One form of the updates serves every cell: the PML factors are exactly 1
+  // outside the PML, and the divisions of the mixture density and of the
+  // void-fraction rate run only in lanes whose void fraction is nonzero (a
+  // branch the warp skips when no lane takes it).  Special y faces (the y0
+  // wall or source face, the source row) are whole rows, so their branch is
+  // uniform across the warp.
   unsigned long long res = 0ull;  // max |dp0| as a bit pattern (NaN sorts above every number)
 #pragma unroll 1
-  for (int j = j0; j <= j1; j++) {
-    const long k = f.idx(i, j);
-    __pipeline_wait_prior(kStripStages - 2);  // row j+1 has landed
-    double pxn = 0.0, pyn = 0.0, fan = 0.0, vxo = 0.0, vyo = 0.0, fgp = 0.0;
-    if (inwin) {
-      pxn = S::staged(slot(j + 1, 0));
-      pyn = S::staged(slot(j + 1, 1));
-      fan = G::staged(slot(j + 1, 2));
-      vxo = V::staged(slot(j, 3));
-      vyo = V::staged(slot(j, 4));
-    }
-    if (own) {
-      fgp = G::stored(3.0 * fac - 3.0 * G::staged(slot(j, 5)) + G::staged(slot(j, 6)));
-      a.fgC.put(k, fgp);
-    }
+  for (int jj = 0; jj < kStripRows; jj++) {
+    const int j = j0 + jj;
+    if (j > j1) break;
+    const unsigned k = kb + (unsigned)(jj + 1) * pitch;  // (i, j) for every lane that stores
+    __pipeline_wait_prior(kStripStages - 2);              // row j+1 has landed
+    const double pxn = S::staged(slot(jj + 2, 0)), pyn = S::staged(slot(jj + 2, 1));
+    const double fan = G::staged(slot(jj + 2, 2));
+    const double vxo = V::staged(slot(jj + 1, 3)), vyo = V::staged(slot(jj + 1, 4));
+    const double fgp = G::stored(3.0 * fac - 3.0 * G::staged(slot(jj + 1, 5)) + G::staged(slot(jj + 1, 6)));
+    if (own) a.fgC.put(k, fgp);
     const double p0n = p0_of(j + 1, pxn, pyn), rhon = rho_of(fan);
     const double p0r = __shfl_down_sync(full, p0c, 1), rhor = __shfl_down_sync(full, rhoc, 1);
-    const double my_j = g.my[j], ny_n = g.ny[j + 1];
-    // Cells with no PML, no void fraction and rho_m = rho_inf around them, away
-    // from the source row, take the division-free forms of the updates (the
-    // values are the same: the skipped factors are exactly 1 and 0).  The
-    // choice is made for the whole warp so that the general forms do not run
-    // predicated on every lane.
-    const bool plain_e = !face || (nx_e == 0.0 && rhoc == g.rho_inf && rhor == g.rho_inf);
-    const bool plain_c = !cell || (ny_n == 0.0 && rhon == g.rho_inf && mx_c == 0.0 && my_j == 0.0 && fgp == 0.0 &&
-                                   fac == 0.0 && !(g.source_row > 0 && j == g.source_row));
-    double fe = 0.0, vyu = 0.0, qx = 0.0, qy = 0.0;
-    if (__all_sync(full, plain_e && plain_c)) {
-      if (face) fe = zero_e ? 0.0 : vxo - g.dt_rho * ((-p0c + p0r) * g.rdx);
-      const double fw = __shfl_up_sync(full, fe, 1);
-      if (cell) {
-        vyu = (j == Y && !g.pml_y1) ? 0.0 : vyo - g.dt_rho * ((-p0c + p0n) * g.rdx);
-        const double s1x = g.cyl ? (-xu_w * fw + xu_e * fe) * g.rdx * rxp_c : (-fw + fe) * g.rdx;
-        const double s1y = (-vyd + vyu) * g.rdy;
-        qx = pxc - g.s3p * (s1x + 0.0);
-        qy = pyc - g.s3p * (s1y + 0.0);
-      }
-    } else {
-      if (face) {
-        fe = velocity_face(g, vxo, p0c, p0r, rhoc, rhor, nx_e);
-        if (zero_e) fe = 0.0;
-      }
-      const double fw = __shfl_up_sync(full, fe, 1);
-      if (cell) {
-        double pre_u;
-        vyu = vy_face_value(g, j, vyo, p0c, p0n, rhoc, rhon, xm, t_cur, pre_u);
-        const double s1x = g.cyl ? (-xu_w * fw + xu_e * fe) * g.rdx * rxp_c : (-fw + fe) * g.rdx;
-        const double s1y = (-vyd + vyu) * g.rdy;
-        const double h = void_rate_half(g, fgp, fac);
-        qx = pressure_component(g, pxc, mx_c, s1x, h);
-        qy = pressure_component(g, pyc, my_j, s1y, h);
-      }
-    }
+    double fe = velocity_face(g, vxo, p0c, p0r, rhoc, rhor, vax_e, vbx_e);
+    if (zero_e) fe = 0.0;
+    const double fw = __shfl_up_sync(full, fe, 1);
+    double pre_u;
+    const double vyu = vy_face_value(g, j, vyo, p0c, p0n, rhoc, rhon, xm, t_cur, pre_u);
+    const double s1x = g.cyl ? (-xu_w * fw + xu_e * fe) * g.rdx * rxp_c : (-fw + fe) * g.rdx;
+    const double s1y = (-vyd + vyu) * g.rdy;
+    const double h = void_rate_half(g, fgp, fac);
+    const double qx = pressure_component(g, pxc, pax_c, pbx_c, s1x, h);
+    const double qy = pressure_component(g, pyc, g.pay[j], g.pby[j], s1y, h);
     if (cell) {
       a.vx_new.put(k, fe);
       a.vy_new.put(k, vyu);
@@ -335,16 +324,16 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
       double p0new = qx + qy;
       if (src_rows && j == g.source_row) p0new = source_row_pressure(g, xm, t_cur);
       res = max(res, (unsigned long long)__double_as_longlong(fabs(p0c - p0new)));
-      vyd = vyu;
     } else if (lane == 0 && i == 0) {
       a.vx_new.put(k, fe);  // the x0 face, vx(0, j)
     }
+    vyd = vyu;
     pxc = pxn;
     pyc = pyn;
     fac = fan;
     p0c = p0n;
     rhoc = rhon;
-    issue(j + kStripStages);  // reuses the slot of row j
+    issue(jj + 1 + kStripStages);  // reuses the slot of row j
   }
   if (j1 == Y && own) predict(f.idx(i, Y + 1), fac);
   // Warp maximum, one atomic per warp with a nonzero residual (no block
@@ -916,8 +905,8 @@ __global__ void __launch_bounds__(256) couple_press(const __grid_constant__ Grid
       double s1x = g.cyl ? (-g.xu[i] * vxl + g.xu[i + 1] * vxr) * g.rdx * g.rxp[i] : (-vxl + vxr) * g.rdx;
       double s1y = (-a.vy.get(f.idx(i, j - 1)) + a.vy.get(k)) * g.rdy;
       const double h = void_rate_half(g, fgv, a.fgn.get(k));
-      double qx = pressure_component(g, a.pnx.get(k), g.mx[i], s1x, h);
-      double qy = pressure_component(g, a.pny.get(k), g.my[j], s1y, h);
+      double qx = pressure_component(g, a.pnx.get(k), g.pax[i], g.pbx[i], s1x, h);
+      double qy = pressure_component(g, a.pny.get(k), g.pay[j], g.pby[j], s1y, h);
       bool forced = g.source_row > 0 && src_pressure(g) && j == g.source_row;
       if (!forced) res = fabs((a.px.get(k) + a.py.get(k)) - (qx + qy));
       a.px.put(k, qx);
@@ -1556,6 +1545,9 @@ struct Sim {
       own_stream = true;
     }
     fill_params();
+    // The grid kernels address the frame with 32-bit element offsets.
+    if ((unsigned long long)gp.f.pitch * (unsigned long long)(gp.f.Y + 4) >= (1ull << 32))
+      return fail(CRP_ERR_UNSUPPORTED, "grid frame of 2^32 elements or more");
     supp[0] = supp[1] = supp[2] = full_box();
     couple_box = full_box();
     pool_bytes = layout(true);
@@ -1694,6 +1686,14 @@ struct Sim {
     gp.ny = b + hs.off_ny;
     gp.xu = b + hs.off_xu;
     gp.rxp = b + hs.off_rxp;
+    gp.vax = b + hs.off_vax;
+    gp.vbx = b + hs.off_vbx;
+    gp.vay = b + hs.off_vay;
+    gp.vby = b + hs.off_vby;
+    gp.pax = b + hs.off_pax;
+    gp.pbx = b + hs.off_pbx;
+    gp.pay = b + hs.off_pay;
+    gp.pby = b + hs.off_pby;
   }
 
   cudaError_t build_bins() {
@@ -2218,10 +2218,9 @@ struct Sim {
     fa.rho_const = stats.steps == 0 ? 1 : 0;
     fa.residual = d_residual;
     const int strips = (gp.f.X + kStripCells - 1) / kStripCells;
-    const int rows = kStripRows;
-    dim3 grid((strips + kStripWarps - 1) / kStripWarps, (gp.f.Y + rows - 1) / rows);
+    dim3 grid((strips + kStripWarps - 1) / kStripWarps, (gp.f.Y + kStripRows - 1) / kStripRows);
     dim3 block(32, kStripWarps);
-    cudaError_t e = launch(kClassFdtd, [&] { fdtd_strip<P><<<grid, block, 0, stream>>>(gp, fa, rows); });
+    cudaError_t e = launch(kClassFdtd, [&] { fdtd_strip<P><<<grid, block, 0, stream>>>(gp, fa); });
     if (e != cudaSuccess) return e;
     const int ng = std::max(gp.f.X, gp.f.Y) + 3;
     const V vxn = view<V>(vx[nv]), vyn = view<V>(vy[nv]);
