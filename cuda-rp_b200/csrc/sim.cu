@@ -82,17 +82,21 @@ __device__ __forceinline__ void block_max_to(double v, unsigned long long* out) 
   }
 }
 
-// Velocity update of VelocityKernel (inc/bubble_CUDA_kernel.cuh:658-676) for one
-// face: (v_old (1 - s3) - q s2) / (1 + s3), with the face's PML factors
-// fa = 1 - s3 and fb = 1 / (1 + s3) precomputed on the host.  Outside the PML
-// both are exactly 1 and the value is the reference's v_old - q s2; inside,
-// the multiplication by fb in place of the division changes it by at most one
-// rounding.  q = dt / mean(rho) is dt / rho_inf, without its division, where
-// both densities are rho_inf.
-__device__ __forceinline__ double velocity_face(const GridParams& g, double v_old, double p0a, double p0b, double rhoa,
-                                                double rhob, double fa, double fb) {
+// q = dt / mean(rho) of a face of VelocityKernel (inc/bubble_CUDA_kernel.cuh:
+// 660-662, 670-672); dt / rho_inf, without its division, where both densities
+// are rho_inf.
+__device__ __forceinline__ double face_q(const GridParams& g, double rhoa, double rhob) {
+  return (rhoa == g.rho_inf && rhob == g.rho_inf) ? g.dt_rho : g.dt / ((rhoa + rhob) * 0.5);
+}
+// Velocity update of VelocityKernel (:658-676) for one face:
+// (v_old (1 - s3) - q s2) / (1 + s3), with the face's PML factors fa = 1 - s3
+// and fb = 1 / (1 + s3) precomputed on the host.  Outside the PML both are
+// exactly 1 and the value is the reference's v_old - q s2; inside, the
+// multiplication by fb in place of the division changes it by at most one
+// rounding.
+__device__ __forceinline__ double velocity_face_q(const GridParams& g, double v_old, double p0a, double p0b, double q,
+                                                  double fa, double fb) {
   const double s2 = (-p0a + p0b) * g.rdx;  // rdx on both faces, as :661 and :671
-  const double q = (rhoa == g.rho_inf && rhob == g.rho_inf) ? g.dt_rho : g.dt / ((rhoa + rhob) * 0.5);
   return (v_old * fa - q * s2) * fb;
 }
 
@@ -134,9 +138,10 @@ __device__ __noinline__ double vy_face_special(const GridParams& g, int jf, doub
 
 // North face jf of a column (VelocityKernel :668-676 with the y sections of
 // VelocityBoundaryKernel): y0 wall or source, [ext] source row, y1 wall.
+// q: dt / mean(rho) of the face (face_q).
 __device__ __forceinline__ double vy_face_value(const GridParams& g, int jf, double v_old, double p0a, double p0b,
-                                                double ra, double rb, double xm, double t_cur, double& pre) {
-  double v = velocity_face(g, v_old, p0a, p0b, ra, rb, g.vay[jf + 1], g.vby[jf + 1]);
+                                                double q, double xm, double t_cur, double& pre) {
+  double v = velocity_face_q(g, v_old, p0a, p0b, q, g.vay[jf + 1], g.vby[jf + 1]);
   pre = v;
   if ((jf == 0 && !g.pml_y0) || (g.source_row > 0 && jf == g.source_row)) v = vy_face_special(g, jf, v, xm, t_cur, &pre);
   if (jf == g.f.Y && !g.pml_y1) v = 0.0;
@@ -271,7 +276,7 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
   double vyd = 0.0;
   if (cell) {
     double pre_d;
-    vyd = vy_face_value(g, j0 - 1, vyob, p0b, p0c, rhob, rhoc, xm, t_cur, pre_d);
+    vyd = vy_face_value(g, j0 - 1, vyob, p0b, p0c, face_q(g, rhob, rhoc), xm, t_cur, pre_d);
     if (j0 == 1) {
       a.vy_new.put(f.idx(i, 0), vyd);
       if (!g.pml_y0) a.vy_new.put(f.idx(i, -1), pre_d);
@@ -288,10 +293,10 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
 
   // One form of the updates serves every cell: the PML factors are exactly 1
   // outside the PML, and the divisions of the mixture density and of the
-  // void-fraction rate run only in lanes whose void fraction is nonzero (a
-  // branch the warp skips when no lane takes it).  Special y faces (the y0
-  // wall or source face, the source row) are whole rows, so their branch is
-  // uniform across the warp.
+  // void-fraction rate run only in warps that hold void fraction (a branch
+  // taken by the whole warp or skipped by it).  Special y faces (the y0 wall or
+  // source face, the source row) are whole rows, so their branch is uniform
+  // across the warp too.
   unsigned long long res = 0ull;  // max |dp0| as a bit pattern (NaN sorts above every number)
 #pragma unroll 1
   for (int jj = 0; jj < kStripRows; jj++) {
@@ -306,14 +311,20 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
     if (own) a.fgC.put(k, fgp);
     const double p0n = p0_of(j + 1, pxn, pyn), rhon = rho_of(fan);
     const double p0r = __shfl_down_sync(full, p0c, 1), rhor = __shfl_down_sync(full, rhoc, 1);
-    double fe = velocity_face(g, vxo, p0c, p0r, rhoc, rhor, vax_e, vbx_e);
+    // dt / mean(rho) of the east and north faces and the void-fraction rate h.
+    double q_e = g.dt_rho, q_n = g.dt_rho, h = 0.0;
+    if (__any_sync(full, rhoc != g.rho_inf || rhor != g.rho_inf || rhon != g.rho_inf || fgp != 0.0 || fac != 0.0)) {
+      q_e = face_q(g, rhoc, rhor);
+      q_n = face_q(g, rhoc, rhon);
+      h = void_rate_half(g, fgp, fac);
+    }
+    double fe = velocity_face_q(g, vxo, p0c, p0r, q_e, vax_e, vbx_e);
     if (zero_e) fe = 0.0;
     const double fw = __shfl_up_sync(full, fe, 1);
     double pre_u;
-    const double vyu = vy_face_value(g, j, vyo, p0c, p0n, rhoc, rhon, xm, t_cur, pre_u);
+    const double vyu = vy_face_value(g, j, vyo, p0c, p0n, q_n, xm, t_cur, pre_u);
     const double s1x = g.cyl ? (-xu_w * fw + xu_e * fe) * g.rdx * rxp_c : (-fw + fe) * g.rdx;
     const double s1y = (-vyd + vyu) * g.rdy;
-    const double h = void_rate_half(g, fgp, fac);
     const double qx = pressure_component(g, pxc, pax_c, pbx_c, s1x, h);
     const double qy = pressure_component(g, pyc, g.pay[j], g.pby[j], s1y, h);
     if (cell) {
