@@ -72,6 +72,7 @@ struct BubbleParams {
   // sub-step's critical path, deciding exactly as the square root would.
   double abs2_cut64;
   float abs2_cut32;
+  float rho32, sig32, mu32, gam32;  // FP32 copies for the mixed path's thermal model
   double pi, pi4r3;
   double dcx, dcy, dcz;  // delta_coef (src/bubble_CUDA.cu:1469-1471)
   long long step_cap;
@@ -271,6 +272,8 @@ using C64 = Cx<double>;
 // Per-bubble constants derived from its R0 (init_bub_params, src/bubble_CUDA.cu:666-670).
 struct BubbleR0 {
   double R0, PG0, R03, coeff_alpha, inv_R0, inv_PG0;
+  double T0_PG0R03;          // T0 / (PG0 R0^3) of the heat flux
+  float R0_32, PG0_32, ca32;  // FP32 copies for the mixed path's thermal model
 };
 __device__ __forceinline__ BubbleR0 bubble_r0(const BubbleParams& b, double R0) {
   BubbleR0 r;
@@ -280,6 +283,10 @@ __device__ __forceinline__ BubbleR0 bubble_r0(const BubbleParams& b, double R0) 
   r.PG0 = b.PL0 + 2.0 * b.sig / R0;
   r.inv_PG0 = 1.0 / r.PG0;
   r.coeff_alpha = b.gam * r.PG0 * r.R03 / (2.0 * (b.gam - 1.0) * b.T0 * b.K0);
+  r.T0_PG0R03 = b.T0 / (r.PG0 * r.R03);
+  r.R0_32 = (float)R0;
+  r.PG0_32 = (float)r.PG0;
+  r.ca32 = (float)r.coeff_alpha;
   return r;
 }
 
@@ -341,13 +348,25 @@ __device__ __forceinline__ float series_cut<float>(const BubbleParams& b) {
   return b.abs2_cut32;
 }
 
+// Constants of the thermal model in its real type.
+template <typename R>
+struct ThermalConst {
+  R rho, sig, mu, gam, ca, R0, PG0, cut2;
+};
+__device__ __forceinline__ ThermalConst<double> thermal_const64(const BubbleParams& b, const BubbleR0& r) {
+  return {b.rho, b.sig, b.mu, b.gam, r.coeff_alpha, r.R0, r.PG0, b.abs2_cut64};
+}
+__device__ __forceinline__ ThermalConst<float> thermal_const32(const BubbleParams& b, const BubbleR0& r) {
+  return {b.rho32, b.sig32, b.mu32, b.gam32, r.ca32, r.R0_32, r.PG0_32, b.abs2_cut32};
+}
+
 // solveOmegaN (:263-288): omega_N and alpha_N for gas pressure PG at radius Rb.
 template <typename R>
-__device__ __forceinline__ R omega_n(Cx<R>& alpha, R PG, R Rb, const BubbleParams& b, const BubbleR0& r) {
+__device__ __forceinline__ R omega_n(Cx<R>& alpha, R PG, R Rb, const ThermalConst<R>& c) {
   const R eps = R(2.22044604925031308e-016);
-  const R rho = R(b.rho), sig = R(b.sig), mu = R(b.mu), gam = R(b.gam), ca = R(r.coeff_alpha);
-  R Rx = xdiv(Rb, R(r.R0));
-  R coef1 = xdiv(R(r.PG0), PG * Rx * Rx * Rx);
+  const R rho = c.rho, sig = c.sig, mu = c.mu, gam = c.gam, ca = c.ca;
+  R Rx = xdiv(Rb, c.R0);
+  R coef1 = xdiv(c.PG0, PG * Rx * Rx * Rx);
   R coef2 = PG * rho;
   R coef3 = xdiv(R(4), Rb * Rb);
   R value1 = xdiv(R(-2) * sig * rho, Rb);
@@ -362,7 +381,7 @@ __device__ __forceinline__ R omega_n(Cx<R>& alpha, R PG, R Rb, const BubbleParam
   for (int k = 0; k < 3; k++) {
     R s = sqrt(ca_Rb * omega);
     const R pg_4w = xdiv(PG, R(4) * omega);  // independent of Upsilon
-    Cx<R> u = cscl(upsilon(Cx<R>{s, s}, gam, series_cut<R>(b)), coef1);
+    Cx<R> u = cscl(upsilon(Cx<R>{s, s}, gam, c.cut2), coef1);
     mu_eff = mu + u.im * pg_4w;
     eta = u.re * coef2 + value1 - mu_eff * mu_eff * coef3;
     omega = sqrt(fmax(eta, R(1.0e-6) * eps)) * inv_rho_Rb;
@@ -372,20 +391,20 @@ __device__ __forceinline__ R omega_n(Cx<R>& alpha, R PG, R Rb, const BubbleParam
   return omega;
 }
 
-// solvePG (:326-340).
-__device__ __forceinline__ double gas_pressure(double PGn, double Rp, double Rn, double omega, double dt, C64 lp,
-                                               const BubbleParams& b, const BubbleR0& r) {
+// solvePG (:326-340).  inv_den = 1 / |Lp|^2 and inv_wdt = 1 / (omega dt),
+// shared with the heat flux of the same sub-step.
+__device__ __forceinline__ double gas_pressure(double PGn, double Rp, double Rn, double inv_wdt, double dt,
+                                               double inv_den, C64 lp, const BubbleParams& b, const BubbleR0& r) {
   double R = 0.5 * (Rp + Rn);
   double Rx = R * r.inv_R0;
   double Rpx = Rp * r.inv_R0;
   double Rnx = Rn * r.inv_R0;
   const double inv_R = 1.0 / R;
-  const double inv_den = 1.0 / (lp.re * lp.re + lp.im * lp.im);
   double lpr = lp.re * inv_den;
   double lpi = lp.im * inv_den;
   double c0 = dt * 3.0 * (b.gam - 1.0) * b.K0 * b.T0 * inv_R * r.inv_PG0;
   double c3 = 1.5 * b.gam * (Rp - Rn) * inv_R + c0 * lpr * 0.5 * Rx * Rx * Rx;
-  const double w = c0 * lpi / (omega * dt);
+  const double w = c0 * lpi * inv_wdt;
   double c1 = 1.0 + c3 - w * Rpx * Rpx * Rpx;
   double c2 = 1.0 - c3 - w * Rnx * Rnx * Rnx;
   return (c2 * PGn + c0 * lpr * r.PG0) / c1;
@@ -401,8 +420,16 @@ __device__ __forceinline__ void rp_substep(double& Rt, double& Rp, double& Rn, d
   double acc = (PG - PL - 2.0 * b.sig * inv_Rn - 4.0 * b.mu * inv_Rn * d1R) * b.inv_rho - 1.5 * d1R * d1R;
   double dtm = dt;
   double dtp = fmin(1.01 * dt, b.dt0);
-  if (fabs(d1R) > eps) dtp = fmin(dtp, 0.01 * Rn / fabs(d1R));
-  if (fabs(acc) > eps) dtp = fmin(dtp, 0.1 * Rn / sqrt(fabs(acc)));
+  // The velocity and acceleration limits, 0.01 Rn / |d1R| and 0.1 Rn / sqrt(|acc|)
+  // (:238-241): each quotient is formed only where it is the smaller step, decided
+  // on the products (the squares for the second), so a quiet sub-step divides
+  // by neither.
+  const double ad = fabs(d1R), aa = fabs(acc);
+  if (ad > eps && 0.01 * Rn < dtp * ad) dtp = fmin(dtp, 0.01 * Rn / ad);
+  if (aa > eps) {
+    const double lim = 0.1 * Rn;
+    if (lim * lim < dtp * dtp * aa) dtp = fmin(dtp, lim / sqrt(aa));
+  }
   double q = dtp / dtm;
   Rt = Rp = (1.0 + q) * Rn - q * Rm + (dtp * inv_Rn) * (0.5 * (dtp + dtm) * acc);
   d1R = (dtm * dtm * Rp + (-dtm * dtm + dtp * dtp) * Rn - dtp * dtp * Rm) / (dtm * dtp * (dtm + dtp)) +

@@ -667,8 +667,13 @@ template <typename T>
 __device__ __forceinline__ void thermal_model(const BubbleParams& bp, const RpState& s, double PGn, double& omega,
                                               C64& lp) {
   Cx<T> alpha_t;
-  omega = (double)omega_n<T>(alpha_t, (T)PGn, (T)s.Rn, bp, s.r);
-  const Cx<T> lp_t = lp_n<T>(alpha_t, (T)s.Rn, series_cut<T>(bp));
+  ThermalConst<T> c;
+  if constexpr (sizeof(T) == sizeof(double))
+    c = thermal_const64(bp, s.r);
+  else
+    c = thermal_const32(bp, s.r);
+  omega = (double)omega_n<T>(alpha_t, (T)PGn, (T)s.Rn, c);
+  const Cx<T> lp_t = lp_n<T>(alpha_t, (T)s.Rn, c.cut2);
   lp = C64{(double)lp_t.re, (double)lp_t.im};
 }
 
@@ -689,14 +694,17 @@ __device__ __forceinline__ void rp_substep_full(const BubbleParams& bp, RpState&
     thermal_model<double>(bp, s, PGn, omega, lp);
   else
     thermal_model<T>(bp, s, PGn, omega, lp);
-  s.PGp = gas_pressure(PGn, s.Rp, s.Rn, omega, s.dtL, lp, bp, s.r);
+  const double inv_den = 1.0 / (lp.re * lp.re + lp.im * lp.im);
+  const double inv_wdt = 1.0 / (omega * s.dtL);
+  s.PGp = gas_pressure(PGn, s.Rp, s.Rn, inv_wdt, s.dtL, inv_den, lp, bp, s.r);
   const double Rp = s.Rp, Rn = s.Rn, PGp = s.PGp;
   const double s0 = 0.5 * (Rp + Rn);
-  const double s1 = 1.0 / (lp.re * lp.re + lp.im * lp.im) * bp.T0 / (s.r.PG0 * s.r.R03);
+  const double s1 = inv_den * s.r.T0_PG0R03;
   const double dTdr = lp.re * s1 * (s.r.PG0 * s.r.R03 - 0.5 * (PGp + PGn) * s0 * s0 * s0) +
-                      lp.im * s1 * (PGp * Rp * Rp * Rp - PGn * Rn * Rn * Rn) / (omega * s.dtL);
+                      lp.im * s1 * (PGp * Rp * Rp * Rp - PGn * Rn * Rn * Rn) * inv_wdt;
   s.heat -= 4.0 * bp.pi * Rp * Rp * bp.K0 * dTdr * s.dtL;
-  s.vis += 4.0 * bp.pi * Rp * Rp * 4.0 * bp.mu * s.d1Rp / Rp * s.d1Rp * s.dtL;
+  // 4 pi Rp^2 (4 mu d1Rp / Rp) d1Rp dt, with Rp^2 / Rp cancelled.
+  s.vis += 4.0 * bp.pi * Rp * 4.0 * bp.mu * s.d1Rp * s.d1Rp * s.dtL;
   s.count++;
 }
 
@@ -739,13 +747,18 @@ __device__ __forceinline__ void rp_end(const GridParams& g, const BubbleParams& 
 // while the queue has work.  Each bubble's arithmetic is the same as a
 // thread-per-bubble solve, so results do not depend on the schedule.
 constexpr int kRpThreads = 128;
-// At least 5 resident blocks per SM (at most 102 registers a thread): more
-// warps to hide the FP64 latency chains of the sub-step, measured faster than
-// the unconstrained 128 registers despite a few spilled values.
-constexpr int kRpMinBlocks = 5;
+// Resident blocks per SM the register budget is set for: 6 for the FP64 path
+// (at most 85 registers a thread), 5 for the mixed path (102): more warps to
+// hide the FP64 latency chains of the sub-step, measured faster than fewer
+// warps with more registers despite a few spilled values (the mixed path's
+// FP32 thermal model gains nothing from the sixth block).
+template <typename P>
+constexpr int rp_min_blocks() {
+  return sizeof(typename P::T) == sizeof(double) ? 6 : 5;
+}
 
 template <typename P>
-__global__ void __launch_bounds__(kRpThreads, kRpMinBlocks) bubble_rp(const __grid_constant__ GridParams g,
+__global__ void __launch_bounds__(kRpThreads, rp_min_blocks<P>()) bubble_rp(const __grid_constant__ GridParams g,
                                                         const __grid_constant__ BubbleParams bp, BubbleArrays b,
                                                         const typename P::S px, const typename P::S py,
                                                         const double* __restrict__ tdev,
@@ -1678,6 +1691,10 @@ struct Sim {
       while (std::sqrt(cf) > 0.1f) cf = std::nextafter(cf, 0.0f);
       while (!(std::sqrt(cf) > 0.1f)) cf = std::nextafter(cf, 1.0f);
       bp.abs2_cut32 = cf;
+      bp.rho32 = (float)bp.rho;
+      bp.sig32 = (float)bp.sig;
+      bp.mu32 = (float)bp.mu;
+      bp.gam32 = (float)bp.gam;
     }
     bp.K0 = cfg.bub_K0;
     bp.dt0 = d.bub_dt0;
