@@ -337,17 +337,26 @@ def focal_mask(sim, cfg, radius=2e-3):
     return np.hypot((ii - 0.5) * d.dx, (jj - 0.5) * d.dy - fy) <= radius
 
 
+def focal_compare_step(cfg):
+    """Mixture step 100 steps after the focused burst reaches the focus: the
+    source delays make every element's wave arrive there at t = focal_dist / c."""
+    dt = cfg.sim_cfl * min(cfg.grid_lx / cfg.grid_x, cfg.grid_ly / cfg.grid_y) / cfg.ext_c_inf
+    return int(np.ceil(cfg.tr_focal_dist / cfg.ext_c_inf / dt)) + 100
+
+
 def compare_at(primary_sim, other_sim, cfg, primary):
-    """Advance the other path's simulation to the primary's step and compare
-    p0 over the grid and within 2 mm of the focus, and the bubble radii."""
+    """Advance both paths' simulations (untimed) to focal_compare_step and
+    compare p0 over the grid and within 2 mm of the focus, and the bubble radii."""
     import crp
 
-    step = int(primary_sim.stats().steps)
-    try:
-        if other_sim.stats().steps < step:
-            other_sim.step(step - int(other_sim.stats().steps))
-    except crp.CrpError as e:
-        return {"at_step": step, "error": f"{'fp64' if primary == 'mixed' else 'mixed'} path: {e}"}
+    step = max(int(primary_sim.stats().steps), focal_compare_step(cfg))
+    for name, sim in (("primary", primary_sim), ("other", other_sim)):
+        try:
+            if sim.stats().steps < step:
+                sim.step(step - int(sim.stats().steps))
+        except crp.CrpError as e:
+            path = primary if name == "primary" else ("fp64" if primary == "mixed" else "mixed")
+            return {"at_step": step, "error": f"{path} path: {e}"}
     a, b = primary_sim.field("p0"), other_sim.field("p0")
     if primary != "mixed":
         a, b = b, a
@@ -410,6 +419,34 @@ def run_ours(args, rank, world, dist):
     n_fdtd = p1s.fdtd_launches - p0s.fdtd_launches
     fdtd_ms = (p1s.ms_fdtd - p0s.ms_fdtd) / max(n_fdtd, 1)
     prof = {k: (getattr(p1s, k) - getattr(p0s, k)) for k in ("ms_fdtd", "ms_rp", "ms_couple", "ms_other")}
+    # End to end through the C ABI: host inputs in, host rawdata arrays out.
+    # Measured before the driven sample, so that no collapse phase precedes it.
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        t0 = time.perf_counter()
+        e2e_steps = 0
+        t_steps = t_read = 0.0
+        with crp.Sim(cfg, bub) as s2:
+            t_create = time.perf_counter() - t0
+            d = s2.dims
+            h2d = 4 * 8 * nb
+            for _ in range(args.steps):
+                ta = time.perf_counter()
+                s2.step(S)
+                tb = time.perf_counter()
+                e2e_steps += S
+                s2.field("p0")
+                s2.bubbles("R_t")
+                t_steps += tb - ta
+                t_read += time.perf_counter() - tb
+        wall = time.perf_counter() - t0
+        e2e = {"value": cells * e2e_steps / wall / 1e6, "unit": "Mcell-upd/s",
+               "h2d_bytes_per_step": h2d // max(args.steps, 1),
+               "d2h_bytes_per_step": 8 * (d.i1m * d.j1m + nb),
+               "seconds": {"create": t_create, "steps": t_steps, "read_back": t_read, "total": wall},
+               "note": "wall clock: crp_create (seeded bubbles uploaded) + steps from t=0 + p0 and R_t "
+                       "read back every bench step"}
+
     driven = driven_sample(sim, args, cells, nb) if with_driven else None
     focal = None
     if driven is not None and len(runs) > 1:
@@ -439,6 +476,8 @@ def run_ours(args, rank, world, dist):
         }
         if driven is not None:
             result["driven"] = driven
+        if e2e is not None:
+            result["e2e"] = e2e
         for prec, r in runs.items():
             result[f"{prec}_path"] = {"value": cells * mix_steps * world / (r["ms"] * 1e-3) / 1e6,
                                       "ms_per_step": r["ms"] / args.steps,
@@ -458,25 +497,6 @@ def run_ours(args, rank, world, dist):
     for r in runs.values():
         if r["sim"] is not None:
             r["sim"].close()
-
-    # End to end through the C ABI: host inputs in, host rawdata arrays out.
-    if rank == 0 and not args.no_e2e:
-        t0 = time.perf_counter()
-        e2e_steps = 0
-        with crp.Sim(cfg, bub) as s2:
-            d = s2.dims
-            h2d = 4 * 8 * nb
-            for _ in range(args.steps):
-                s2.step(S)
-                e2e_steps += S
-                s2.field("p0")
-                s2.bubbles("R_t")
-        wall = time.perf_counter() - t0
-        result["e2e"] = {"value": cells * e2e_steps / wall / 1e6, "unit": "Mcell-upd/s",
-                         "h2d_bytes_per_step": h2d // max(args.steps, 1),
-                         "d2h_bytes_per_step": 8 * (d.i1m * d.j1m + nb),
-                         "note": "wall clock: crp_create (seeded bubbles uploaded) + steps from t=0 + p0 and R_t "
-                                 "read back every bench step"}
 
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
