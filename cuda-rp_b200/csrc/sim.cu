@@ -868,17 +868,29 @@ __global__ void __launch_bounds__(kLptScatterThreads)
 // Void fraction of one cell from the bubbles of the four bins whose stencils
 // cover it (bins (i-1..i) x (j-1..j), each in ascending bubble order): their
 // contributions sit contiguously at 4 * (position in the sorted bins).
-__device__ __forceinline__ double gather_fg(const Frame& f, const int* __restrict__ start,
-                                            const double* __restrict__ contrib, int i, int j) {
+// One of the four bins whose bubbles contribute to cell (i, j): bin b = 0..3 is
+// (i-1, j-1), (i, j-1), (i-1, j), (i, j); the sum of its bubbles' contributions
+// to (i, j), in the bin's sorted order.
+__device__ __forceinline__ double gather_bin(const Frame& f, const int* __restrict__ start,
+                                             const double* __restrict__ contrib, int i, int j, int b) {
+  const int bx = i - 1 + (b & 1), by = j - 1 + (b >> 1);
+  const int c = (by + 1) * (f.X + 3) + (bx + 1);
+  const int slot = (i - bx) * 2 + (j - by);
   double s = 0.0;
-  for (int by = j - 1; by <= j; by++) {
-    for (int bx = i - 1; bx <= i; bx++) {
-      const int c = (by + 1) * (f.X + 3) + (bx + 1);
-      const int slot = (i - bx) * 2 + (j - by);
-      for (int k = start[c]; k < start[c + 1]; k++) s += contrib[4 * (long)k + slot];
-    }
-  }
+  for (int k = start[c]; k < start[c + 1]; k++) s += contrib[4 * (long)k + slot];
   return s;
+}
+// Sum over the four bins of cell (i, j), as (b0 + b1) + (b2 + b3); with the
+// axis fold (fold: cells 0 and 1 take the sum of both) each bin's part is that
+// of cell 0 plus that of cell 1.  couple_press forms the same sums in the same
+// order across four lanes, so both give bit-identical void fractions.
+__device__ __forceinline__ double gather_fg(const Frame& f, const int* __restrict__ start,
+                                            const double* __restrict__ contrib, int i, int j, bool fold = false) {
+  double sb[4];
+  for (int b = 0; b < 4; b++)
+    sb[b] = fold ? gather_bin(f, start, contrib, 0, j, b) + gather_bin(f, start, contrib, 1, j, b)
+                 : gather_bin(f, start, contrib, i, j, b);
+  return (sb[0] + sb[1]) + (sb[2] + sb[3]);
 }
 
 template <typename P>
@@ -898,7 +910,13 @@ struct CoupleArgs {
 
 // calculate_void_fraction (memset, scatter, VoidFractionCylinderKernel fold:
 // :1198-1218, :559-573) as a gather, then MixturePressureKernel (:816-867) on
-// the new void fraction and the residual of calculate_pressure_field.
+// the new void fraction and the residual of calculate_pressure_field.  Four
+// lanes per cell, one per contributing bin, so that the per-bin runs are
+// summed side by side; the cell's void fraction is (b0 + b1) + (b2 + b3), the
+// same in the four lanes and the same from run to run.  A block covers
+// kCoupleW x 8 cells.
+constexpr int kCoupleW = 8;
+
 template <typename P>
 __global__ void __launch_bounds__(256) couple_press(const __grid_constant__ GridParams g, const CoupleArgs<P> a) {
   const Frame& f = g.f;
@@ -910,17 +928,23 @@ __global__ void __launch_bounds__(256) couple_press(const __grid_constant__ Grid
     i1 = a.dbox[2];
     j1 = a.dbox[3];
     // Launched over the whole window: blocks past the box leave at once.
-    if (i0 + (int)(blockIdx.x * blockDim.x) > i1 || j0 + (int)(blockIdx.y * blockDim.y) > j1) return;
+    if (i0 + (int)(blockIdx.x * kCoupleW) > i1 || j0 + (int)(blockIdx.y * blockDim.y) > j1) return;
   }
-  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int bin = threadIdx.x & 3;
+  const int i = i0 + blockIdx.x * kCoupleW + (threadIdx.x >> 2);
   const int j = j0 + blockIdx.y * blockDim.y + threadIdx.y;
-  double res = 0.0;
-  if (i <= i1 && j <= j1) {
-    double fgv;
-    if (g.cyl && i <= 1)
-      fgv = gather_fg(f, a.start, a.contrib, 0, j) + gather_fg(f, a.start, a.contrib, 1, j);
+  const bool in = i <= i1 && j <= j1;
+  double fgv = 0.0;
+  if (in) {
+    if (g.cyl && i <= 1)  // the axis fold: cells 0 and 1 both take the sum of the two
+      fgv = gather_bin(f, a.start, a.contrib, 0, j, bin) + gather_bin(f, a.start, a.contrib, 1, j, bin);
     else
-      fgv = gather_fg(f, a.start, a.contrib, i, j);
+      fgv = gather_bin(f, a.start, a.contrib, i, j, bin);
+  }
+  fgv += __shfl_xor_sync(0xffffffffu, fgv, 1);
+  fgv += __shfl_xor_sync(0xffffffffu, fgv, 2);
+  double res = 0.0;
+  if (in && bin == 0) {
     long k = f.idx(i, j);
     a.fg.put(k, fgv);
     fgv = a.fg.get(k);  // the stored value (FP32 in the mixed path) is what the step uses
@@ -2482,12 +2506,7 @@ __global__ void __launch_bounds__(256) couple_fg_only(const __grid_constant__ Gr
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i > f.X + 1 || j > f.Y + 1) return;
-  double fgv;
-  if (g.cyl && i <= 1)
-    fgv = gather_fg(f, a.start, a.contrib, 0, j) + gather_fg(f, a.start, a.contrib, 1, j);
-  else
-    fgv = gather_fg(f, a.start, a.contrib, i, j);
-  a.fg.put(f.idx(i, j), fgv);
+  a.fg.put(f.idx(i, j), gather_fg(f, a.start, a.contrib, i, j, g.cyl && i <= 1));
 }
 
 cudaError_t Sim::launch_contrib_only() {
@@ -2533,7 +2552,7 @@ cudaError_t Sim::launch_couple_t(bool pressure) {
     ca.i1 = gp.f.X + 1;
     ca.j1 = gp.f.Y + 1;
     ca.dbox = d_scalars->box;
-    dim3 grd((gp.f.X + 2 + 31) / 32, (gp.f.Y + 2 + 7) / 8);
+    dim3 grd((gp.f.X + 2 + kCoupleW - 1) / kCoupleW, (gp.f.Y + 2 + 7) / 8);
     return launch(kClassCouple, [&] { couple_press<P><<<grd, blk, 0, stream>>>(gp, ca); });
   }
   if (pressure) {
@@ -2543,7 +2562,7 @@ cudaError_t Sim::launch_couple_t(bool pressure) {
     ca.j0 = b.j0;
     ca.i1 = b.i1;
     ca.j1 = b.j1;
-    dim3 grd((b.i1 - b.i0 + 1 + 31) / 32, (b.j1 - b.j0 + 1 + 7) / 8);
+    dim3 grd((b.i1 - b.i0 + 1 + kCoupleW - 1) / kCoupleW, (b.j1 - b.j0 + 1 + 7) / 8);
     return launch(kClassCouple, [&] { couple_press<P><<<grd, blk, 0, stream>>>(gp, ca); });
   }
   dim3 grd((gp.f.X + 2 + 31) / 32, (gp.f.Y + 2 + 7) / 8);
