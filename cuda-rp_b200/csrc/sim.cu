@@ -870,15 +870,22 @@ __global__ void __launch_bounds__(kLptScatterThreads)
 // contributions sit contiguously at 4 * (position in the sorted bins).
 // One of the four bins whose bubbles contribute to cell (i, j): bin b = 0..3 is
 // (i-1, j-1), (i, j-1), (i-1, j), (i, j); the sum of its bubbles' contributions
-// to (i, j), in the bin's sorted order.
+// to (i, j): the even and the odd positions of the bin's sorted run summed
+// separately (two independent chains), then added.
 __device__ __forceinline__ double gather_bin(const Frame& f, const int* __restrict__ start,
                                              const double* __restrict__ contrib, int i, int j, int b) {
   const int bx = i - 1 + (b & 1), by = j - 1 + (b >> 1);
   const int c = (by + 1) * (f.X + 3) + (bx + 1);
   const int slot = (i - bx) * 2 + (j - by);
-  double s = 0.0;
-  for (int k = start[c]; k < start[c + 1]; k++) s += contrib[4 * (long)k + slot];
-  return s;
+  double s = 0.0, t = 0.0;
+  int k = start[c];
+  const int e = start[c + 1];
+  for (; k + 1 < e; k += 2) {
+    s += contrib[4 * (long)k + slot];
+    t += contrib[4 * (long)k + 4 + slot];
+  }
+  if (k < e) s += contrib[4 * (long)k + slot];
+  return s + t;
 }
 // Sum over the four bins of cell (i, j), as (b0 + b1) + (b2 + b3); with the
 // axis fold (fold: cells 0 and 1 take the sum of both) each bin's part is that
