@@ -183,7 +183,7 @@ __device__ __noinline__ double source_row_pressure(const GridParams& g, double x
 // unrolled chunk measured slower).
 constexpr int kStripCells = 30;
 constexpr int kStripWarps = 4;
-constexpr int kStripRows = 6;    // rows per chunk (measured best of 4-16 at 1024 x 2048)
+constexpr int kStripRows = 8;    // rows per chunk (measured best of 4-16 at 1024 x 2048)
 constexpr int kStripStages = 4;  // ring slots (rows) per warp; a smaller ring leaves more L1 (measured)
 constexpr int kStripFields = 7;  // pnx, pny, fgA, vx_old, vy_old, fgB, fgC
 
