@@ -46,7 +46,7 @@ class Config(ctypes.Structure):
         ("ext_picard_cap", c_int), ("ext_rp_step_cap", c_int), ("ext_bubble_count", c_int),
         ("ext_bubble_seed", ctypes.c_uint64), ("ext_r0_sigma_ln", c_dbl), ("ext_cloud_shape", c_int),
         ("ext_cloud_r", c_dbl), ("ext_cloud_h", c_dbl), ("ext_n_b", c_dbl), ("ext_picard_tol", c_dbl),
-        ("ext_graphs", c_int),
+        ("ext_graphs", c_int), ("ext_elements", c_int),
     ]
 
 
@@ -65,6 +65,11 @@ class Stats(ctypes.Structure):
 
 
 PROGRESS = ctypes.CFUNCTYPE(None, ctypes.c_int64, c_dbl, ctypes.c_void_p)
+
+
+class Objective(ctypes.Structure):
+    """crp_objective: steps to run and differentiate over, focal radius [m]."""
+    _fields_ = [("steps", c_int), ("focal_radius", c_dbl)]
 
 
 class FocusState(ctypes.Structure):
@@ -149,6 +154,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "crp_focus_history": (ctypes.c_int64, [vp, c_int, vp, ctypes.c_int64]),
         "crp_get_focus_state": (c_int, [vp, P(FocusState)]),
         "crp_set_focus_state": (c_int, [vp, P(FocusState)]),
+        "crp_set_source_elements": (c_int, [vp, c_int, vp, vp]),
+        "crp_adjoint": (c_int, [vp, P(Objective), P(c_dbl), vp, vp]),
         "crp_batch_create": (c_int, [c_int, P(Config), P(BubblesIn), P(vp)]),
         "crp_batch_run": (c_int, [vp, P(c_int), c_int, P(c_int)]),
         "crp_batch_count": (c_int, [vp]),
@@ -273,6 +280,25 @@ class Sim:
 
     def set_focus_state(self, st: FocusState):
         self._check(self.lib.crp_set_focus_state(self.h, ctypes.byref(st)))
+
+    def set_source_elements(self, amp, phase):
+        """Amplitude factors and phase offsets of the cfg.ext_elements source elements."""
+        a = np.ascontiguousarray(amp, dtype=np.float64)
+        p = np.ascontiguousarray(phase, dtype=np.float64)
+        assert a.shape == p.shape and a.ndim == 1
+        self._check(self.lib.crp_set_source_elements(self.h, int(a.size), _ptr(a), _ptr(p)))
+
+    def adjoint(self, steps: int, focal_radius: float, n_elements: int = 0):
+        """Advance `steps` steps and return (J, dJ/d amplitudes, dJ/d phases) of
+        the focal objective (crp_adjoint); the gradients are None without elements."""
+        obj = Objective(int(steps), float(focal_radius))
+        J = c_dbl(0.0)
+        ga = np.zeros(n_elements) if n_elements > 0 else None
+        gp = np.zeros(n_elements) if n_elements > 0 else None
+        self._check(self.lib.crp_adjoint(self.h, ctypes.byref(obj), ctypes.byref(J),
+                                         _ptr(ga) if ga is not None else None,
+                                         _ptr(gp) if gp is not None else None))
+        return J.value, ga, gp
 
     def write_sph(self, directory: str):
         self._check(self.lib.crp_write_sph(self.h, directory.encode()))

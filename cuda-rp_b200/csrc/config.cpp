@@ -158,6 +158,7 @@ const Key kKeys[] = {
     K("ext.n_b", kDouble, ext_n_b),
     K("ext.picard_tol", kDouble, ext_picard_tol),
     K("ext.graphs", kBool, ext_graphs),
+    K("ext.elements", kInt, ext_elements),
 };
 #undef K
 
@@ -294,6 +295,7 @@ crp_status crp_config_defaults(crp_config* cfg) {
   cfg->ext_precision = CRP_PREC_FP64;
   cfg->ext_picard_cap = 1000;
   cfg->ext_graphs = 0;
+  cfg->ext_elements = 0;
   cfg->ext_rp_step_cap = 1000000;
   cfg->ext_n_b = 1.0;
   return CRP_OK;

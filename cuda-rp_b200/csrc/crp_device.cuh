@@ -60,6 +60,12 @@ struct GridParams {
   const double* pbx;
   const double* pay;
   const double* pby;
+  // Source elements (ext.elements): count, aperture radius, and per-element
+  // amplitude factors and phase offsets (device arrays of elem_n values).
+  int elem_n;
+  double elem_rap;
+  const double* elem_amp;
+  const double* elem_phase;
 };
 
 // bub_params_t scalars shared by every bubble (inc/bubble_CUDA.h:135-154); the
@@ -92,16 +98,31 @@ __device__ __forceinline__ double burst_ramp(const GridParams& g, double tau) {
   return w;
 }
 
+// Source element of the cell at x = xm: equal bands of |xm - ctl_x| over the
+// aperture radius elem_rap.
+__device__ __forceinline__ int element_of(const GridParams& g, double xm) {
+  const int e = (int)(fabs(xm - g.ctl_x) * (double)g.elem_n / g.elem_rap);
+  return e < g.elem_n ? e : g.elem_n - 1;
+}
+
 // Transducer value at (xm, ym), time t.  Plane source then focused source, as
 // inc/bubble_CUDA_kernel.cuh:749-787 (velocity) and :889-925 (pressure).  Returns
-// false when no source of that kind is configured.
+// false when no source of that kind is configured.  With ext.elements, the
+// pressure source's value at a cell of element e is a_e times the reference's,
+// with phi_e added to the sine's argument.
 __device__ __forceinline__ bool source_value(const GridParams& g, bool pressure, double xm, double ym, double t,
                                              double& out) {
   double amp = pressure ? g.pamp : g.amp;
+  double ph = 0.0;
+  if (pressure && g.elem_n > 0) {
+    const int e = element_of(g, xm);
+    amp = g.elem_amp[e] * amp;
+    ph = g.elem_phase[e];
+  }
   bool set = false;
   if (pressure ? g.plane_p : g.plane_v) {
     double tau = fmod(t, g.period);
-    out = (tau <= g.on_time) ? amp * burst_ramp(g, tau) * sin(g.omega * t) : 0.0;
+    out = (tau <= g.on_time) ? amp * burst_ramp(g, tau) * sin(g.omega * t + ph) : 0.0;
     set = true;
   }
   if (pressure ? g.focused_p : g.focused_v) {
@@ -109,13 +130,49 @@ __device__ __forceinline__ bool source_value(const GridParams& g, bool pressure,
     if (s1 <= g.focal_dist) {
       s1 = fmax(t - (g.focal_dist - s1) / g.c_inf, 0.0);
       double s2 = fmod(s1, g.period);
-      out = (s2 < g.on_time) ? amp * burst_ramp(g, s2) * sin(g.omega * s2) : 0.0;
+      out = (s2 < g.on_time) ? amp * burst_ramp(g, s2) * sin(g.omega * s2 + ph) : 0.0;
     } else {
       out = 0.0;
     }
     set = true;
   }
+  // At t = 0 the pressure source is 0: the reference's p0 array starts at zero
+  // and is first written by the pressure evaluation of step 1, so the first
+  // velocity update reads no source.  (Its own source is 0 at t = 0 anyway; an
+  // element's phase offset would not be.)
+  if (pressure && set && !(t > 0.0)) out = 0.0;
   return set;
+}
+
+// Derivatives of the pressure source's value at (xm, ym), time t, with respect
+// to the amplitude factor (dA) and the phase offset (dP) of the cell's element
+// (ext.elements > 0).  The focused source, when set, is the value the source
+// takes (source_value applies it last).
+__device__ __forceinline__ void source_derivatives(const GridParams& g, double xm, double ym, double t, double& dA,
+                                                   double& dP) {
+  dA = dP = 0.0;
+  if (!(t > 0.0)) return;  // the source is 0 at t = 0 (source_value)
+  const int e = element_of(g, xm);
+  const double a = g.elem_amp[e], ph = g.elem_phase[e];
+  double arg, env;
+  if (g.focused_p) {
+    double s1 = sqrt((g.ctl_x - xm) * (g.ctl_x - xm) + (g.ctl_y - ym) * (g.ctl_y - ym));
+    if (!(s1 <= g.focal_dist)) return;
+    s1 = fmax(t - (g.focal_dist - s1) / g.c_inf, 0.0);
+    const double s2 = fmod(s1, g.period);
+    if (!(s2 < g.on_time)) return;
+    env = g.pamp * burst_ramp(g, s2);
+    arg = g.omega * s2 + ph;
+  } else if (g.plane_p) {
+    const double tau = fmod(t, g.period);
+    if (!(tau <= g.on_time)) return;
+    env = g.pamp * burst_ramp(g, tau);
+    arg = g.omega * t + ph;
+  } else {
+    return;
+  }
+  dA = env * sin(arg);
+  dP = a * env * cos(arg);
 }
 
 // Field storage.  FP64 path: one double per value.  Mixed path: an FP32 value

@@ -11,6 +11,7 @@ namespace crp {
 // Scalars derived once from the configuration (init_grid_size, init_transducer,
 // init_mix, mix_set_time_increment, init_bub_params: src/bubble_CUDA.cu:487-518).
 struct Derived {
+  double elem_rap = 0.0;  // aperture radius of the source elements (ext.elements > 0), element_aperture()
   double dx, dy, rdx, rdy;
   double dt;
   double rho_inf, c_inf, P_inf, T_inf;
@@ -33,6 +34,12 @@ struct HostSetup {
   int nb = 0;
   std::vector<double> bx, by, r0, nb_w;
 };
+
+// Largest distance from the focus axis, |x - ctl_x|, among the cells that
+// carry the pressure source (row ext.source_row, or the y = 0 ghost row when
+// it is 0; a focused source only within focal_dist of the focus): the radius
+// that ext.elements splits into equal bands.  0 without such cells.
+double element_aperture(const crp_config& c, double dx, double dy, double ctl_x, double ctl_y, double focal_dist);
 
 // Validate the configuration and compute everything crp_create uploads.
 crp_status host_setup(const crp_config& cfg, const crp_bubbles_in* bubbles, HostSetup* out, std::string* err);

@@ -74,6 +74,20 @@ void pml_profiles(const crp_config& c, const Derived& d, std::vector<double>& mx
 
 }  // namespace
 
+double element_aperture(const crp_config& c, double dx, double dy, double ctl_x, double ctl_y, double focal_dist) {
+  const double ym = c.ext_source_row > 0 ? ((double)c.ext_source_row - 0.5) * dy : -0.5 * dy;
+  double r = 0.0;
+  for (int i = 1; i <= c.grid_x; i++) {
+    const double xm = ((double)i - 0.5) * dx;
+    if (c.tr_focused_p) {
+      const double s1 = std::sqrt((ctl_x - xm) * (ctl_x - xm) + (ctl_y - ym) * (ctl_y - ym));
+      if (!(s1 <= focal_dist)) continue;
+    }
+    r = std::max(r, std::fabs(xm - ctl_x));
+  }
+  return r;
+}
+
 crp_status host_setup(const crp_config& c, const crp_bubbles_in* bin, HostSetup* out, std::string* err) {
   HostSetup& h = *out;
   if (c.grid_x < 2 || c.grid_y < 2) return bad(err, "grid.x and grid.y must be at least 2");
@@ -89,6 +103,10 @@ crp_status host_setup(const crp_config& c, const crp_bubbles_in* bin, HostSetup*
     return bad(err, "a source needs transducer.freq > 0 and on_wave + off_wave > 0");
   if (c.ext_source_row < 0 || c.ext_source_row > c.grid_y) return bad(err, "ext.source_row out of range");
   if (c.ext_picard_cap < 0 || c.ext_rp_step_cap <= 0) return bad(err, "ext.picard_cap/ext.rp_step_cap out of range");
+  if (c.ext_elements < 0 || c.ext_elements > 65536) return bad(err, "ext.elements out of range (0..65536)");
+  if (c.ext_elements > 0 && (!(c.tr_plane_p || c.tr_focused_p) || c.tr_plane_v || c.tr_focused_v))
+    return bad(err, "ext.elements needs a pressure source and no velocity source");
+  if (c.ext_elements > 0 && c.tr_pid) return bad(err, "ext.elements with transducer.pid is not supported");
   Derived& d = h.d;
   d.dx = (double)c.grid_lx / (double)c.grid_x;
   d.dy = (double)c.grid_ly / (double)c.grid_y;
@@ -106,6 +124,8 @@ crp_status host_setup(const crp_config& c, const crp_bubbles_in* bin, HostSetup*
   d.ctl_y = d.fpy;
   if (c.tr_pid && c.tr_init_control) d.ctl_x = 0.0, d.ctl_y = c.tr_init_control;
   d.focal_dist = d.ctl_y / 0.5 / std::sqrt(3.0);
+  d.elem_rap = c.ext_elements > 0 ? element_aperture(c, d.dx, d.dy, d.ctl_x, d.ctl_y, d.focal_dist) : 0.0;
+  if (c.ext_elements > 0 && !(d.elem_rap > 0.0)) return bad(err, "ext.elements: the source has no cells");
   d.bub_dt0 = 0.1 * d.dt;
   d.pi = std::acos(-1.0);
   d.pi4r3 = d.pi * 4.0 / 3.0;

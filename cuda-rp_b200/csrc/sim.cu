@@ -33,6 +33,7 @@
 
 #include "crp.h"
 #include "crp_device.cuh"
+#include "adjoint.cuh"
 #include "crp_host.h"
 
 namespace crp {
@@ -1437,6 +1438,7 @@ struct Sim {
   bool mixed = false;
   double* scratch = nullptr;  // dense (X+2) x (Y+2) doubles for readback
   double* d_sigma = nullptr;
+  double* d_elem = nullptr;  // source elements: amplitude factors, then phase offsets
   BubbleArrays bub{};
   Bins bins{};
   // Device scalars written by the kernels, read back once per pressure evaluation.
@@ -1529,6 +1531,7 @@ struct Sim {
     }
     scratch = carve<double>((size_t)(f.X + 2) * (f.Y + 2), off, dry);
     d_sigma = carve<double>(hs.sigma_block.size(), off, dry);
+    d_elem = carve<double>(2 * (size_t)std::max(cfg.ext_elements, 1), off, dry);
     d_scalars = carve<Scalars>(1, off, dry);
     if (!dry) {
       d_residual = &d_scalars->residual;
@@ -1631,6 +1634,17 @@ struct Sim {
     CRP_CUDA(cudaMemcpyAsync(d_sigma, hs.sigma_block.data(), sizeof(double) * hs.sigma_block.size(),
                              cudaMemcpyHostToDevice, stream));
     set_sigma_pointers();
+    if (cfg.ext_elements > 0) {
+      std::vector<double> e0(2 * (size_t)cfg.ext_elements, 0.0);
+      std::fill(e0.begin(), e0.begin() + cfg.ext_elements, 1.0);
+      // On the simulation's stream, after the pool's clearing (a pageable
+      // source is staged before the call returns).
+      CRP_CUDA(cudaMemcpyAsync(d_elem, e0.data(), sizeof(double) * e0.size(), cudaMemcpyHostToDevice, stream));
+    }
+    gp.elem_n = cfg.ext_elements;
+    gp.elem_rap = hs.d.elem_rap;
+    gp.elem_amp = d_elem;
+    gp.elem_phase = d_elem + std::max(cfg.ext_elements, 1);
     // Bubbles: initial state of bubble_input (src/bubble_CUDA.cu:900-943).
     if (hs.nb > 0) {
       const int n = hs.nb;
@@ -2286,6 +2300,20 @@ struct Sim {
     return launch(kClassOther, [&] { vghost<V><<<(ng + 255) / 256, 256, 0, stream>>>(gp, vxn, vyn); });
   }
 
+  // Source elements (crp_set_source_elements).
+  crp_status set_source_elements(int n, const double* amp, const double* phase) {
+    if (n <= 0 || n != gp.elem_n || !amp || !phase) return fail(CRP_ERR_INVALID, "source elements: n must equal ext.elements");
+    std::vector<double> e(2 * (size_t)n);
+    std::copy(amp, amp + n, e.begin());
+    std::copy(phase, phase + n, e.begin() + n);
+    CRP_CUDA(cudaMemcpyAsync(d_elem, e.data(), sizeof(double) * e.size(), cudaMemcpyHostToDevice, stream));
+    CRP_CUDA(cudaStreamSynchronize(stream));
+    return CRP_OK;
+  }
+
+  // crp_adjoint (defined below, after the buffer views).
+  crp_status adjoint(const crp_objective* obj, double* J, double* grad_amp, double* grad_phase);
+
   // Fourth-order Butterworth low-pass of the tracked depth (filter_loop,
   // inc/bubble_CUDA_kernel.cuh:117-129), with this simulation's state.
   double filter_depth(double input) {
@@ -2576,6 +2604,136 @@ cudaError_t Sim::launch_couple_t(bool pressure) {
   return launch(kClassOther, [&] { couple_fg_only<P><<<grd, blk, 0, stream>>>(gp, ca); });
 }
 
+// crp_adjoint: obj->steps forward steps recording the focal p0, the
+// objective, then the reverse sweep of adj_faces / adj_cells / adj_force
+// (adjoint.cuh) and the per-element sums of the per-column gradients.
+crp_status Sim::adjoint(const crp_objective* obj, double* J, double* grad_amp, double* grad_phase) {
+  if (!obj || obj->steps <= 0 || !(obj->focal_radius > 0.0))
+    return fail(CRP_ERR_INVALID, "adjoint: steps > 0 and focal_radius > 0 are required");
+  if ((grad_amp || grad_phase) && gp.elem_n == 0)
+    return fail(CRP_ERR_INVALID, "adjoint: gradients need ext.elements > 0");
+  // The temperature branch, when on, is driven by the pressure and does not act
+  // back on it: the forward steps advance it, the objective does not see it.
+  if (hs.nb > 0 || src_velocity(gp) || !src_pressure(gp))
+    return fail(CRP_ERR_UNSUPPORTED, "adjoint: bubbles off and a pressure source only");
+  const Frame& f = gp.f;
+  const int X = f.X, Y = f.Y, N = obj->steps;
+  // Focal box: cell centres within focal_radius of the focus.
+  const double cx = gp.ctl_x, cy = gp.ctl_y, r = obj->focal_radius;
+  int bi0 = X + 1, bi1 = 0, bj0 = Y + 1, bj1 = 0;
+  for (int i = 1; i <= X; i++)
+    if (std::fabs(((double)i - 0.5) * gp.dx - cx) <= r) bi0 = std::min(bi0, i), bi1 = std::max(bi1, i);
+  for (int j = 1; j <= Y; j++)
+    if (std::fabs(((double)j - 0.5) * gp.dy - cy) <= r) bj0 = std::min(bj0, j), bj1 = std::max(bj1, j);
+  const int bw = std::max(bi1 - bi0 + 1, 1), bh = std::max(bj1 - bj0 + 1, 1);
+  if (bi1 < bi0 || bj1 < bj0) bi0 = bj0 = 1;  // empty: one cell of weight 0
+  const size_t cells_box = (size_t)bw * bh;
+  std::vector<double> w(cells_box, 0.0);
+  const double pi = std::acos(-1.0);
+  for (int jj = 0; jj < bh; jj++)
+    for (int ii = 0; ii < bw; ii++) {
+      const int i = bi0 + ii, j = bj0 + jj;
+      if (i > bi1 || j > bj1 || (gp.source_row > 0 && j == gp.source_row)) continue;
+      const double xm = ((double)i - 0.5) * gp.dx, ym = ((double)j - 0.5) * gp.dy;
+      if ((xm - cx) * (xm - cx) + (ym - cy) * (ym - cy) > r * r) continue;
+      w[(size_t)jj * bw + ii] = gp.cyl ? 2.0 * pi * xm * gp.dx * gp.dy : gp.dx * gp.dy;
+    }
+  // Device buffers: six adjoint frames, two per-column gradients, weights,
+  // the focal history and the per-step objective.
+  const size_t hist_n = (size_t)N * cells_box;
+  if (hist_n * sizeof(double) > ((size_t)32 << 30))
+    return fail(CRP_ERR_TOO_LARGE, "adjoint: focal history above 32 GiB (steps x focal cells)");
+  const size_t n_doubles = 6 * cells + 2 * (size_t)(X + 2) + cells_box + hist_n + (size_t)N;
+  double* buf = nullptr;
+  if (cudaMalloc(&buf, n_doubles * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CRP_ERR_ALLOC, "adjoint: device memory");
+  }
+  struct Free {  // on every return: let the queued work finish, then release the buffers
+    double* p;
+    cudaStream_t st;
+    ~Free() {
+      cudaStreamSynchronize(st);
+      cudaFree(p);
+    }
+  } guard{buf, stream};
+  AdjBuffers ab;
+  ab.LX = buf;
+  ab.LY = ab.LX + cells;
+  ab.LXt = ab.LY + cells;
+  ab.LYt = ab.LXt + cells;
+  ab.MX = ab.LYt + cells;
+  ab.MY = ab.MX + cells;
+  ab.gA = ab.MY + cells;
+  ab.gP = ab.gA + (X + 2);
+  double* d_w = ab.gP + (X + 2);
+  double* hist = d_w + cells_box;
+  double* d_Jn = hist + hist_n;
+  CRP_CUDA(cudaMemsetAsync(buf, 0, n_doubles * sizeof(double), stream));
+  CRP_CUDA(cudaMemcpyAsync(d_w, w.data(), sizeof(double) * cells_box, cudaMemcpyHostToDevice, stream));
+  const FocalBox box{bi0, bj0, bw, bh, d_w};
+  const int rb = (int)((cells_box + 255) / 256);
+  // Forward, recording the focal p0 after every step.
+  std::vector<double> times((size_t)N + 1);
+  times[0] = tstep;
+  for (int n = 1; n <= N; n++) {
+    const crp_status st = step_once();
+    if (st != CRP_OK) return st;
+    double* out = hist + (size_t)(n - 1) * cells_box;
+    cudaError_t e;
+    if (mixed) {
+      const F32c a = view<F32c>(px[cur_p]), b = view<F32c>(py[cur_p]);
+      e = launch(kClassOther, [&] { adj_record<F32c><<<rb, 256, 0, stream>>>(gp, a, b, box, out); });
+    } else {
+      const F64 a = view<F64>(px[cur_p]), b = view<F64>(py[cur_p]);
+      e = launch(kClassOther, [&] { adj_record<F64><<<rb, 256, 0, stream>>>(gp, a, b, box, out); });
+    }
+    CRP_CUDA(e);
+    times[n] = tstep;
+  }
+  // Objective.
+  CRP_CUDA(launch(kClassOther, [&] { adj_objective<<<N, kAdjSumThreads, 0, stream>>>(box, hist, d_Jn); }));
+  std::vector<double> Jn(N);
+  CRP_CUDA(cudaMemcpyAsync(Jn.data(), d_Jn, sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
+  CRP_CUDA(cudaStreamSynchronize(stream));
+  double Jsum = 0.0;
+  for (int n = 0; n < N; n++) Jsum += Jn[n];
+  if (J) *J = gp.dt * Jsum;
+  // Reverse sweep.
+  const dim3 blk(32, 8);
+  const dim3 gfaces((X + 2 + 31) / 32, (Y + 2 + 7) / 8), gcells((X + 31) / 32, (Y + 7) / 8);
+  CRP_CUDA(launch(kClassOther, [&] { adj_force<<<rb, 256, 0, stream>>>(gp, ab, box, hist + (size_t)(N - 1) * cells_box); }));
+  for (int n = N; n >= 1; n--) {
+    CRP_CUDA(launch(kClassOther, [&] { adj_faces<<<gfaces, blk, 0, stream>>>(gp, ab); }));
+    const double t_src = times[n - 1];
+    CRP_CUDA(launch(kClassOther, [&] { adj_cells<<<gcells, blk, 0, stream>>>(gp, ab, t_src); }));
+    if (n >= 2) {
+      const double* p0 = hist + (size_t)(n - 2) * cells_box;
+      CRP_CUDA(launch(kClassOther, [&] { adj_force<<<rb, 256, 0, stream>>>(gp, ab, box, p0); }));
+    }
+  }
+  if (gp.elem_n > 0) {
+    std::vector<double> gA(X + 2), gPh(X + 2);
+    CRP_CUDA(cudaMemcpyAsync(gA.data(), ab.gA, sizeof(double) * (X + 2), cudaMemcpyDeviceToHost, stream));
+    CRP_CUDA(cudaMemcpyAsync(gPh.data(), ab.gP, sizeof(double) * (X + 2), cudaMemcpyDeviceToHost, stream));
+    CRP_CUDA(cudaStreamSynchronize(stream));
+    const int ne = gp.elem_n;
+    std::vector<double> sa(ne, 0.0), sp(ne, 0.0);
+    for (int i = 1; i <= X; i++) {
+      const double xm = ((double)i - 0.5) * gp.dx;
+      int e = (int)(std::fabs(xm - gp.ctl_x) * (double)ne / gp.elem_rap);
+      if (e >= ne) e = ne - 1;
+      sa[e] += gA[i];
+      sp[e] += gPh[i];
+    }
+    if (grad_amp) std::copy(sa.begin(), sa.end(), grad_amp);
+    if (grad_phase) std::copy(sp.begin(), sp.end(), grad_phase);
+  } else {
+    CRP_CUDA(cudaStreamSynchronize(stream));
+  }
+  return CRP_OK;
+}
+
 cudaError_t Sim::launch_couple(bool pressure) {
   return mixed ? launch_couple_t<PrecMixed>(pressure) : launch_couple_t<PrecFP64>(pressure);
 }
@@ -2674,6 +2832,16 @@ crp_status crp_set_focus_state(crp_sim* h, const crp_focus_state* st) {
     h->s.control_hist.assign(1, st->control_y);
   }
   return CRP_OK;
+}
+
+crp_status crp_set_source_elements(crp_sim* h, int32_t n, const double* amp, const double* phase) {
+  if (!h) return CRP_ERR_INVALID;
+  return h->s.set_source_elements(n, amp, phase);
+}
+
+crp_status crp_adjoint(crp_sim* h, const crp_objective* obj, double* J, double* grad_amp, double* grad_phase) {
+  if (!h) return CRP_ERR_INVALID;
+  return h->s.adjoint(obj, J, grad_amp, grad_phase);
 }
 
 crp_status crp_minmax_T(const crp_sim* h, double* T_min, double* T_max) {

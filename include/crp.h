@@ -120,6 +120,11 @@ typedef struct crp_config {
                                 every step driven from the host.  Graphs save about 10 us per step on
                                 small grids; on 1024 x 2048 and with many concurrent simulations the
                                 host-driven steps measured faster */
+  int32_t ext_elements;      /* >0: the pressure source's aperture is split into this many elements
+                                (equal bands of distance from the focus axis; rings about the axis
+                                in the axisymmetric geometry), each with an amplitude factor and a
+                                phase offset (crp_set_source_elements; default 1 and 0, which leave
+                                the source unchanged) */
 } crp_config;
 
 /* Dense host layouts of the readable fields, in the reference's index order:
@@ -335,6 +340,35 @@ crp_status crp_batch_run(crp_batch* batch, const int32_t* steps, int32_t threads
 int32_t crp_batch_count(const crp_batch* batch);
 crp_sim* crp_batch_sim(crp_batch* batch, int32_t k);
 void crp_batch_destroy(crp_batch* batch);
+
+/* Phased-array source and its adjoint.  Neither has a counterpart in the
+ * reference (its source is one focused aperture, src/bubble_CUDA.cu:542-551,
+ * inc/bubble_CUDA_kernel.cuh:883-926); they extend the same source.
+ *
+ * crp_set_source_elements: amplitude factors amp[e] and phase offsets phase[e]
+ * (radians, added to the burst's sine) of the cfg.ext_elements elements; n must
+ * equal cfg.ext_elements.  Element e covers the source cells whose distance from
+ * the focus axis is in [e, e+1) r_ap / n, r_ap the largest such distance among
+ * the source's cells.
+ *
+ * crp_adjoint: advances the simulation obj->steps mixture steps (as crp_step)
+ * and returns J = sum over those steps of dt * sum over the cells within
+ * obj->focal_radius of the focus of w p0^2 (w the cell volume: 2 pi r dx dy in
+ * the axisymmetric geometry, dx dy otherwise; source-row cells excluded), and
+ * its gradient with respect to the elements' amplitudes and phases, the state
+ * at the call held fixed.  The gradient comes from a hand-written discrete
+ * adjoint of the FDTD/PML step run backwards over the recorded focal pressure
+ * (the step is linear without bubbles, so no other forward state is needed).
+ * Supported: bubbles off, pressure sources (plane or focused), any PML faces;
+ * otherwise CRP_ERR_UNSUPPORTED (the temperature branch, when on, runs with the
+ * forward steps; it does not act on the pressure).  grad_amp and
+ * grad_phase receive cfg.ext_elements values each (either may be NULL). */
+typedef struct crp_objective {
+  int32_t steps;        /* mixture steps to run and differentiate over */
+  double focal_radius;  /* [m] radius of the focal region around the source's focus */
+} crp_objective;
+crp_status crp_set_source_elements(crp_sim* sim, int32_t n, const double* amp, const double* phase);
+crp_status crp_adjoint(crp_sim* sim, const crp_objective* obj, double* J, double* grad_amp, double* grad_phase);
 
 const char* crp_last_error(const crp_sim* sim);
 const char* crp_status_string(crp_status s);

@@ -388,6 +388,11 @@ struct crpo_sim {
   int64_t nstep = 0;
   crp_stats stats{};
   int source_row;  // row carrying the source (0: reference ghost row)
+  // Source elements (ext.elements, an extension without a reference
+  // counterpart): count, aperture radius, amplitude factors, phase offsets.
+  int elem_n = 0;
+  double elem_rap = 0.0;
+  std::vector<double> elem_amp, elem_phase;
 
   // ---- helpers ----
   double delta_x(int pos, double bx) const {
@@ -402,15 +407,25 @@ struct crpo_sim {
   // Source value at x = xm, y = ym, time t; amplitude amp_scale * amp.
   // Plane source: inc/bubble_CUDA_kernel.cuh:749-762 / 889-902; focused: :763-787 / :903-925.
   // Returns false when neither source of this kind is active (value unchanged).
+  // With ext.elements, a pressure source cell of element e (equal bands of
+  // |xm - ctl_x| over the aperture radius) takes a_e times the value, with
+  // phi_e added to the sine's argument.
   bool source_value(bool pressure, double xm, double ym, double t, double& out) const {
     const crp_config& c = cfg;
     double period = ((double)c.tr_on_wave + (double)c.tr_off_wave) / c.tr_freq;
     double amp = pressure ? d.rho_inf * d.cs_inf * c.tr_amp : c.tr_amp;
+    double ph = 0.0;
+    if (pressure && elem_n > 0) {
+      int e = (int)(std::fabs(xm - d.ctlx) * (double)elem_n / elem_rap);
+      if (e >= elem_n) e = elem_n - 1;
+      amp = elem_amp[e] * amp;
+      ph = elem_phase[e];
+    }
     bool set = false;
     if (pressure ? c.tr_plane_p : c.tr_plane_v) {
       double tau = std::fmod(t, period);
       if (tau <= ((double)c.tr_on_wave) / c.tr_freq)
-        out = amp * ramp(c, tau) * std::sin(d.omega * t);
+        out = amp * ramp(c, tau) * std::sin(d.omega * t + ph);
       else
         out = 0.0;
       set = true;
@@ -421,7 +436,7 @@ struct crpo_sim {
         s1 = std::max(t - (d.focal_dist - s1) / d.cs_inf, 0.0);
         double s2 = std::fmod(s1, period);
         if (s2 < (double)c.tr_on_wave / c.tr_freq)
-          out = amp * ramp(c, s2) * std::sin(d.omega * s2);
+          out = amp * ramp(c, s2) * std::sin(d.omega * s2 + ph);
         else
           out = 0.0;
       } else {
@@ -442,6 +457,25 @@ struct crpo_sim {
     cyl = c.tr_cylindrical != 0;
     bubbles_on = c.bub_enable != 0;
     source_row = c.ext_source_row;
+    if (c.ext_elements > 0) {
+      // Aperture radius: the largest |x - ctl_x| among the pressure source's
+      // cells (a focused source only within focal_dist of the focus).
+      if (!(c.tr_plane_p || c.tr_focused_p) || c.tr_plane_v || c.tr_focused_v || c.tr_pid) return CRP_ERR_INVALID;
+      const double ym = source_row > 0 ? ((double)source_row - 0.5) * d.dy : -0.5 * d.dy;
+      elem_rap = 0.0;
+      for (int i = 1; i <= X; i++) {
+        const double xm = ((double)i - 0.5) * d.dx;
+        if (c.tr_focused_p) {
+          const double s1 = std::sqrt((d.ctlx - xm) * (d.ctlx - xm) + (d.ctly - ym) * (d.ctly - ym));
+          if (!(s1 <= d.focal_dist)) continue;
+        }
+        elem_rap = std::max(elem_rap, std::fabs(xm - d.ctlx));
+      }
+      if (!(elem_rap > 0.0)) return CRP_ERR_INVALID;
+      elem_n = c.ext_elements;
+      elem_amp.assign(elem_n, 1.0);
+      elem_phase.assign(elem_n, 0.0);
+    }
     make_sigma(c, a, d, mx, my, nx, ny);
     // init_grid_vector, src/bubble_CUDA.cu:690-713.
     rxp.assign(a.iend2m - a.ista2m + 1, 0.0);
@@ -1031,6 +1065,13 @@ crp_status crpo_create(const crp_config* cfg, const crp_bubbles_in* bubbles, crp
     return st;
   }
   *out = s;
+  return CRP_OK;
+}
+
+crp_status crpo_set_source_elements(crpo_sim* s, int32_t n, const double* amp, const double* phase) {
+  if (!s || n != s->elem_n || n <= 0 || !amp || !phase) return CRP_ERR_INVALID;
+  s->elem_amp.assign(amp, amp + n);
+  s->elem_phase.assign(phase, phase + n);
   return CRP_OK;
 }
 

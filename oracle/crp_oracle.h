@@ -27,6 +27,8 @@ typedef struct crpo_sim crpo_sim;
 /* Same meaning as crp_create; bubbles == NULL selects the reference lattice. */
 crp_status crpo_create(const crp_config* cfg, const crp_bubbles_in* bubbles, crpo_sim** out);
 crp_status crpo_step(crpo_sim* sim, int32_t n);
+/* Same meaning as crp_set_source_elements. */
+crp_status crpo_set_source_elements(crpo_sim* sim, int32_t n, const double* amp, const double* phase);
 crp_status crpo_get_dims(const crpo_sim* sim, crp_dims* dims);
 crp_status crpo_get_stats(const crpo_sim* sim, crp_stats* stats);
 crp_status crpo_read_field(crpo_sim* sim, crp_field field, double* host);

@@ -34,6 +34,7 @@ def oracle_lib():
         sig = {
             "crpo_create": (ctypes.c_int32, [P(crp.Config), P(crp.BubblesIn), P(vp)]),
             "crpo_step": (ctypes.c_int32, [vp, ctypes.c_int32]),
+            "crpo_set_source_elements": (ctypes.c_int32, [vp, ctypes.c_int32, vp, vp]),
             "crpo_get_dims": (ctypes.c_int32, [vp, P(crp.Dims)]),
             "crpo_get_stats": (ctypes.c_int32, [vp, P(crp.Stats)]),
             "crpo_read_field": (ctypes.c_int32, [vp, ctypes.c_int32, vp]),
@@ -78,6 +79,13 @@ class OracleSim:
         st = self.lib.crpo_step(self.h, n)
         if st:
             raise crp.CrpError(st, "crpo_step")
+
+    def set_source_elements(self, amp, phase):
+        a = np.ascontiguousarray(amp, dtype=np.float64)
+        p = np.ascontiguousarray(phase, dtype=np.float64)
+        st = self.lib.crpo_set_source_elements(self.h, int(a.size), _ptr(a), _ptr(p))
+        if st:
+            raise crp.CrpError(st, "crpo_set_source_elements")
 
     def stats(self):
         s = crp.Stats()
@@ -189,3 +197,42 @@ def small_config(**over) -> crp.Config:
     for k, v in over.items():
         setattr(cfg, k, v)
     return cfg
+
+
+def focal_weights(cfg: crp.Config, radius: float) -> np.ndarray:
+    """Cell weights of the focal objective of crp_adjoint on the dense p0 layout
+    [j][i] (i in 0..X+1, j in 0..Y+1): the cell volume (2 pi r dx dy in the
+    axisymmetric geometry, dx dy otherwise) for interior cells whose centre lies
+    within `radius` of the source's focus, 0 elsewhere and on the source row."""
+    X, Y = cfg.grid_x, cfg.grid_y
+    dx, dy = cfg.grid_lx / X, cfg.grid_ly / Y
+    cx = 0.0
+    cy = cfg.tr_focal_dist * 0.5 * np.sqrt(3.0) if cfg.tr_focal_dist else cfg.grid_ly * 0.5
+    xm = (np.arange(X + 2) - 0.5) * dx
+    ym = (np.arange(Y + 2) - 0.5) * dy
+    ii, jj = np.meshgrid(np.arange(X + 2), np.arange(Y + 2))
+    xx, yy = np.meshgrid(xm, ym)
+    inside = (ii >= 1) & (ii <= X) & (jj >= 1) & (jj <= Y) & ((xx - cx) * (xx - cx) + (yy - cy) * (yy - cy) <= radius * radius)
+    if cfg.ext_source_row > 0:
+        inside &= jj != cfg.ext_source_row
+    vol = 2.0 * np.pi * xx * dx * dy if cfg.tr_cylindrical else np.full_like(xx, dx * dy)
+    return np.where(inside, vol, 0.0)
+
+
+def oracle_focal_objective(cfg: crp.Config, amp, phase, steps: int, radius: float) -> float:
+    """J = sum over `steps` steps from t = 0 of dt sum w p0^2 (focal_weights), on the oracle."""
+    sim = OracleSim(cfg)
+    try:
+        if amp is not None:
+            sim.set_source_elements(amp, phase)
+        w = focal_weights(cfg, radius)
+        dt = cfg.sim_cfl * min(cfg.grid_lx / cfg.grid_x, cfg.grid_ly / cfg.grid_y) / cfg.ext_c_inf
+        J = 0.0
+        for _ in range(steps):
+            sim.step(1)
+            p0 = sim.field("p0")
+            assert p0.shape == w.shape
+            J += dt * float(np.sum(w * p0 * p0))
+        return J
+    finally:
+        sim.close()
