@@ -85,6 +85,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--primary", default="mixed", choices=["fp64", "mixed"])
     args = ap.parse_args()
@@ -342,6 +343,52 @@ def focal_mask(sim, cfg, radius=2e-3):
     return np.hypot((ii - 0.5) * d.dx, (jj - 0.5) * d.dy - fy) <= radius
 
 
+def adjoint_cost(cfg, args):
+    """Cost of crp_adjoint against the forward it differentiates, on the same
+    grid without bubbles (the adjoint's scope), FP64, 64 source elements: the
+    device time of focal_compare_step(cfg) forward steps from t = 0, then of
+    crp_adjoint over the same steps (its own forward with the focal record, the
+    objective and the reverse sweep), both with CUDA events on the simulation's
+    stream."""
+    import torch
+
+    import crp
+
+    c = crp.Config.from_buffer_copy(cfg)
+    c.bub_enable = 0
+    c.ext_precision = 0
+    c.ext_elements = 64
+    c.dbg_T = 0
+    steps = focal_compare_step(cfg)
+    rng = np.random.default_rng(0xC0DA0004)
+    amp, phase = rng.uniform(0.8, 1.2, 64), rng.uniform(-0.3, 0.3, 64)
+
+    def timed(fn, sim):
+        st = torch.cuda.ExternalStream(sim.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        out = fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    with crp.Sim(c) as fwd:
+        fwd.set_source_elements(amp, phase)
+        fwd.step(1)  # first-step set-up outside the timing, as below
+        ms_fwd, _ = timed(lambda: fwd.step(steps - 1), fwd)
+    with crp.Sim(c) as adj:
+        adj.set_source_elements(amp, phase)
+        ms_adj, (J, ga, gp) = timed(lambda: adj.adjoint(steps, 2.0e-3, 64), adj)
+    ms_fwd *= steps / (steps - 1)
+    return {"steps": steps, "focal_radius_m": 2.0e-3, "elements": 64, "precision": "fp64", "bubbles": 0,
+            "forward_ms": ms_fwd, "adjoint_ms": ms_adj, "adjoint_over_forward": ms_adj / ms_fwd,
+            "J": J, "grad_amp_norm": float(np.linalg.norm(ga)), "grad_phase_norm": float(np.linalg.norm(gp)),
+            "note": "crp_adjoint (its forward with the focal record, the objective and the reverse sweep) over "
+                    "the forward's device time on the same grid and steps; gradients checked against finite "
+                    "differences and the oracle in tests/test_adjoint_gpu.py"}
+
+
 def focal_compare_step(cfg):
     """Mixture step 100 steps after the focused burst reaches the focus: the
     source delays make every element's wave arrive there at t = focal_dist / c."""
@@ -452,6 +499,7 @@ def run_ours(args, rank, world, dist):
                "note": "wall clock: crp_create (seeded bubbles uploaded) + steps from t=0 + p0 and R_t "
                        "read back every bench step; the simulation's teardown is not included"}
 
+    adjoint = adjoint_cost(cfg, args) if rank == 0 and world == 1 and not args.no_adjoint else None
     driven = driven_sample(sim, args, cells, nb) if with_driven else None
     focal = None
     if driven is not None and len(runs) > 1:
@@ -483,6 +531,8 @@ def run_ours(args, rank, world, dist):
             result["driven"] = driven
         if e2e is not None:
             result["e2e"] = e2e
+        if adjoint is not None:
+            result["adjoint"] = adjoint
         for prec, r in runs.items():
             result[f"{prec}_path"] = {"value": cells * mix_steps * world / (r["ms"] * 1e-3) / 1e6,
                                       "ms_per_step": r["ms"] / args.steps,
