@@ -157,3 +157,18 @@ def test_unsupported_and_invalid():
     with crp.Sim(_cfg("ghost_row_focused")) as sim:
         with pytest.raises(crp.CrpError):
             sim.set_source_elements(np.ones(3), np.zeros(3))  # n must equal ext.elements
+
+
+def test_mixed_path_forward_gives_the_same_gradient():
+    """The reverse sweep is FP64 in both paths; with the mixed path's forward
+    (FP32 value + compensation fields) J and the gradient move only by that
+    storage's rounding."""
+    cfg64 = _cfg("source_row_ramp")
+    cfgmx = _cfg("source_row_ramp", ext_precision=1)
+    amp, phase = _params(cfg64.ext_elements)
+    J64, ga64, gp64 = gpu_objective(cfg64, amp, phase, grads=True)
+    Jmx, gamx, gpmx = gpu_objective(cfgmx, amp, phase, grads=True)
+    scale = max(np.abs(ga64).max(), np.abs(gp64).max())
+    assert abs(Jmx - J64) <= 1e-6 * J64
+    assert np.abs(gamx - ga64).max() <= 1e-6 * scale
+    assert np.abs(gpmx - gp64).max() <= 1e-6 * scale
