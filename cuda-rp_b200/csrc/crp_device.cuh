@@ -500,12 +500,22 @@ __device__ __forceinline__ void rp_substep(double& Rt, double& Rp, double& Rn, d
   remain -= dtp;
 }
 
-// Smooth delta (inc/bubble_CUDA_kernel.cuh:214-222).
-__device__ __forceinline__ double delta_x(const BubbleParams& b, const GridParams& g, int pos, double bx) {
-  return b.dcx * (1.0 + cos(b.dcy * (((double)pos - 0.5) * g.dx - bx)));
+// Smooth delta (inc/bubble_CUDA_kernel.cuh:214-222), band 2 (the only band
+// this path implements): delta(pos) = dcx (1 + cos(dcy ((pos - 1/2) dx - x))).
+// Adjacent points' arguments differ by dcy dx = pi, so the cosines of a
+// stencil's points alternate in sign: with c0 the cosine at one point p0,
+// delta(p0 + k) = dcx (1 + c0) for even k and dcx (1 - c0) for odd k.  Each
+// bubble then needs one cosine per axis instead of one per point (the values
+// move by a rounding at most).
+__device__ __forceinline__ double delta_cos_x(const BubbleParams& b, const GridParams& g, int pos, double bx) {
+  return cos(b.dcy * (((double)pos - 0.5) * g.dx - bx));
 }
-__device__ __forceinline__ double delta_y(const BubbleParams& b, const GridParams& g, int pos, double by) {
-  return b.dcx * (1.0 + cos(b.dcz * (((double)pos - 0.5) * g.dy - by)));
+__device__ __forceinline__ double delta_cos_y(const BubbleParams& b, const GridParams& g, int pos, double by) {
+  return cos(b.dcz * (((double)pos - 0.5) * g.dy - by));
+}
+// Weight of the point p0 + k, from c0 = delta_cos_* at p0 (any integer k).
+__device__ __forceinline__ double delta_w(const BubbleParams& b, double c0, int k) {
+  return b.dcx * (1.0 + ((k & 1) ? -c0 : c0));
 }
 
 }  // namespace crp

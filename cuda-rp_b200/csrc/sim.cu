@@ -437,18 +437,19 @@ __device__ __forceinline__ void move_one(const GridParams& g, const BubbleParams
   double x = b.x[n], y = b.y[n];
   int imx = b.ibmx[n], imy = b.ibmy[n], inx = b.ibnx[n], iny = b.ibny[n];
   double vlx = 0.0, vly = 0.0;
-  // Delta weights of the two rows/columns of each stencil (the same values the
-  // reference recomputes inside its loops).
-  const double dyn[2] = {delta_y(bp, g, iny, y), delta_y(bp, g, iny + 1, y)};
-  const double dym[2] = {delta_y(bp, g, imy - 1, y), delta_y(bp, g, imy, y)};
+  // Delta weights of the two rows/columns of each stencil, from one cosine per
+  // axis (delta_w).
+  const double cx0 = delta_cos_x(bp, g, imx - 1, x), cy0 = delta_cos_y(bp, g, imy - 1, y);
+  const double dyn[2] = {delta_w(bp, cy0, iny - (imy - 1)), delta_w(bp, cy0, iny + 1 - (imy - 1))};
+  const double dym[2] = {delta_w(bp, cy0, 0), delta_w(bp, cy0, 1)};
   for (int i = imx - 1; i <= imx; i++) {
-    double dxw = delta_x(bp, g, i, x);
+    double dxw = delta_w(bp, cx0, i - (imx - 1));
     for (int j = iny; j <= iny + 1; j++) {
       if (i >= -1 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) vlx += vx.get(f.idx(i, j)) * dxw * dyn[j - iny];
     }
   }
   for (int i = inx; i <= inx + 1; i++) {
-    double dxw = delta_x(bp, g, i, x);
+    double dxw = delta_w(bp, cx0, i - (imx - 1));
     for (int j = imy - 1; j <= imy; j++) {
       if (i >= 0 && i <= f.X + 1 && j >= -1 && j <= f.Y + 1) vly += vy.get(f.idx(i, j)) * dxw * dym[j - imy + 1];
     }
@@ -632,12 +633,13 @@ __device__ __forceinline__ void rp_begin(const GridParams& g, const BubbleParams
   const double x = b.x[n], y = b.y[n];
   const int inx = b.ibnx[n], iny = b.ibny[n];
   double PLp = 0.0;
+  const double cx0 = delta_cos_x(bp, g, inx, x), cy0 = delta_cos_y(bp, g, iny, y);
   for (int qi = 0; qi < 2; qi++) {
     const int i = inx + qi;
-    const double dxw = delta_x(bp, g, i, x);
+    const double dxw = delta_w(bp, cx0, qi);
     for (int qj = 0; qj < 2; qj++) {
       const int j = iny + qj;
-      const double dyw = delta_y(bp, g, j, y);
+      const double dyw = delta_w(bp, cy0, qj);
       if (i >= 0 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) PLp += p0_at(g, px, py, i, j, t_cur) * dxw * dyw;
     }
   }
@@ -726,8 +728,9 @@ __device__ __forceinline__ void rp_end(const GridParams& g, const BubbleParams& 
   b.nsub[n] = (int)min(s.count, (long long)INT32_MAX);
   const double x = b.x[n], y = b.y[n];
   const int inx = b.ibnx[n], iny = b.ibny[n];
-  const double dx0 = delta_x(bp, g, inx, x), dx1 = delta_x(bp, g, inx + 1, x);
-  const double dy0 = delta_y(bp, g, iny, y), dy1 = delta_y(bp, g, iny + 1, y);
+  const double cx0 = delta_cos_x(bp, g, inx, x), cy0 = delta_cos_y(bp, g, iny, y);
+  const double dx0 = delta_w(bp, cx0, 0), dx1 = delta_w(bp, cx0, 1);
+  const double dy0 = delta_w(bp, cy0, 0), dy1 = delta_w(bp, cy0, 1);
   const double Rt = s.Rt;
   const double vol = g.cyl ? bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy / x
                            : bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy;
@@ -1022,8 +1025,9 @@ __global__ void heat_contrib(const __grid_constant__ GridParams g, const __grid_
   const double x = b.x[n], y = b.y[n];
   const int inx = b.ibnx[n], iny = b.ibny[n];
   const double q = g.cyl ? b.n_B[n] * b.Q_B[n] * g.rdx * g.rdy / x : b.n_B[n] * b.Q_B[n] * g.rdx * g.rdy;
-  const double dx0 = delta_x(bp, g, inx, x), dx1 = delta_x(bp, g, inx + 1, x);
-  const double dy0 = delta_y(bp, g, iny, y), dy1 = delta_y(bp, g, iny + 1, y);
+  const double cx0 = delta_cos_x(bp, g, inx, x), cy0 = delta_cos_y(bp, g, iny, y);
+  const double dx0 = delta_w(bp, cx0, 0), dx1 = delta_w(bp, cx0, 1);
+  const double dy0 = delta_w(bp, cy0, 0), dy1 = delta_w(bp, cy0, 1);
   const int p = b.pos[n];
   if (p < 0) return;
   double* c = hc + 4 * (long)p;
@@ -2518,9 +2522,10 @@ __global__ void bubble_contrib(const __grid_constant__ GridParams g, const __gri
   const double x = b.x[n], y = b.y[n];
   const int inx = b.ibnx[n], iny = b.ibny[n];
   double dxw[2], dyw[2];
+  const double cx0 = delta_cos_x(bp, g, inx, x), cy0 = delta_cos_y(bp, g, iny, y);
   for (int q = 0; q < 2; q++) {
-    dxw[q] = delta_x(bp, g, inx + q, x);
-    dyw[q] = delta_y(bp, g, iny + q, y);
+    dxw[q] = delta_w(bp, cx0, q);
+    dyw[q] = delta_w(bp, cy0, q);
   }
   const double Rt = b.R_t[n];
   const double vol = g.cyl ? bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy / x
