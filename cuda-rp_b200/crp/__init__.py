@@ -245,13 +245,21 @@ class Sim:
         self._check(self.lib.crp_get_stats(self.h, ctypes.byref(s)))
         return s
 
-    def field(self, name: str) -> np.ndarray:
-        out = np.empty(field_shape(self.dims, name), dtype=np.float64)
+    def field(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        """Dense copy of a field; into `out` (float64, C-contiguous, the field's
+        shape) when given, e.g. a pinned host buffer."""
+        shape = field_shape(self.dims, name)
+        if out is None:
+            out = np.empty(shape, dtype=np.float64)
+        assert out.shape == shape and out.dtype == np.float64 and out.flags.c_contiguous
         self._check(self.lib.crp_read_field(self.h, FIELDS[name], _ptr(out)))
         return out
 
-    def bubbles(self, name: str) -> np.ndarray:
-        out = np.empty(self.dims.num_bubbles, dtype=np.float64)
+    def bubbles(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        """One bubble quantity; into `out` (float64, num_bubbles) when given."""
+        if out is None:
+            out = np.empty(self.dims.num_bubbles, dtype=np.float64)
+        assert out.shape == (self.dims.num_bubbles,) and out.dtype == np.float64 and out.flags.c_contiguous
         self._check(self.lib.crp_read_bubbles(self.h, BUBBLE_FIELDS[name], _ptr(out)))
         return out
 
