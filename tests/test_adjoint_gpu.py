@@ -6,7 +6,7 @@ of the FDTD/PML step, against
   quadratic in them, so the difference quotient is exact up to rounding;
   phases: h = 1e-4 rad, truncation O(h^2));
 - an FP64 reference gradient: central finite differences of J on the CPU
-  oracle (the north star's bar: within 1e-3 relative);
+  oracle (the accuracy bar: within 1e-3 relative);
 - torch.autograd.gradcheck through a thin torch.autograd.Function whose
   backward is crp_adjoint (only here, for the gradient tests).
 
