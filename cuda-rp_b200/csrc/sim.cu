@@ -928,22 +928,17 @@ struct CoupleArgs {
 // kCoupleW x 8 cells.
 constexpr int kCoupleW = 8;
 
+// One tile of kCoupleW x 8 cells (tile (tx, ty) of the box [i0, i1] x [j0, j1]):
+// returns this thread's residual |dp0| (0 where it updates nothing; NaN sorts
+// above every number in the bit-pattern maximum taken by the caller).
 template <typename P>
-__global__ void __launch_bounds__(256) couple_press(const __grid_constant__ GridParams g, const CoupleArgs<P> a) {
+__device__ __forceinline__ double couple_tile(const GridParams& g, const CoupleArgs<P>& a, int i0, int j0, int i1,
+                                              int j1, int tx, int ty) {
   const Frame& f = g.f;
   const int X = f.X, Y = f.Y;
-  int i0 = a.i0, j0 = a.j0, i1 = a.i1, j1 = a.j1;
-  if (a.dbox) {
-    i0 = a.dbox[0];
-    j0 = a.dbox[1];
-    i1 = a.dbox[2];
-    j1 = a.dbox[3];
-    // Launched over the whole window: blocks past the box leave at once.
-    if (i0 + (int)(blockIdx.x * kCoupleW) > i1 || j0 + (int)(blockIdx.y * blockDim.y) > j1) return;
-  }
   const int bin = threadIdx.x & 3;
-  const int i = i0 + blockIdx.x * kCoupleW + (threadIdx.x >> 2);
-  const int j = j0 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = i0 + tx * kCoupleW + (threadIdx.x >> 2);
+  const int j = j0 + ty * blockDim.y + threadIdx.y;
   const bool in = i <= i1 && j <= j1;
   double fgv = 0.0;
   if (in) {
@@ -972,7 +967,26 @@ __global__ void __launch_bounds__(256) couple_press(const __grid_constant__ Grid
       a.py.put(k, qy);
     }
   }
-  block_max_to(res, a.residual);
+  return res;
+}
+
+// Host-driven steps launch one block per tile of the box.  Graph steps, whose
+// box is decided on the device (dbox), launch a fixed grid whose blocks stride
+// over the box's tiles.
+template <typename P>
+__global__ void __launch_bounds__(256) couple_press(const __grid_constant__ GridParams g, const CoupleArgs<P> a) {
+  unsigned long long rb = 0ull;  // max |dp0| as a bit pattern
+  if (a.dbox) {
+    const int i0 = a.dbox[0], j0 = a.dbox[1], i1 = a.dbox[2], j1 = a.dbox[3];
+    if (i0 <= i1 && j0 <= j1) {
+      const int tw = (i1 - i0 + kCoupleW) / kCoupleW, th = (j1 - j0 + (int)blockDim.y) / (int)blockDim.y;
+      for (int t = blockIdx.x; t < tw * th; t += gridDim.x)  // the same trip count in every thread of a block
+        rb = max(rb, (unsigned long long)__double_as_longlong(couple_tile(g, a, i0, j0, i1, j1, t % tw, t / tw)));
+    }
+  } else {
+    rb = (unsigned long long)__double_as_longlong(couple_tile(g, a, a.i0, a.j0, a.i1, a.j1, blockIdx.x, blockIdx.y));
+  }
+  block_max_to(__longlong_as_double((long long)rb), a.residual);
 }
 
 // p0 with its boundary values into a dense (X+2) x (Y+2) array, for readback.
@@ -1495,6 +1509,7 @@ struct Sim {
     int* order;   // n
   } lpt{};
   int rp_grid = 1;
+  int couple_graph_grid = 1;  // blocks of the graph steps' coupling launch (striding over the box's tiles)
 
   MinMax mm;       // running min/max of written rawdata values
   int cur_v = 0;   // velocity buffer holding the latest velocities
@@ -1633,6 +1648,7 @@ struct Sim {
       else
         CRP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bubble_rp<PrecFP64>, kRpThreads, 0));
       rp_grid = std::max(1, std::min(sms * std::max(per_sm, 1), (hs.nb + kRpThreads - 1) / kRpThreads));
+      couple_graph_grid = 4 * sms;
     }
     // PML profiles and metrics.
     CRP_CUDA(cudaMemcpyAsync(d_sigma, hs.sigma_block.data(), sizeof(double) * hs.sigma_block.size(),
@@ -2592,8 +2608,7 @@ cudaError_t Sim::launch_couple_t(bool pressure) {
     ca.i1 = gp.f.X + 1;
     ca.j1 = gp.f.Y + 1;
     ca.dbox = d_scalars->box;
-    dim3 grd((gp.f.X + 2 + kCoupleW - 1) / kCoupleW, (gp.f.Y + 2 + 7) / 8);
-    return launch(kClassCouple, [&] { couple_press<P><<<grd, blk, 0, stream>>>(gp, ca); });
+    return launch(kClassCouple, [&] { couple_press<P><<<couple_graph_grid, blk, 0, stream>>>(gp, ca); });
   }
   if (pressure) {
     const Box& b = couple_box;
