@@ -1278,10 +1278,21 @@ struct Scalars {
 };
 
 // Fast2Sum time step (src/bubble_CUDA.cu:208-212), written by the host path.
+// Start of a host-driven step: the step's times, and the residual and the
+// bubble-motion flags cleared (one launch instead of a kernel and two memsets).
 __global__ void set_time(Scalars* s, double t_prev, double t, double carry) {
   s->t[0] = t_prev;
   s->t[1] = t;
   s->t[2] = carry;
+  s->residual = 0ull;
+  s->moved = 0;
+  for (int k = 0; k < 4; k++) s->bbox[k] = 0;
+}
+// Start of a Picard iteration of a host-driven step: residual and work-queue
+// head cleared.
+__global__ void picard_begin(Scalars* s) {
+  s->residual = 0ull;
+  s->next = 0;
 }
 
 struct CtlParams {
@@ -1885,8 +1896,6 @@ struct Sim {
     const int nv = cur_v ^ 1, np = cur_p ^ 1;
     // Ring rotation of store_variables: the predicted f_g goes to the f_gm buffer.
     const int a = fg_a, b = fg_b, c = fg_c;
-    CRP_CUDA(cudaMemsetAsync(d_residual, 0, sizeof(unsigned long long), stream));
-    CRP_CUDA(cudaMemsetAsync(d_moved, 0, sizeof(int) * 5, stream));
     CRP_CUDA(mixed ? launch_fdtd<PrecMixed>(nv, np, a, b, c) : launch_fdtd<PrecFP64>(nv, np, a, b, c));
     cur_v = nv;
     cur_p = np;
@@ -1915,8 +1924,7 @@ struct Sim {
       while (resimax > picard_tol) {
         if (loop >= cfg.ext_picard_cap) return fail(CRP_ERR_PICARD, "Picard iteration cap reached");
         loop++;
-        CRP_CUDA(cudaMemsetAsync(d_residual, 0, sizeof(unsigned long long), stream));
-        CRP_CUDA(cudaMemsetAsync(d_next, 0, sizeof(int), stream));
+        CRP_CUDA(launch(kClassOther, [&] { picard_begin<<<1, 1, 0, stream>>>(d_scalars); }));
         CRP_CUDA(mixed ? launch_rp<PrecMixed>() : launch_rp<PrecFP64>());
         CRP_CUDA(launch_couple(true));
         st = read_scalars();
