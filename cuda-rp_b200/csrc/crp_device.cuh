@@ -314,15 +314,22 @@ template <typename R>
 __device__ __forceinline__ bool above_series_cut(Cx<R> a, R cut2) {
   return a.re * a.re + a.im * a.im >= cut2;
 }
-// coth(a) = N / D with N = (1, tanh(re) tan(im)) and D = (tanh(re), tan(im))
-// (inc/complex.cuh's coth before its division).  Callers fold the division into
-// their own, so a sub-step carries one complex division per Upsilon / Lp
-// evaluation on its critical path instead of three.
+// coth(a) = N / D for Re a >= 0 (every argument here is (s, s), s >= 0):
+// N = 1 + E, D = 1 - E with E = exp(-2a) = exp(-2 re) (cos 2 im - i sin 2 im).
+// The reference evaluates coth as (1, tanh(re) tan(im)) / (tanh(re), tan(im))
+// (inc/complex.cuh); this form needs one exp and one sincos instead of a tanh
+// and a tan (whose range reduction and pole at pi/2 sit on the sub-step's
+// critical path), and cannot overflow.  Callers fold the division into their
+// own and use N and D only in ratios homogeneous in the pair, so a sub-step
+// carries one complex division per Upsilon / Lp evaluation.
 template <typename R>
 __device__ __forceinline__ void coth_parts(Cx<R> a, Cx<R>& N, Cx<R>& D) {
-  const R x = tanh(a.re), y = tan(a.im);
-  N = Cx<R>{R(1), x * y};
-  D = Cx<R>{x, y};
+  const R m = exp(R(-2) * a.re);
+  R sn, cs;
+  sincos(R(2) * a.im, &sn, &cs);
+  const R er = m * cs, ei = -m * sn;
+  N = Cx<R>{R(1) + er, ei};
+  D = Cx<R>{R(1) - er, -ei};
 }
 using C64 = Cx<double>;
 
