@@ -78,7 +78,7 @@ struct BubbleParams {
   // sub-step's critical path, deciding exactly as the square root would.
   double abs2_cut64;
   float abs2_cut32;
-  float rho32, sig32, mu32, gam32;  // FP32 copies for the mixed path's thermal model
+  float rho32, sig32, mu32, gam32, inv_rho32;  // FP32 copies for the mixed path's thermal model
   double pi, pi4r3;
   double dcx, dcy, dcz;  // delta_coef (src/bubble_CUDA.cu:1469-1471)
   long long step_cap;
@@ -291,15 +291,16 @@ template <typename R>
 __device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
   return {a.re * b.re - a.im * b.im, a.im * b.re + a.re * b.im};
 }
+// Complex quotients with one real division (the reciprocal of |b|^2).
 template <typename R>
 __device__ __forceinline__ Cx<R> cdiv(Cx<R> a, Cx<R> b) {
-  R c = b.re * b.re + b.im * b.im;
-  return {xdiv(a.re * b.re + a.im * b.im, c), xdiv(a.im * b.re - a.re * b.im, c)};
+  const R ic = xdiv(R(1), b.re * b.re + b.im * b.im);
+  return {(a.re * b.re + a.im * b.im) * ic, (a.im * b.re - a.re * b.im) * ic};
 }
 template <typename R>
 __device__ __forceinline__ Cx<R> rdiv(R a, Cx<R> b) {
-  R c = b.re * b.re + b.im * b.im;
-  return {xdiv(a * b.re, c), xdiv(-a * b.im, c)};
+  const R ic = xdiv(R(1), b.re * b.re + b.im * b.im);
+  return {(a * b.re) * ic, (-a * b.im) * ic};
 }
 template <typename R>
 __device__ __forceinline__ Cx<R> cscl(Cx<R> a, R s) {
@@ -336,8 +337,8 @@ using C64 = Cx<double>;
 // Per-bubble constants derived from its R0 (init_bub_params, src/bubble_CUDA.cu:666-670).
 struct BubbleR0 {
   double R0, PG0, R03, coeff_alpha, inv_R0, inv_PG0;
-  double T0_PG0R03;          // T0 / (PG0 R0^3) of the heat flux
-  float R0_32, PG0_32, ca32;  // FP32 copies for the mixed path's thermal model
+  double T0_PG0R03;                      // T0 / (PG0 R0^3) of the heat flux
+  float PG0_32, ca32, inv_R0_32;  // FP32 copies for the mixed path's thermal model
 };
 __device__ __forceinline__ BubbleR0 bubble_r0(const BubbleParams& b, double R0) {
   BubbleR0 r;
@@ -348,9 +349,9 @@ __device__ __forceinline__ BubbleR0 bubble_r0(const BubbleParams& b, double R0) 
   r.inv_PG0 = 1.0 / r.PG0;
   r.coeff_alpha = b.gam * r.PG0 * r.R03 / (2.0 * (b.gam - 1.0) * b.T0 * b.K0);
   r.T0_PG0R03 = b.T0 / (r.PG0 * r.R03);
-  r.R0_32 = (float)R0;
   r.PG0_32 = (float)r.PG0;
   r.ca32 = (float)r.coeff_alpha;
+  r.inv_R0_32 = (float)r.inv_R0;
   return r;
 }
 
@@ -415,13 +416,13 @@ __device__ __forceinline__ float series_cut<float>(const BubbleParams& b) {
 // Constants of the thermal model in its real type.
 template <typename R>
 struct ThermalConst {
-  R rho, sig, mu, gam, ca, R0, PG0, cut2;
+  R rho, sig, mu, gam, ca, inv_R0, PG0, cut2, inv_rho;
 };
 __device__ __forceinline__ ThermalConst<double> thermal_const64(const BubbleParams& b, const BubbleR0& r) {
-  return {b.rho, b.sig, b.mu, b.gam, r.coeff_alpha, r.R0, r.PG0, b.abs2_cut64};
+  return {b.rho, b.sig, b.mu, b.gam, r.coeff_alpha, r.inv_R0, r.PG0, b.abs2_cut64, b.inv_rho};
 }
 __device__ __forceinline__ ThermalConst<float> thermal_const32(const BubbleParams& b, const BubbleR0& r) {
-  return {b.rho32, b.sig32, b.mu32, b.gam32, r.ca32, r.R0_32, r.PG0_32, b.abs2_cut32};
+  return {b.rho32, b.sig32, b.mu32, b.gam32, r.ca32, r.inv_R0_32, r.PG0_32, b.abs2_cut32, b.inv_rho32};
 }
 
 // solveOmegaN (:263-288): omega_N and alpha_N for gas pressure PG at radius Rb.
@@ -429,18 +430,20 @@ template <typename R>
 __device__ __forceinline__ R omega_n(Cx<R>& alpha, R PG, R Rb, const ThermalConst<R>& c) {
   const R eps = R(2.22044604925031308e-016);
   const R rho = c.rho, sig = c.sig, mu = c.mu, gam = c.gam, ca = c.ca;
-  R Rx = xdiv(Rb, c.R0);
+  // One division for the five quotients by the radius.
+  const R inv_Rb = xdiv(R(1), Rb);
+  R Rx = Rb * c.inv_R0;
   R coef1 = xdiv(c.PG0, PG * Rx * Rx * Rx);
   R coef2 = PG * rho;
-  R coef3 = xdiv(R(4), Rb * Rb);
-  R value1 = xdiv(R(-2) * sig * rho, Rb);
+  R coef3 = R(4) * inv_Rb * inv_Rb;
+  R value1 = R(-2) * sig * rho * inv_Rb;
   R ups_re = R(3) * gam * coef1;
   R mu_eff = mu;
   R eta = ups_re * coef2 + value1 - mu_eff * mu_eff * coef3;
   // Loop invariants as reciprocals/quotients, so that the iteration's chain is
   // sqrt -> Upsilon (one division) -> sqrt.
-  const R inv_rho_Rb = xdiv(R(1), rho * Rb);
-  const R ca_Rb = xdiv(ca, Rb);
+  const R inv_rho_Rb = c.inv_rho * inv_Rb;
+  const R ca_Rb = ca * inv_Rb;
   R omega = sqrt(fmax(eta, R(1.0e-6) * eps)) * inv_rho_Rb;
   for (int k = 0; k < 3; k++) {
     R s = sqrt(ca_Rb * omega);

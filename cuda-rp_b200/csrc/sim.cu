@@ -1771,6 +1771,7 @@ struct Sim {
       bp.sig32 = (float)bp.sig;
       bp.mu32 = (float)bp.mu;
       bp.gam32 = (float)bp.gam;
+      bp.inv_rho32 = (float)bp.inv_rho;
     }
     bp.K0 = cfg.bub_K0;
     bp.dt0 = d.bub_dt0;
