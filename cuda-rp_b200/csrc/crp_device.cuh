@@ -458,23 +458,24 @@ __device__ __forceinline__ R omega_n(Cx<R>& alpha, R PG, R Rb, const ThermalCons
   return omega;
 }
 
-// solvePG (:326-340).  inv_den = 1 / |Lp|^2 and inv_wdt = 1 / (omega dt),
-// shared with the heat flux of the same sub-step.
+// solvePG (:326-340), with the reference's c1, c2, c3 and numerator multiplied
+// by den = |Lp|^2, so that Lp = (lpr, lpi) |Lp|^2 enters without a division of
+// its own and the gas pressure costs one division on the sub-step's critical
+// path.  inv_wdt = 1 / (omega dt), shared with the heat flux of the sub-step.
 __device__ __forceinline__ double gas_pressure(double PGn, double Rp, double Rn, double inv_wdt, double dt,
-                                               double inv_den, C64 lp, const BubbleParams& b, const BubbleR0& r) {
+                                               double den, C64 lp, const BubbleParams& b, const BubbleR0& r) {
   double R = 0.5 * (Rp + Rn);
   double Rx = R * r.inv_R0;
   double Rpx = Rp * r.inv_R0;
   double Rnx = Rn * r.inv_R0;
   const double inv_R = 1.0 / R;
-  double lpr = lp.re * inv_den;
-  double lpi = lp.im * inv_den;
   double c0 = dt * 3.0 * (b.gam - 1.0) * b.K0 * b.T0 * inv_R * r.inv_PG0;
-  double c3 = 1.5 * b.gam * (Rp - Rn) * inv_R + c0 * lpr * 0.5 * Rx * Rx * Rx;
-  const double w = c0 * lpi * inv_wdt;
-  double c1 = 1.0 + c3 - w * Rpx * Rpx * Rpx;
-  double c2 = 1.0 - c3 - w * Rnx * Rnx * Rnx;
-  return (c2 * PGn + c0 * lpr * r.PG0) / c1;
+  const double g = 1.5 * b.gam * (Rp - Rn) * inv_R;      // c3 without its Lp term
+  const double a3 = c0 * lp.re * 0.5 * Rx * Rx * Rx;     // den x (c3 - g)
+  const double wn = c0 * lp.im * inv_wdt;                 // den x w
+  const double c1 = den * (1.0 + g) + a3 - wn * Rpx * Rpx * Rpx;
+  const double c2 = den * (1.0 - g) - a3 - wn * Rnx * Rnx * Rnx;
+  return (c2 * PGn + c0 * lp.re * r.PG0) / c1;
 }
 
 // solveRayleighPlesset (:227-260): one variable sub-step of the three-level scheme.

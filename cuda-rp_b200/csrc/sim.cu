@@ -697,9 +697,10 @@ __device__ __forceinline__ void rp_substep_full(const BubbleParams& bp, RpState&
     thermal_model<double>(bp, s, PGn, omega, lp);
   else
     thermal_model<T>(bp, s, PGn, omega, lp);
-  const double inv_den = 1.0 / (lp.re * lp.re + lp.im * lp.im);
+  const double den = lp.re * lp.re + lp.im * lp.im;
   const double inv_wdt = 1.0 / (omega * s.dtL);
-  s.PGp = gas_pressure(PGn, s.Rp, s.Rn, inv_wdt, s.dtL, inv_den, lp, bp, s.r);
+  s.PGp = gas_pressure(PGn, s.Rp, s.Rn, inv_wdt, s.dtL, den, lp, bp, s.r);
+  const double inv_den = 1.0 / den;  // for the heat flux only, off the chain to the next sub-step
   const double Rp = s.Rp, Rn = s.Rn, PGp = s.PGp;
   const double s0 = 0.5 * (Rp + Rn);
   const double s1 = inv_den * s.r.T0_PG0R03;
