@@ -1295,6 +1295,21 @@ __global__ void picard_begin(Scalars* s) {
   s->residual = 0ull;
   s->next = 0;
 }
+// The first Picard iteration's start, launched with the radius solve before the
+// host has read the prediction's residual: the iteration runs when the host
+// will run it (residual above the tolerance, computed as the host computes it,
+// and no bubble changed bin, so the bins stand).  Otherwise the work queue is
+// left closed (head at n) and the radius solve returns without touching a
+// bubble; the host then rebuilds the bins and starts the loop itself, or skips it.
+__global__ void picard_gate(Scalars* s, double P_inf, double tol, int n) {
+  const double r = __longlong_as_double((long long)s->residual) / P_inf;
+  if (r > tol && s->moved == 0) {
+    s->residual = 0ull;
+    s->next = 0;
+  } else {
+    s->next = n;
+  }
+}
 
 struct CtlParams {
   double tol, P_inf, dt, stall;
@@ -1479,6 +1494,7 @@ struct Sim {
   int* d_next = nullptr;
   int* d_moved = nullptr;
   Scalars* h_scalars = nullptr;  // pinned
+  cudaEvent_t ev_scalars = nullptr;  // the prediction's scalars have reached h_scalars
   double picard_tol = 1.0e-7f;
   // Cell boxes {i0, j0, i1, j1} (empty when i0 > i1).  supp[q] bounds the
   // nonzero void fraction of step n-1-q; the coupling kernel updates only the
@@ -1644,6 +1660,8 @@ struct Sim {
     layout(false);
     CRP_CUDA(cudaMemsetAsync(pool, 0, pool_bytes, stream));
     CRP_CUDA(cudaMallocHost(&h_scalars, sizeof(Scalars)));
+    std::memset(h_scalars, 0, sizeof(Scalars));
+    CRP_CUDA(cudaEventCreateWithFlags(&ev_scalars, cudaEventDisableTiming));
     CRP_CUDA(cudaMallocHost(&h_focal, 2 * sizeof(double)));
     // Control system start (src/bubble_CUDA.cu:123-153): the first tracked
     // point is (0, 0); the first control point is the focus the source uses.
@@ -1905,29 +1923,51 @@ struct Sim {
     fg_b = a;  // f_gn
     fg_c = b;  // f_gm
     if (hs.nb > 0) CRP_CUDA(mixed ? launch_move<PrecMixed>() : launch_move<PrecFP64>());
-    crp_status st = read_scalars();
-    if (st != CRP_OK) return st;
+    // The first radius solve is queued right behind the read-back of the
+    // prediction's scalars, and picard_gate decides on the device whether it
+    // runs, so that the GPU does not idle while the host decides.  Not while
+    // the bins are already known to be stale: the solve stores each bubble's
+    // contributions at its place in the bins.  The solve order depends only on
+    // the sub-step counts of earlier solves, known before this read-back.
+    // Bins change only when a bubble crosses into another cell; the order is
+    // left as it is while no bubble has needed more than kLptMinSubsteps
+    // sub-steps (all equal: the order cannot shorten the launch).
+    const long long substep_prev = h_scalars->substep_max;
+    const bool ahead = hs.nb > 0 && !bins_stale && cfg.ext_picard_cap > 0;
+    CRP_CUDA(cudaMemcpyAsync(h_scalars, d_scalars, sizeof(Scalars), cudaMemcpyDeviceToHost, stream));
+    if (ahead) {
+      CRP_CUDA(cudaEventRecord(ev_scalars, stream));
+      if (substep_prev > kLptMinSubsteps) CRP_CUDA(build_order());
+      CRP_CUDA(launch(kClassOther,
+                      [&] { picard_gate<<<1, 1, 0, stream>>>(d_scalars, gp.P_inf, picard_tol, hs.nb); }));
+      CRP_CUDA(mixed ? launch_rp<PrecMixed>() : launch_rp<PrecFP64>());
+      CRP_CUDA(cudaEventSynchronize(ev_scalars));
+    } else {
+      CRP_CUDA(cudaStreamSynchronize(stream));
+      prof.resolve();
+    }
+    crp_status st = CRP_OK;
     double resimax = __longlong_as_double_host(h_scalars->residual) / gp.P_inf;
     int loop = 0;
+    // picard_gate's decision: the first iteration's solve is already queued.
+    const bool first_queued = ahead && resimax > picard_tol && h_scalars->moved == 0;
     bins_stale = bins_stale || h_scalars->moved != 0;
     const Box bnow = hs.nb > 0 ? bubble_box() : Box{1, 1, 0, 0};
     couple_box = box_union(box_union(bnow, supp[0]), box_union(supp[1], supp[2]));
-    if (hs.nb > 0 && resimax > picard_tol) {
-      // Bins change only when a bubble crosses into another cell; the solve
-      // order follows the latest sub-step counts, and is left as it is while
-      // no bubble has needed more than kLptMinSubsteps sub-steps (all equal:
-      // the order cannot shorten the launch).
+    if (hs.nb > 0 && resimax > picard_tol && !first_queued) {
       if (bins_stale) CRP_CUDA(build_bins());
       bins_stale = false;
-      if (h_scalars->substep_max > kLptMinSubsteps) CRP_CUDA(build_order());
+      if (!ahead && substep_prev > kLptMinSubsteps) CRP_CUDA(build_order());
     }
     if (hs.nb > 0) {
       double prev = resimax;
       while (resimax > picard_tol) {
         if (loop >= cfg.ext_picard_cap) return fail(CRP_ERR_PICARD, "Picard iteration cap reached");
         loop++;
-        CRP_CUDA(launch(kClassOther, [&] { picard_begin<<<1, 1, 0, stream>>>(d_scalars); }));
-        CRP_CUDA(mixed ? launch_rp<PrecMixed>() : launch_rp<PrecFP64>());
+        if (!(first_queued && loop == 1)) {
+          CRP_CUDA(launch(kClassOther, [&] { picard_begin<<<1, 1, 0, stream>>>(d_scalars); }));
+          CRP_CUDA(mixed ? launch_rp<PrecMixed>() : launch_rp<PrecFP64>());
+        }
         CRP_CUDA(launch_couple(true));
         st = read_scalars();
         if (st != CRP_OK) return st;
@@ -1941,6 +1981,11 @@ struct Sim {
         }
         prev = resimax;
       }
+    }
+    if (ahead && loop == 0 && prof.on) {
+      // The gated solve and its timing events are still in flight.
+      CRP_CUDA(cudaStreamSynchronize(stream));
+      prof.resolve();
     }
     if (std::isnan(resimax)) return fail(CRP_ERR_NONFINITE, "non-finite pressure");
     if (temperature_on) {
@@ -2535,6 +2580,7 @@ struct Sim {
     if (h_push) cudaFreeHost(h_push);
     if (pool) cudaFree(pool);
     if (h_scalars) cudaFreeHost(h_scalars);
+    if (ev_scalars) cudaEventDestroy(ev_scalars);
     if (h_focal) cudaFreeHost(h_focal);
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
