@@ -5,9 +5,11 @@
 //                  boundary overrides (VelocityKernel, VelocityBoundaryKernel),
 //                  first pressure evaluation (MixturePressureKernel) and its
 //                  residual, one HBM pass in column strips
-//   vghost         velocity ghost cells (the rest of VelocityBoundaryKernel)
+//   vghost         velocity ghost cells (the rest of VelocityBoundaryKernel),
+//                  a launch of its own only without bubbles
 //   bubble_move    bubble state rotation (store_variables), velocity gather,
-//                  motion, cell indices, occupied-bin box
+//                  motion, cell indices, occupied-bin box; its last blocks
+//                  write the velocity ghost cells
 //   bin_*          counting sort of bubbles by cell (deterministic order), only
 //                  when a bubble changed cell
 //   lpt_*          radius-solve order, heaviest sub-step counts first
@@ -356,12 +358,12 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
 
 // Velocity ghost cells (VelocityBoundaryKernel, inc/bubble_CUDA_kernel.cuh:701-811,
 // the parts outside the faces the update computes).  Each value is written in
-// closed form from computed faces, in the section order of the reference.
+// closed form from computed faces, in the section order of the reference;
+// thread k of the launch writes the k-th cell of each ghost row and column.
 template <typename V>
-__global__ void vghost(const __grid_constant__ GridParams g, const V vx, const V vy) {
+__device__ __forceinline__ void vghost_cells(const GridParams& g, const V& vx, const V& vy, int k) {
   const Frame& f = g.f;
   const int X = f.X, Y = f.Y;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
   // vx after the x-face section (:702-721), for rows 1..Y.
   auto vxA = [&](int i, int j) -> double {
     if (i == -1) return g.pml_x0 ? 0.0 : vx.get(f.idx(1, j));
@@ -389,6 +391,43 @@ __global__ void vghost(const __grid_constant__ GridParams g, const V vx, const V
     // The X1 mirror reads row X+1 of the array, logical (X, X) (:808).
     vy.put(f.idx(X + 1, j), (X <= Y + 1) ? vyC(X, X) : vyC(X, j));
   }
+}
+
+// Threads for vghost_cells: max(X, Y) + 3 cover every ghost row and column.
+__host__ __device__ __forceinline__ int vghost_threads(const Frame& f) { return (f.X > f.Y ? f.X : f.Y) + 3; }
+
+template <typename V>
+__global__ void vghost(const __grid_constant__ GridParams g, const V vx, const V vy) {
+  vghost_cells(g, vx, vy, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The values vghost_cells leaves in the ghost cells, formed from the computed
+// faces (and the stored value where it writes none), so that a kernel can read
+// the velocity stencil in the same launch that writes the ghost cells.  Copies
+// and sign changes only: equal to what a read after vghost_cells returns.
+template <typename V>
+__device__ __forceinline__ double vx_final(const GridParams& g, const V& vx, int i, int j) {
+  const Frame& f = g.f;
+  const int X = f.X, Y = f.Y;
+  if (j == 0 || j == Y + 1) j = j == 0 ? 1 : Y;  // rows 0 and Y+1: vxA(i, 1), vxA(i, Y)
+  else if (!((i == -1 && !g.pml_x0) || (i == X + 1 && !g.pml_x1))) return vx.get(f.idx(i, j));
+  if (i == -1) return g.pml_x0 ? 0.0 : vx.get(f.idx(1, j));
+  if (i == X + 1) return g.pml_x1 ? 0.0 : -vx.get(f.idx(X - 1, j));
+  return vx.get(f.idx(i, j));
+}
+template <typename V>
+__device__ __forceinline__ double vy_final(const GridParams& g, const V& vy, int i, int j) {
+  const Frame& f = g.f;
+  const int X = f.X, Y = f.Y;
+  if (i == 0) i = 1;  // column 0: vyC(1, j)
+  else if (i == X + 1) {  // column X+1: vyC(X, X) or vyC(X, j)
+    if (X <= Y + 1) j = X;
+    i = X;
+  } else if (j != Y + 1 || g.pml_y1) {
+    return vy.get(f.idx(i, j));
+  }
+  if (j == Y + 1) return g.pml_y1 ? 0.0 : vy.get(f.idx(i, Y - 1));
+  return vy.get(f.idx(i, j));
 }
 
 struct BubbleArrays {
@@ -445,13 +484,13 @@ __device__ __forceinline__ void move_one(const GridParams& g, const BubbleParams
   for (int i = imx - 1; i <= imx; i++) {
     double dxw = delta_w(bp, cx0, i - (imx - 1));
     for (int j = iny; j <= iny + 1; j++) {
-      if (i >= -1 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) vlx += vx.get(f.idx(i, j)) * dxw * dyn[j - iny];
+      if (i >= -1 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) vlx += vx_final(g, vx, i, j) * dxw * dyn[j - iny];
     }
   }
   for (int i = inx; i <= inx + 1; i++) {
     double dxw = delta_w(bp, cx0, i - (imx - 1));
     for (int j = imy - 1; j <= imy; j++) {
-      if (i >= 0 && i <= f.X + 1 && j >= -1 && j <= f.Y + 1) vly += vy.get(f.idx(i, j)) * dxw * dym[j - imy + 1];
+      if (i >= 0 && i <= f.X + 1 && j >= -1 && j <= f.Y + 1) vly += vy_final(g, vy, i, j) * dxw * dym[j - imy + 1];
     }
   }
   b.vbx[n] = vlx;
@@ -489,10 +528,18 @@ __device__ __forceinline__ void move_one(const GridParams& g, const BubbleParams
   }
 }
 
+// Blocks [0, move_blocks) move the bubbles; the blocks after them write the
+// velocity ghost cells (vghost_cells), which the bubbles' stencils read in
+// closed form (vx_final, vy_final), so one launch does both.
 template <typename V>
 __global__ void __launch_bounds__(kMoveThreads) bubble_move(const __grid_constant__ GridParams g,
                                                             const __grid_constant__ BubbleParams bp, BubbleArrays b,
-                                                            const V vx, const V vy, int* __restrict__ moved) {
+                                                            const V vx, const V vy, int* __restrict__ moved,
+                                                            int move_blocks) {
+  if ((int)blockIdx.x >= move_blocks) {
+    vghost_cells(g, vx, vy, ((int)blockIdx.x - move_blocks) * kMoveThreads + (int)threadIdx.x);
+    return;
+  }
   __shared__ int s_box[4];
   if (threadIdx.x < 4) s_box[threadIdx.x] = 0;
   __syncthreads();
@@ -2054,7 +2101,7 @@ struct Sim {
   // ---- Graph path --------------------------------------------------------
   // One mixture step as a CUDA graph whose control flow runs on the device:
   //   ctl_step_begin -> IF(step ok) {
-  //     fdtd_strip, vghost, bubble_move, ctl_enter -> IF(Picard needed) {
+  //     fdtd_strip, bubble_move (with the ghost cells), ctl_enter -> IF(Picard needed) {
   //       ctl_bins -> IF(bins stale) { counting sort } -> solve order ->
   //       WHILE(residual > threshold) { bubble_rp, couple_press, ctl_iter } }
   //     -> ctl_end }
@@ -2370,7 +2417,8 @@ struct Sim {
     dim3 block(32, kStripWarps);
     cudaError_t e = launch(kClassFdtd, [&] { fdtd_strip<P><<<grid, block, 0, stream>>>(gp, fa); });
     if (e != cudaSuccess) return e;
-    const int ng = std::max(gp.f.X, gp.f.Y) + 3;
+    if (hs.nb > 0) return cudaSuccess;  // bubble_move, which follows, writes the ghost cells
+    const int ng = vghost_threads(gp.f);
     const V vxn = view<V>(vx[nv]), vyn = view<V>(vy[nv]);
     return launch(kClassOther, [&] { vghost<V><<<(ng + 255) / 256, 256, 0, stream>>>(gp, vxn, vyn); });
   }
@@ -2503,7 +2551,9 @@ struct Sim {
     using V = typename P::V;
     const V vxc = view<V>(vx[cur_v]), vyc = view<V>(vy[cur_v]);
     return launch(kClassOther, [&] {
-      bubble_move<V><<<(bub.n + kMoveThreads - 1) / kMoveThreads, kMoveThreads, 0, stream>>>(gp, bp, bub, vxc, vyc, d_moved);
+      const int mb = (bub.n + kMoveThreads - 1) / kMoveThreads;
+      const int gb = (vghost_threads(gp.f) + kMoveThreads - 1) / kMoveThreads;
+      bubble_move<V><<<mb + gb, kMoveThreads, 0, stream>>>(gp, bp, bub, vxc, vyc, d_moved, mb);
     });
   }
 
