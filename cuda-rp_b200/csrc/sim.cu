@@ -460,6 +460,10 @@ __device__ __forceinline__ int bin_of(const Frame& f, int bx, int by) {
 constexpr int kBoxOff = 4;
 
 constexpr int kMoveThreads = 256;
+// Resident blocks per SM the register budget is set for: 7 x 148 SMs hold the
+// 1024 blocks of 262,144 bubbles plus the ghost-cell blocks in one wave (at
+// the unbounded 48 registers only 5 fit, and the launch took 1.4 waves).
+constexpr int kMoveMinBlocks = 7;
 
 template <typename V>
 __device__ __forceinline__ void move_one(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
@@ -481,16 +485,24 @@ __device__ __forceinline__ void move_one(const GridParams& g, const BubbleParams
   const double cx0 = delta_cos_x(bp, g, imx - 1, x), cy0 = delta_cos_y(bp, g, imy - 1, y);
   const double dyn[2] = {delta_w(bp, cy0, iny - (imy - 1)), delta_w(bp, cy0, iny + 1 - (imy - 1))};
   const double dym[2] = {delta_w(bp, cy0, 0), delta_w(bp, cy0, 1)};
-  for (int i = imx - 1; i <= imx; i++) {
-    double dxw = delta_w(bp, cx0, i - (imx - 1));
-    for (int j = iny; j <= iny + 1; j++) {
-      if (i >= -1 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) vlx += vx_final(g, vx, i, j) * dxw * dyn[j - iny];
+#pragma unroll
+  for (int qi = 0; qi < 2; qi++) {
+    const int i = imx - 1 + qi;
+    const double dxw = delta_w(bp, cx0, qi);
+#pragma unroll
+    for (int qj = 0; qj < 2; qj++) {
+      const int j = iny + qj;
+      if (i >= -1 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) vlx += vx_final(g, vx, i, j) * dxw * dyn[qj];
     }
   }
-  for (int i = inx; i <= inx + 1; i++) {
-    double dxw = delta_w(bp, cx0, i - (imx - 1));
-    for (int j = imy - 1; j <= imy; j++) {
-      if (i >= 0 && i <= f.X + 1 && j >= -1 && j <= f.Y + 1) vly += vy_final(g, vy, i, j) * dxw * dym[j - imy + 1];
+#pragma unroll
+  for (int qi = 0; qi < 2; qi++) {
+    const int i = inx + qi;
+    const double dxw = delta_w(bp, cx0, i - (imx - 1));
+#pragma unroll
+    for (int qj = 0; qj < 2; qj++) {
+      const int j = imy - 1 + qj;
+      if (i >= 0 && i <= f.X + 1 && j >= -1 && j <= f.Y + 1) vly += vy_final(g, vy, i, j) * dxw * dym[qj];
     }
   }
   b.vbx[n] = vlx;
@@ -532,7 +544,7 @@ __device__ __forceinline__ void move_one(const GridParams& g, const BubbleParams
 // velocity ghost cells (vghost_cells), which the bubbles' stencils read in
 // closed form (vx_final, vy_final), so one launch does both.
 template <typename V>
-__global__ void __launch_bounds__(kMoveThreads) bubble_move(const __grid_constant__ GridParams g,
+__global__ void __launch_bounds__(kMoveThreads, kMoveMinBlocks) bubble_move(const __grid_constant__ GridParams g,
                                                             const __grid_constant__ BubbleParams bp, BubbleArrays b,
                                                             const V vx, const V vy, int* __restrict__ moved,
                                                             int move_blocks) {
