@@ -52,8 +52,7 @@ struct Job {
   double work = 0.0;   // cells x steps, for the order (0 when the file does not parse)
 };
 
-std::string local_time(const char* fmt) {
-  const time_t now = time(nullptr);
+std::string local_time(time_t now, const char* fmt) {
   struct tm t;
   localtime_r(&now, &t);
   char buf[64];
@@ -137,8 +136,9 @@ int main(int argc, char** argv) {
     if (crp_config_parse_file(j.conf.c_str(), &c, nullptr, 0) == CRP_OK)
       j.work = (double)c.grid_x * (double)c.grid_y * (double)std::max(c.sim_n_step_max, 1);
   }
-  const fs::path day = fs::path(results) / local_time("%Y-%m-%d");
-  const fs::path run_dir = day / local_time("%H:%M");
+  const time_t now = time(nullptr);
+  const fs::path day = fs::path(results) / local_time(now, "%Y-%m-%d");
+  const fs::path run_dir = day / local_time(now, "%H:%M");
   if (dry) {
     std::cout << "results: " << run_dir.string() << std::endl;
     for (const Job& j : jobs)
