@@ -18,6 +18,7 @@
 // target, the evident intent.
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <ctime>
 #include <filesystem>
 #include <iostream>
@@ -86,7 +87,7 @@ int main(int argc, char** argv) {
     auto value = [&](const char* opt) -> const char* {
       if (k + 1 >= argc) {
         std::cerr << "the required argument for option '" << opt << "' is missing" << std::endl;
-        exit(1);
+        std::exit(1);
       }
       return argv[++k];
     };
