@@ -1,37 +1,44 @@
 """Benchmark of the CUDA-RP simulation path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload axisym_1024x2048|axisym_256x512] [--chunk S] [--preroll P]
+                    [--workload axisym_1024x2048|axisym_256x512|sweep_64] [--chunk S]
 
-One bench step is S mixture time steps (default 100, one save interval of the
-workload) of the full hot path: fused FDTD/PML update, bubble motion and
-binning, and every Picard iteration of Rayleigh-Plesset + void-fraction
-gather + pressure re-evaluation the step needs.  The run starts at t = 0 (or
-after P untimed mixture steps, --preroll), takes W untimed bench steps and
-times K: with the defaults, mixture steps 300-1300 of the workload, which end
-as the burst's leading edge reaches the bubble cloud.  The "driven" object then
-advances the same run untimed to --driven-start (default: where the burst
-starts to drive the cloud) and times up to D chunks of 10 mixture steps there
-(--driven-chunks, --driven-chunk, bounded by --driven-seconds of wall time),
-recording where the run stops if a step fails (the workloads' drive grows the
-bubbles until the mixture model stops converging).  The state (about 200 MB at
-1024 x 2048) is larger than L2, so no flush is needed between steps.
+One bench step is S mixture time steps of the full hot path: fused FDTD/PML
+update, bubble motion and binning, and every Picard iteration of
+Rayleigh-Plesset + void-fraction gather + pressure re-evaluation the step
+needs.  The run starts at t = 0; W untimed bench steps, then K timed ones.
 
-metric: Mcell-upd/s — interior cells x mixture steps / device time (CUDA events
-on the simulation's stream, max over ranks).  Also reported: bubble-steps/s,
-the roofline of the fused FDTD kernel, a bounded CPU-oracle baseline and the
-error of the GPU state against the FP64 oracle on that sample, an end-to-end
-number through the C ABI with host buffers, clocks sampled during the timed
-region.
+The timed window stays inside the quiet phase of the workload whatever W and K
+are (`window`): S = min(100, QUIET_END // (W + K + 1)), so mixture steps
+[W S, (W + K) S) plus one profiling chunk end before the burst drives the
+bubble cloud (QUIET_END: mixture step 1700 of the 1024 x 2048 workload, 900 of
+256 x 512).  Both BASELINE drives later grow the cloud until the mixture model
+stops converging (the Picard loop at step 2187 of 1024 x 2048, 1219 of
+256 x 512; the FP64 oracle does the same), so a window that reached there would
+time a failing run.  The "driven" object then continues the same run untimed to
+DRIVEN_START and times chunks of 10 mixture steps one by one (bounded by
+--driven-seconds), recording where the run stops if a step fails.  The state
+(about 200 MB at 1024 x 2048) is larger than L2, so no flush is needed between
+steps.
+
+metric: Mcell-upd/s of the plain FP64 path (the reference's precision) -
+interior cells x mixture steps / device time (CUDA events on the simulation's
+stream, max over ranks).  Also reported: bubble-steps/s; the mixed-precision
+path's rate with its relative L2 against the FP64 path and the oracle; the
+roofline of the fused FDTD kernel; a bounded CPU-oracle baseline and the error
+of the GPU state against the FP64 oracle on that sample; an end-to-end number
+through the C ABI with host buffers; clocks sampled during the timed region.
 
 Multi-GPU (--gpus N under torchrun): independent replicas, one per GPU, no
 data-path collective ("replicas only": the simulation does not shard across
 GPUs here); value = all ranks' cell updates / max rank time.
 
 --impl reference: the reference simulator has no CPU implementation (its
-simulation is CUDA-only), so the reference arm times the FP64 host oracle —
-the restatement of the reference's kernels — on all host cores, each bench
-step one mixture step of the same workload.
+simulation is CUDA-only), so the reference arm times the FP64 host oracle -
+the restatement of the reference's kernels - on all host cores, over the same
+window start as this arm: untimed to mixture step W S, then K timed bench steps
+of one mixture step each (a bounded sample of the window).  Its inputs come
+from the oracle's own parser and seeding; it loads no product library.
 """
 from __future__ import annotations
 
@@ -54,7 +61,10 @@ import numpy as np  # noqa: E402
 # largest bubble radius leaves R0 by more than 1 %), measured with the FP64
 # path; the Picard loop of both workloads stops converging about 500 and 300
 # steps later (steps 2187 and 1219).
-DRIVEN_START = {"axisym_1024x2048": 1700, "axisym_256x512": 900}
+DRIVEN_START = {"axisym_1024x2048": 1700, "axisym_256x512": 900, "sweep_64": 500}
+# Timed windows end here (see the module docstring).
+QUIET_END = dict(DRIVEN_START)
+MAX_CHUNK = {"axisym_1024x2048": 100, "axisym_256x512": 100, "sweep_64": 25}
 WORKLOADS = {
     "axisym_1024x2048": os.path.join(PKG, "configs", "axisym_1024x2048.conf"),
     "axisym_256x512": os.path.join(PKG, "configs", "axisym_256x512.conf"),
@@ -67,7 +77,7 @@ DTYPE = {"fp64": "f64", "mixed": "f32 fields + f32 compensation (f64 arithmetic)
                                   "f32 thermal model while |R/R0-1| <= 1e-3, f64 RP"}
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -75,9 +85,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="axisym_1024x2048", choices=list(WORKLOADS) + ["sweep_64"])
     ap.add_argument("--chunk", type=int, default=None,
-                    help="mixture steps per bench step (default 100; 25 for sweep_64, whose strongest drives "
-                         "reach cavitation and stop converging from about step 500)")
-    ap.add_argument("--preroll", type=int, default=0)
+                    help="mixture steps per bench step (default: the largest that keeps the window quiet, "
+                         "at most 100; 25 for sweep_64)")
     ap.add_argument("--driven-start", type=int, default=None)
     ap.add_argument("--driven-chunks", type=int, default=10)
     ap.add_argument("--driven-chunk", type=int, default=10)
@@ -87,18 +96,28 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
-    ap.add_argument("--primary", default="mixed", choices=["fp64", "mixed"])
-    args = ap.parse_args()
-    if args.chunk is None:
-        args.chunk = 25 if args.workload == "sweep_64" else 100
+    ap.add_argument("--primary", default="fp64", choices=["fp64", "mixed"])
+    args = ap.parse_args(argv)
+    args.chunk, args.window = window(args.workload, args.warmup, args.steps, args.chunk)
     return args
+
+
+def window(workload, warmup, steps, chunk=None):
+    """Mixture steps per bench step and the timed window [start, end) of mixture
+    steps: the window and one profiling chunk after it end by QUIET_END for any
+    warm-up and step counts (chunk >= 1 always; an explicit chunk is kept)."""
+    if chunk is None:
+        chunk = max(1, min(MAX_CHUNK[workload], QUIET_END[workload] // (warmup + steps + 1)))
+    start = warmup * chunk
+    return chunk, (start, start + steps * chunk)
 
 
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, period_ms: int = 50):
         self.gpu = gpu_index
+        self.period = period_ms
         self.samples = []
         self.proc = None
 
@@ -109,7 +128,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(self.period)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
@@ -143,7 +162,7 @@ class Clocks:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "period_ms": self.period}
 
 
 def peaks():
@@ -168,10 +187,21 @@ def traffic(workload, precision):
 
 
 def load_workload(name):
+    """Configuration and seeded bubbles of a workload, through the product's parser."""
     import crp
 
     cfg = crp.parse_file(WORKLOADS[name])
     bub = crp.seed_bubbles(cfg) if cfg.ext_bubble_count > 0 else None
+    return cfg, bub
+
+
+def load_workload_oracle(name):
+    """The same inputs built by the oracle's own parser and seeding (bit-equal to
+    load_workload's, tests/test_oracle_workload.py); loads no product library."""
+    import _bind as B
+
+    cfg = B.oracle_parse_file(WORKLOADS[name])
+    bub = B.oracle_seed_bubbles(cfg) if cfg.ext_bubble_count > 0 else None
     return cfg, bub
 
 
@@ -191,40 +221,34 @@ def cpu_baseline(cfg, bub, seconds, threads):
     return rate, n + 1, t3 - t2, o
 
 
-def oracle_error(gpu_sim_factory, oracle, steps):
-    """Relative errors of a fresh GPU run of `steps` steps against the oracle state."""
-    with gpu_sim_factory() as g:
-        g.step(steps)
-        out = {}
-        for k in ("p0", "vx", "vy", "f_g"):
-            a, b = g.field(k), oracle.field(k)
-            nrm = np.linalg.norm(b)
-            out[k] = {"rel_l2": float(np.linalg.norm(a - b) / nrm) if nrm > 0 else float(np.linalg.norm(a)),
-                      "rel_max": float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))}
-        if g.dims.num_bubbles:
-            a, b = g.bubbles("R_t"), oracle.bubbles("R_t")
-            out["R_t"] = {"rel_l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
-                          "rel_max": float(np.abs(a - b).max() / np.abs(b).max())}
-        out["steps"] = steps
-        return out
+def state_error(g, oracle):
+    """Relative L2 and max errors of a simulation's state against the oracle's."""
+    out = {}
+    for k in ("p0", "vx", "vy", "f_g"):
+        a, b = g.field(k), oracle.field(k)
+        out[k] = {"rel_l2": rel_l2(a, b), "rel_max": float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))}
+    if g.dims.num_bubbles:
+        a, b = g.bubbles("R_t"), oracle.bubbles("R_t")
+        out["R_t"] = {"rel_l2": rel_l2(a, b), "rel_max": float(np.abs(a - b).max() / np.abs(b).max())}
+    return out
 
 
-def run_reference(args, rank, world):
-    """Reference arm: the host oracle on all cores, one mixture step per bench step."""
-    if rank != 0:
-        return None
+def reference_sample(args, world):
+    """Reference arm: the host oracle on all cores over the start of this
+    workload's timed window (see the module docstring)."""
     import _bind as B
 
     if args.workload == "sweep_64":
-        import crp
-
-        cfgs, _ = sweep_configs()
+        cfgs, _ = sweep_configs(B.oracle_parse_file)
         cfg = cfgs[0]
-        bub = crp.seed_bubbles(cfg)
+        bub = B.oracle_seed_bubbles(cfg)
     else:
-        cfg, bub = load_workload(args.workload)
+        cfg, bub = load_workload_oracle(args.workload)
     threads = os.cpu_count() or 1
     o = B.OracleSim(cfg, bub, threads=threads)
+    start = args.window[0]
+    pre = max(0, start - args.warmup)
+    o.step(pre) if pre else None
     for _ in range(args.warmup):
         o.step(1)
     t0 = time.perf_counter()
@@ -233,46 +257,62 @@ def run_reference(args, rank, world):
     dt = time.perf_counter() - t0
     cells = cfg.grid_x * cfg.grid_y
     value = cells * args.steps / dt / 1e6
+    t_start = int(o.stats().steps) - args.steps
+    sample = (f"mixture steps {t_start}-{t_start + args.steps} of {args.workload} (untimed from t=0 to step "
+              f"{t_start}), one per bench step, FP64 oracle with OpenMP")
     return {
         "impl": "reference", "metric": "Mcell-upd/s", "value": value, "unit": "Mcell-upd/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bubbles)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bubbles, Philox-4x32-10)",
         "config": {"workload": args.workload, "grid": [cfg.grid_x, cfg.grid_y], "bubbles": o.dims.num_bubbles,
-                   "mixture_steps_per_step": 1, "start": "t=0"},
+                   "mixture_steps_per_step": 1, "window_start": t_start, "precision": "fp64"},
         "bubble_steps_per_s": o.dims.num_bubbles * args.steps / dt,
-        "cpu_baseline": {"value": value, "unit": "Mcell-upd/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.warmup}+{args.steps} mixture steps of {args.workload} from t=0"},
+        "cpu_baseline": {"value": value, "unit": "Mcell-upd/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "Mcell-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 
-def timed_run(cfg, bub, args, preroll, dist, dev):
-    """Pre-roll, warm up, then time args.steps bench steps on the simulation's
-    stream (CUDA events, max over ranks).  Returns (ms, stats0, stats1, sim)."""
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    return reference_sample(args, world)
+
+
+def timed_run(cfg, bub, args, dist, dev):
+    """Warm up, then time args.steps bench steps on the simulation's stream
+    (CUDA events, max over ranks).  Returns a dict: ms, stats before/after,
+    the simulation and the clocks; or {"error": ...} naming the failing step."""
     import torch
 
     import crp
 
     sim = crp.Sim(cfg, bub)
     stream = torch.cuda.ExternalStream(sim.stream)
-    sim.step(preroll)
-    for _ in range(args.warmup):
-        sim.step(args.chunk)
-    s0 = sim.stats()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(dev) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
+    phase = "warm-up"
+    try:
+        for _ in range(args.warmup):
             sim.step(args.chunk)
-        e1.record(stream)
-        e1.synchronize()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    ms = max_over_ranks(ms, dist)
-    return ms, s0, sim.stats(), sim, clk.summary()
+        s0 = sim.stats()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        phase = "timed window"
+        with Clocks(dev) as clk:
+            e0.record(stream)
+            for _ in range(args.steps):
+                sim.step(args.chunk)
+            e1.record(stream)
+            e1.synchronize()
+        torch.cuda.synchronize()
+    except crp.CrpError as e:
+        torch.cuda.synchronize()
+        step = int(sim.stats().steps) + 1
+        sim.close()
+        return {"error": f"{phase}: mixture step {step}: {e}"}
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    return {"ms": ms, "s0": s0, "s1": sim.stats(), "sim": sim, "clocks": clk.summary(),
+            "p0": sim.field("p0"), "R_t": sim.bubbles("R_t")}
 
 
 def driven_sample(sim, args, cells, nb):
@@ -284,9 +324,14 @@ def driven_sample(sim, args, cells, nb):
 
     stream = torch.cuda.ExternalStream(sim.stream)
     start = DRIVEN_START[args.workload] if args.driven_start is None else args.driven_start
-    if sim.stats().steps < start:
-        sim.step(start - sim.stats().steps)
-    out = {"start_step": int(sim.stats().steps), "chunks": [], "stopped": None}
+    out = {"chunks": [], "stopped": None}
+    try:
+        if sim.stats().steps < start:
+            sim.step(start - sim.stats().steps)
+    except crp.CrpError as e:
+        out["stopped"] = f"before the sample, step {sim.stats().steps + 1}: {e}"
+        return out
+    out["start_step"] = int(sim.stats().steps)
     t_wall = time.perf_counter()
     ms_tot, steps_tot = 0.0, 0
     for _ in range(args.driven_chunks):
@@ -343,7 +388,7 @@ def focal_mask(sim, cfg, radius=2e-3):
     return np.hypot((ii - 0.5) * d.dx, (jj - 0.5) * d.dy - fy) <= radius
 
 
-def adjoint_cost(cfg, args):
+def adjoint_cost(cfg):
     """Cost of crp_adjoint against the forward it differentiates, on the same
     grid without bubbles (the adjoint's scope), FP64, 64 source elements: the
     device time of focal_compare_step(cfg) forward steps from t = 0, then of
@@ -396,33 +441,82 @@ def focal_compare_step(cfg):
     return int(np.ceil(cfg.tr_focal_dist / cfg.ext_c_inf / dt)) + 100
 
 
-def compare_at(primary_sim, other_sim, cfg, primary):
-    """Advance both paths' simulations (untimed) to focal_compare_step and
-    compare p0 over the grid and within 2 mm of the focus, and the bubble radii."""
+def compare_at(sims, cfg):
+    """Advance the FP64 and mixed simulations (untimed) to focal_compare_step and
+    compare the mixed p0 with the FP64 p0 over the grid and within 2 mm of the
+    focus, and the bubble radii."""
     import crp
 
-    step = max(int(primary_sim.stats().steps), focal_compare_step(cfg))
-    for name, sim in (("primary", primary_sim), ("other", other_sim)):
+    step = max(max(int(s.stats().steps) for s in sims.values()), focal_compare_step(cfg))
+    for prec, sim in sims.items():
         try:
             if sim.stats().steps < step:
                 sim.step(step - int(sim.stats().steps))
         except crp.CrpError as e:
-            path = primary if name == "primary" else ("fp64" if primary == "mixed" else "mixed")
-            return {"at_step": step, "error": f"{path} path: {e}"}
-    a, b = primary_sim.field("p0"), other_sim.field("p0")
-    if primary != "mixed":
-        a, b = b, a
-    ra, rb = primary_sim.bubbles("R_t"), other_sim.bubbles("R_t")
-    if primary != "mixed":
-        ra, rb = rb, ra
-    m = focal_mask(primary_sim, cfg)
+            return {"at_step": step, "error": f"{prec} path: {e}"}
+    a, b = sims["mixed"].field("p0"), sims["fp64"].field("p0")
+    m = focal_mask(sims["fp64"], cfg)
     return {"at_step": step, "p0_rel_l2": rel_l2(a, b), "p0_focal_rel_l2": rel_l2(a[m], b[m]),
-            "p0_focal_max_pa": float(np.max(np.abs(b[m]))), "R_t_rel_l2": rel_l2(ra, rb)}
+            "p0_focal_max_pa": float(np.max(np.abs(b[m]))),
+            "R_t_rel_l2": rel_l2(sims["mixed"].bubbles("R_t"), sims["fp64"].bubbles("R_t"))}
 
 
 def rel_l2(a, b):
     n = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / n) if n > 0 else float(np.linalg.norm(a))
+
+
+def e2e_run(cfg, bub, args, nb):
+    """End to end through the C ABI: crp_create from pinned host inputs (config
+    and seeded bubbles), then the warm-up and timed bench steps from t = 0 with
+    p0 and R_t read back into pinned host buffers after every bench step; wall
+    clock over all of it (the teardown is not included)."""
+    import torch
+
+    import crp
+
+    def pinned(a):
+        t = torch.empty(a.shape if hasattr(a, "shape") else a, dtype=torch.float64, pin_memory=True).numpy()
+        if hasattr(a, "shape"):
+            t[...] = a
+        return t
+
+    bub_pinned = crp.Bubbles(*(pinned(a) for a in (bub.x, bub.y, bub.r0, bub.n_b))) if bub is not None else None
+    p0_host = pinned((cfg.grid_y + 2, cfg.grid_x + 2))
+    r_host = pinned((nb,)) if nb > 0 else None
+    n_steps = args.warmup + args.steps
+    t_steps = t_read = 0.0
+    t0 = time.perf_counter()
+    with crp.Sim(cfg, bub_pinned) as s2:
+        t_create = time.perf_counter() - t0
+        d = s2.dims
+        for _ in range(n_steps):
+            ta = time.perf_counter()
+            s2.step(args.chunk)
+            tb = time.perf_counter()
+            s2.field("p0", out=p0_host)
+            if r_host is not None:
+                s2.bubbles("R_t", out=r_host)
+            t_steps += tb - ta
+            t_read += time.perf_counter() - tb
+        wall = time.perf_counter() - t0
+    h2d = 4 * 8 * nb
+    return {"value": cfg.grid_x * cfg.grid_y * n_steps * args.chunk / wall / 1e6, "unit": "Mcell-upd/s",
+            "h2d_bytes_per_step": h2d // n_steps, "d2h_bytes_per_step": 8 * (d.i1m * d.j1m + nb),
+            "seconds": {"create": t_create, "steps": t_steps, "read_back": t_read, "total": wall},
+            "mixture_steps": [0, n_steps * args.chunk],
+            "note": "wall clock: crp_create (seeded bubbles uploaded from pinned host memory) + the warm-up and "
+                    "timed bench steps from t=0 (the window's own steps and the ones before it) + p0 and R_t read "
+                    "back into pinned host buffers after every bench step; the teardown is not included"}
+
+
+def guarded(fn, *a, **k):
+    """fn's result, or {"error": ...} if it raised: one failing leg of the bench
+    does not cost the others their numbers."""
+    try:
+        return fn(*a, **k)
+    except Exception as e:  # noqa: BLE001 - reported in the JSON line
+        return {"error": f"{type(e).__name__}: {e}"}
 
 
 def run_ours(args, rank, world, dist):
@@ -434,153 +528,139 @@ def run_ours(args, rank, world, dist):
     torch.cuda.set_device(dev)
     cfg, bub = load_workload(args.workload)
     cells = cfg.grid_x * cfg.grid_y
-    preroll = args.preroll
     S = args.chunk
     mix_steps = args.steps * S
+    base = {
+        "metric": "Mcell-upd/s", "unit": "Mcell-upd/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "data": "synthetic (seeded bubbles, Philox-4x32-10)",
+        "config": {"workload": args.workload, "grid": [cfg.grid_x, cfg.grid_y],
+                   "mixture_steps_per_step": S, "window": list(args.window), "precision": args.primary,
+                   "parallelism": f"replicas x{world}", "l2": "state > L2 (no flush needed)"},
+    }
 
     # Both forms of the workload: the plain FP64 path and the mixed form.
     runs = {}
-    for prec in (["mixed", "fp64"] if args.precision == "both" else [args.precision]):
+    for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]):
         cfg.ext_precision = 1 if prec == "mixed" else 0
-        ms, s0, s1, sim, clocks = timed_run(cfg, bub, args, preroll, dist, dev)
-        runs[prec] = {"ms": ms, "s0": s0, "s1": s1, "clocks": clocks,
-                      "p0": sim.field("p0"), "R_t": sim.bubbles("R_t"), "sim": sim}
-    # The other path's simulation stays open when a driven sample follows: the
-    # two are compared again once the burst has reached the focus.
-    with_driven = rank == 0 and args.driven_chunks > 0 and world == 1
-    for prec, r in runs.items():
-        if prec != args.primary and len(runs) > 1 and not with_driven:
-            r["sim"].close()
-            r["sim"] = None
+        runs[prec] = timed_run(cfg, bub, args, dist, dev)
     primary = args.primary if args.primary in runs else next(iter(runs))
     run = runs[primary]
-    sim = run["sim"]
     cfg.ext_precision = 1 if primary == "mixed" else 0
+    if "error" in run:
+        for r in runs.values():
+            if r.get("sim") is not None:
+                r["sim"].close()
+        return dict(base, value=None, error=f"{primary} path: {run['error']}", dtype=DTYPE[primary])
+    sim = run["sim"]
     nb = sim.dims.num_bubbles
     ms, s0, s1 = run["ms"], run["s0"], run["s1"]
     value = job_rate(cells * mix_steps, world, ms) / 1e6
-    launches = s1.kernel_launches - s0.kernel_launches
-    picard = s1.picard_total - s0.picard_total
+    # The other path's simulation stays open when a driven sample follows: the
+    # two are compared again once the burst has reached the focus.
+    with_driven = rank == 0 and args.driven_chunks > 0 and world == 1
 
-    # Roofline of the fused FDTD kernel: device time per launch from profiling events.
+    # Roofline of the fused FDTD kernel: device time per launch from profiling
+    # events over one more chunk (still before QUIET_END).
     sim.set_profiling(True)
     p0s = sim.stats()
-    sim.step(S)
+    prof_err = guarded(sim.step, S)
     p1s = sim.stats()
     sim.set_profiling(False)
     n_fdtd = p1s.fdtd_launches - p0s.fdtd_launches
     fdtd_ms = (p1s.ms_fdtd - p0s.ms_fdtd) / max(n_fdtd, 1)
     prof = {k: (getattr(p1s, k) - getattr(p0s, k)) for k in ("ms_fdtd", "ms_rp", "ms_couple", "ms_other")}
-    # End to end through the C ABI: host inputs in, host rawdata arrays out.
-    # Measured before the driven sample, so that no collapse phase precedes it.
-    e2e = None
-    if rank == 0 and not args.no_e2e:
-        # Pinned host memory for the inputs and the read-backs, prepared before
-        # the timed region.
-        def pinned(a):
-            t = torch.empty(a.shape if hasattr(a, "shape") else a, dtype=torch.float64, pin_memory=True).numpy()
-            if hasattr(a, "shape"):
-                t[...] = a
-            return t
 
-        bub_pinned = crp.Bubbles(*(pinned(a) for a in (bub.x, bub.y, bub.r0, bub.n_b))) if bub is not None else None
-        p0_host = pinned((cfg.grid_y + 2, cfg.grid_x + 2))
-        r_host = pinned((nb,)) if nb > 0 else None
-        t0 = time.perf_counter()
-        e2e_steps = 0
-        t_steps = t_read = 0.0
-        with crp.Sim(cfg, bub_pinned) as s2:
-            t_create = time.perf_counter() - t0
-            d = s2.dims
-            h2d = 4 * 8 * nb
-            for _ in range(args.steps):
-                ta = time.perf_counter()
-                s2.step(S)
-                tb = time.perf_counter()
-                e2e_steps += S
-                s2.field("p0", out=p0_host)
-                if r_host is not None:
-                    s2.bubbles("R_t", out=r_host)
-                t_steps += tb - ta
-                t_read += time.perf_counter() - tb
-            wall = time.perf_counter() - t0  # teardown (freeing the device memory) is not part of it
-        e2e = {"value": cells * e2e_steps / wall / 1e6, "unit": "Mcell-upd/s",
-               "h2d_bytes_per_step": h2d // max(args.steps, 1),
-               "d2h_bytes_per_step": 8 * (d.i1m * d.j1m + nb),
-               "seconds": {"create": t_create, "steps": t_steps, "read_back": t_read, "total": wall},
-               "note": "wall clock: crp_create (seeded bubbles uploaded from pinned host memory) + steps from "
-                       "t=0 + p0 and R_t read back into pinned host buffers every bench step; the simulation's "
-                       "teardown is not included"}
-
-    adjoint = adjoint_cost(cfg, args) if rank == 0 and world == 1 and not args.no_adjoint else None
-    driven = driven_sample(sim, args, cells, nb) if with_driven else None
+    e2e = guarded(e2e_run, cfg, bub, args, nb) if rank == 0 and not args.no_e2e else None
+    adjoint = guarded(adjoint_cost, cfg) if rank == 0 and world == 1 and not args.no_adjoint else None
+    driven = guarded(driven_sample, sim, args, cells, nb) if with_driven else None
     focal = None
-    if driven is not None and len(runs) > 1:
-        other = next(r for prec, r in runs.items() if prec != primary)
-        focal = compare_at(sim, other["sim"], cfg, primary)
+    if with_driven and all("sim" in r for r in runs.values()) and len(runs) > 1:
+        focal = guarded(compare_at, {p: r["sim"] for p, r in runs.items()}, cfg)
     hbm, kind = peaks()
     bpc = BYTES_PER_CELL[primary]
-    achieved = bpc * cells / (fdtd_ms * 1e-3) / 1e9
+    achieved = bpc * cells / (fdtd_ms * 1e-3) / 1e9 if n_fdtd else None
     result = None
     if rank == 0:
-        result = {
-            "metric": "Mcell-upd/s", "value": value, "unit": "Mcell-upd/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": DTYPE[primary], "data": "synthetic (seeded bubbles, Philox-4x32-10)",
-            "config": {"workload": args.workload, "grid": [cfg.grid_x, cfg.grid_y], "bubbles": nb,
-                       "mixture_steps_per_step": S, "preroll_steps": preroll, "precision": primary,
-                       "parallelism": f"replicas x{world}", "l2": "state > L2 (no flush needed)"},
+        result = dict(base)
+        result.update({
+            "value": value, "ms_per_step": ms / args.steps, "dtype": DTYPE[primary],
             "bubble_steps_per_s": nb * mix_steps * world / (ms * 1e-3),
-            "picard_iterations_per_step": picard / mix_steps,
-            "gpu_launches": int(launches),
+            "picard_iterations_per_step": (s1.picard_total - s0.picard_total) / mix_steps,
+            "gpu_launches": int(s1.kernel_launches - s0.kernel_launches),
             "roofline": {"kernel": "fdtd_strip", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "peak_kind": kind, "traffic": traffic(args.workload, primary),
-                         "bytes_per_cell": bpc,
-                         "ms_per_launch": fdtd_ms},
+                         "frac": achieved / hbm if achieved else None, "peak_kind": kind,
+                         "traffic": traffic(args.workload, primary), "bytes_per_cell": bpc,
+                         "ms_per_launch": fdtd_ms if n_fdtd else None,
+                         "launches": int(n_fdtd)},
             "kernel_ms_per_chunk": prof,
             "clocks": run["clocks"],
-        }
-        if driven is not None:
-            result["driven"] = driven
-        if e2e is not None:
-            result["e2e"] = e2e
-        if adjoint is not None:
-            result["adjoint"] = adjoint
+        })
+        result["config"]["bubbles"] = nb
+        if prof_err:
+            result["roofline"]["error"] = prof_err["error"]
+        for key, obj in (("driven", driven), ("e2e", e2e), ("adjoint", adjoint)):
+            if obj is not None:
+                result[key] = obj
         for prec, r in runs.items():
+            if "error" in r:
+                result[f"{prec}_path"] = {"error": r["error"]}
+                continue
             result[f"{prec}_path"] = {"value": cells * mix_steps * world / (r["ms"] * 1e-3) / 1e6,
                                       "ms_per_step": r["ms"] / args.steps,
                                       "picard_iterations_per_step": (r["s1"].picard_total - r["s0"].picard_total)
                                       / mix_steps,
-                                      "rp_substeps_max": int(r["s1"].rp_substeps_max)}
-        if "fp64" in runs and "mixed" in runs:
+                                      "rp_substeps_max": int(r["s1"].rp_substeps_max), "clocks": r["clocks"]}
+        if "ms" in runs.get("fp64", {}) and "ms" in runs.get("mixed", {}):
             a, b = runs["mixed"], runs["fp64"]
-            result["mixed_vs_fp64"] = {
-                "speedup": b["ms"] / a["ms"],
-                "quiet": {"at_step": int(preroll + (args.warmup + args.steps) * S),
-                          "p0_rel_l2": rel_l2(a["p0"], b["p0"]), "R_t_rel_l2": rel_l2(a["R_t"], b["R_t"])},
-                "driven": focal,
-                "note": "relative L2 of the mixed path against the FP64 GPU path, which matches the FP64 "
-                        "oracle to ~1e-14 (oracle_error, tests/test_parity_gpu.py); the focal figure is over "
-                        "the cells within 2 mm of the focus, once the burst has reached it"}
+            result["mixed_path"].update({
+                "speedup_over_fp64": b["ms"] / a["ms"],
+                "vs_fp64_at_window_end": {"at_step": int(args.window[1]),
+                                          "p0_rel_l2": rel_l2(a["p0"], b["p0"]),
+                                          "R_t_rel_l2": rel_l2(a["R_t"], b["R_t"])},
+                "vs_fp64_at_focus": focal,
+                "note": "relative L2 of the mixed path against the FP64 GPU path (which matches the FP64 oracle, "
+                        "oracle_error); the focal figure is over the cells within 2 mm of the focus once the burst "
+                        "has reached it"})
     for r in runs.values():
-        if r["sim"] is not None:
+        if r.get("sim") is not None:
             r["sim"].close()
 
     if rank == 0 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        cfg64 = crp.parse_file(WORKLOADS[args.workload])
-        rate, n, wall, oracle = cpu_baseline(cfg64, bub, args.cpu_seconds, threads)
-        result["cpu_baseline"] = {"value": rate / 1e6, "unit": "Mcell-upd/s", "cores": threads, "kind": "port",
-                                  "sample": f"{n} mixture steps of {args.workload} from t=0 "
-                                            f"({wall:.1f} s, OpenMP)"}
-        result["oracle_error"] = oracle_error(lambda: crp.Sim(cfg, bub), oracle, n)
+        cpu = guarded(cpu_leg, args, cfg, bub)
+        if "error" in cpu:
+            result["cpu_baseline"] = cpu
+        else:
+            result.update(cpu)
     return result
+
+
+def cpu_leg(args, cfg, bub):
+    """The oracle on all host cores from t = 0 (inputs from its own parser and
+    seeding), then fresh GPU runs of the same steps in both precisions compared
+    with its state."""
+    import crp
+
+    threads = os.cpu_count() or 1
+    ocfg, obub = load_workload_oracle(args.workload)
+    rate, n, wall, oracle = cpu_baseline(ocfg, obub, args.cpu_seconds, threads)
+    errors = {"steps": n}
+    for prec in ("fp64", "mixed"):
+        c = crp.Config.from_buffer_copy(cfg)
+        c.ext_precision = 1 if prec == "mixed" else 0
+        with crp.Sim(c, bub) as g:
+            g.step(n)
+            errors[prec] = state_error(g, oracle)
+    oracle.close()
+    return {"cpu_baseline": {"value": rate / 1e6, "unit": "Mcell-upd/s", "cores": threads, "kind": "port",
+                             "sample": f"{n} mixture steps of {args.workload} from t=0 ({wall:.1f} s, OpenMP)"},
+            "oracle_error": errors}
 
 
 SWEEP_SEED = 0xC0DA0004
 
 
-def sweep_configs(n=64):
+def sweep_configs(parse_file, n=64):
     """The batched-sweep workload: n axisymmetric simulations with grids X in
     [128, 512] (Y = 2X, dx = 0.1 mm), 1k-64k seeded bubbles (log-uniform), R0
     median 2-5 um (sigma_ln 0.3), 0.2-2.5 MPa surface drive at 0.5-2 MHz, the
@@ -589,7 +669,7 @@ def sweep_configs(n=64):
     import crp
 
     rng = np.random.default_rng(SWEEP_SEED)
-    base = crp.parse_file(WORKLOADS["axisym_256x512"])
+    base = parse_file(WORKLOADS["axisym_256x512"])
     cfgs, steps = [], []
     for k in range(n):
         c = crp.Config.from_buffer_copy(base)
@@ -618,7 +698,7 @@ def run_sweep(args, rank, world):
     import crp
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    cfgs, nominal = sweep_configs()
+    cfgs, nominal = sweep_configs(crp.parse_file)
     n = len(cfgs)
     for c in cfgs:
         c.ext_precision = 1 if args.primary == "mixed" else 0
@@ -664,7 +744,7 @@ def run_sweep(args, rank, world):
             "config": {"workload": "sweep_64", "simulations": n,
                        "cells": int(sum(c.grid_x * c.grid_y for c in cfgs)),
                        "bubbles": int(sum(sim.dims.num_bubbles for sim in batch.sims)),
-                       "mixture_steps_per_step": args.chunk, "start": f"t = 0 + {args.warmup * args.chunk} steps",
+                       "mixture_steps_per_step": args.chunk, "window": list(args.window),
                        "nominal_steps": [min(nominal), max(nominal)], "parallelism": "concurrent streams x64",
                        "l2": "state > L2 (no flush needed)"},
             "bubble_steps_per_s": bub_steps / (ms * 1e-3), "gpu_launches": int(launches),
@@ -682,7 +762,7 @@ def main():
         res = run_reference(args, rank, world)
         if res is not None:
             print(json.dumps(res), flush=True)
-        return
+        return 0
     if world > 1:
         import datetime
 
@@ -692,15 +772,18 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
+    rc = 0
     try:
         res = run_sweep(args, rank, world) if args.workload == "sweep_64" else run_ours(args, rank, world, dist)
         if rank == 0 and res is not None:
             print(json.dumps(res), flush=True)
+            rc = 1 if res.get("value") is None else 0
     finally:
         if dist:
             dist.barrier()
             dist.destroy_process_group()
+    return rc
 
 
 if __name__ == "__main__":
-    main()
+    sys.exit(main())

@@ -17,12 +17,16 @@
 // it; make that first call outside any stream capture.  All calls share the
 // one array and leave their contents in it: each call clears what must start
 // at zero, and two calls whose work overlaps on the GPU (different streams,
-// or different host threads on the same device) race on the array.
+// or different host threads on the same device) race on the array.  The cached
+// address belongs to the device's context: after cudaDeviceReset on a device,
+// do not call this entry point on that device again in the same process.
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <mutex>
+#include <string>
 
 #include "crp.h"
 
@@ -34,6 +38,15 @@ __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 void* g_scratch_addr[kMaxDevices] = {};
 std::mutex g_scratch_mutex;
+
+// Message of the calling thread's last failed call (crp_last_error(NULL)).
+thread_local std::string t_last_error;
+
+crp_status failed(crp_status st, const char* what, cudaError_t e = cudaSuccess) {
+  t_last_error = what;
+  if (e != cudaSuccess) t_last_error += std::string(": ") + cudaGetErrorString(e);
+  return st;
+}
 
 struct Geometry {
   int X, Y;
@@ -236,22 +249,33 @@ extern "C" {
 
 size_t crp_void_fraction_noalloc_scratch(int32_t grid_x, int32_t grid_y, int32_t n) {
   if (grid_x < 2 || grid_y < 2 || n < 0) return 0;
-  return scratch_bytes((grid_x + 3) * (grid_y + 3), n, nullptr, nullptr);
+  const long long nbins = ((long long)grid_x + 3) * ((long long)grid_y + 3);
+  if (nbins > (1LL << 30)) return SIZE_MAX;
+  return scratch_bytes((int)nbins, n, nullptr, nullptr);
 }
 
 crp_status crp_void_fraction_noalloc(const crp_config* cfg, int32_t n, const double* x, const double* y,
                                      const double* r, const double* n_b, double* f_g, void* stream) {
-  if (!cfg || !f_g || n < 0 || (n > 0 && (!x || !y || !r || !n_b))) return CRP_ERR_INVALID;
-  if (cfg->grid_x < 2 || cfg->grid_y < 2 || !(cfg->grid_lx > 0) || !(cfg->grid_ly > 0)) return CRP_ERR_INVALID;
-  if (cfg->sim_smooth_delta_band != 2) return CRP_ERR_UNSUPPORTED;
+  if (!cfg || !f_g || n < 0 || (n > 0 && (!x || !y || !r || !n_b)))
+    return failed(CRP_ERR_INVALID, "crp_void_fraction_noalloc: null pointer or negative count");
+  if (cfg->grid_x < 2 || cfg->grid_y < 2 || !(cfg->grid_lx > 0) || !(cfg->grid_ly > 0))
+    return failed(CRP_ERR_INVALID, "crp_void_fraction_noalloc: grid of fewer than 2 x 2 cells or zero length");
+  if (cfg->sim_smooth_delta_band != 2)
+    return failed(CRP_ERR_UNSUPPORTED, "crp_void_fraction_noalloc: smooth_delta_band 2 only");
   const int X = cfg->grid_x, Y = cfg->grid_y;
-  const long long nbins_ll = (long long)(X + 3) * (Y + 3);
-  if (nbins_ll > (1LL << 30)) return CRP_ERR_TOO_LARGE;
+  const long long nbins_ll = ((long long)X + 3) * ((long long)Y + 3);
+  if (nbins_ll > (1LL << 30)) return failed(CRP_ERR_TOO_LARGE, "crp_void_fraction_noalloc: grid too large");
   const int nbins = (int)nbins_ll;
-  if (scratch_bytes(nbins, n, nullptr, nullptr) > kScratchBytes) return CRP_ERR_TOO_LARGE;
+  if (scratch_bytes(nbins, n, nullptr, nullptr) > kScratchBytes)
+    return failed(CRP_ERR_TOO_LARGE, "crp_void_fraction_noalloc: grid and bubbles need more than the fixed scratch");
+  // A launch error left pending by earlier work on this thread is not this
+  // call's: drop it, so that the check after this call's launches reports
+  // only their own errors.  (A sticky error still fails the launches below.)
+  (void)cudaGetLastError();
 
   void* base = nullptr;
-  if (scratch_address(&base) != cudaSuccess) return CRP_ERR_CUDA;
+  cudaError_t e = scratch_address(&base);
+  if (e != cudaSuccess) return failed(CRP_ERR_CUDA, "crp_void_fraction_noalloc: cudaGetSymbolAddress", e);
   Scratch s;
   scratch_bytes(nbins, n, &s, (unsigned char*)base);
 
@@ -280,7 +304,12 @@ crp_status crp_void_fraction_noalloc(const crp_config* cfg, int32_t n, const dou
   na_sort<<<(nbins + 255) / 256, 256, 0, st>>>(s, nbins);
   dim3 blk(32, 8), grd((X + 2 + 31) / 32, (Y + 2 + 7) / 8);
   na_gather<<<grd, blk, 0, st>>>(g, s, f_g);
-  return cudaGetLastError() == cudaSuccess ? CRP_OK : CRP_ERR_CUDA;
+  e = cudaGetLastError();
+  return e == cudaSuccess ? CRP_OK : failed(CRP_ERR_CUDA, "crp_void_fraction_noalloc: kernel launch", e);
 }
 
 }  // extern "C"
+
+namespace crp {
+const char* noalloc_last_error() { return t_last_error.c_str(); }
+}  // namespace crp

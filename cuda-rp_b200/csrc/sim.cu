@@ -1525,6 +1525,7 @@ struct Sim {
   BubbleParams bp{};
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  int device = 0;  // the device current at crp_create
   std::string err;
 
   // Device memory: one allocation carved into aligned pieces.
@@ -1702,6 +1703,7 @@ struct Sim {
     temperature_on = cfg.dbg_T != 0 || cfg.tr_pid != 0;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CRP_ERR_NO_DEVICE, "no CUDA device");
+    CRP_CUDA(cudaGetDevice(&device));
     if (user_stream) {
       stream = (cudaStream_t)user_stream;
     } else {
@@ -2883,6 +2885,35 @@ struct crp_sim {
   crp::Sim s;
 };
 
+namespace crp {
+const char* noalloc_last_error();
+}
+
+namespace {
+// Makes a simulation's device current for the duration of an entry point and
+// restores the caller's device afterwards: the handle may be driven from any
+// host thread, whose current device need not be the one it was created on.
+class DeviceScope {
+ public:
+  explicit DeviceScope(const crp_sim* h) {
+    if (cudaGetDevice(&prev_) != cudaSuccess) prev_ = -1;
+    if (h && prev_ != h->s.device) {
+      ok_ = cudaSetDevice(h->s.device) == cudaSuccess;
+      switched_ = ok_;
+    }
+  }
+  ~DeviceScope() {
+    if (switched_ && prev_ >= 0) cudaSetDevice(prev_);
+  }
+  bool ok() const { return ok_; }
+
+ private:
+  int prev_ = -1;
+  bool ok_ = true;
+  bool switched_ = false;
+};
+}  // namespace
+
 extern "C" {
 
 crp_status crp_create(const crp_config* cfg, const crp_bubbles_in* bubbles, void* stream, crp_sim** out) {
@@ -2902,6 +2933,8 @@ crp_status crp_create(const crp_config* cfg, const crp_bubbles_in* bubbles, void
 
 crp_status crp_step(crp_sim* h, int32_t n) {
   if (!h || n < 0) return CRP_ERR_INVALID;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
   return h->s.step_n(n);
 }
 
@@ -2929,6 +2962,8 @@ crp_status crp_get_stats(const crp_sim* h, crp_stats* st) {
 
 crp_status crp_set_profiling(crp_sim* h, int32_t enable) {
   if (!h) return CRP_ERR_INVALID;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
   if (cudaStreamSynchronize(h->s.stream) != cudaSuccess) return CRP_ERR_CUDA;
   h->s.prof.resolve();
   h->s.prof.on = enable != 0;
@@ -2938,11 +2973,15 @@ crp_status crp_set_profiling(crp_sim* h, int32_t enable) {
 
 crp_status crp_read_field(crp_sim* h, crp_field f, double* host) {
   if (!h || !host) return CRP_ERR_INVALID;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
   return h->s.read_field(f, host);
 }
 
 crp_status crp_read_bubbles(crp_sim* h, crp_bubble_field w, double* host) {
   if (!h || !host) return CRP_ERR_INVALID;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
   return h->s.read_bubbles(w, host);
 }
 
@@ -2962,6 +3001,8 @@ crp_status crp_get_focus_state(const crp_sim* h, crp_focus_state* st) {
 
 crp_status crp_set_focus_state(crp_sim* h, const crp_focus_state* st) {
   if (!h || !st) return CRP_ERR_INVALID;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
   if (h->s.stats.steps != 0) return CRP_ERR_INVALID;
   h->s.focus = *st;
   if (h->s.cfg.tr_pid) {
@@ -2974,11 +3015,15 @@ crp_status crp_set_focus_state(crp_sim* h, const crp_focus_state* st) {
 
 crp_status crp_set_source_elements(crp_sim* h, int32_t n, const double* amp, const double* phase) {
   if (!h) return CRP_ERR_INVALID;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
   return h->s.set_source_elements(n, amp, phase);
 }
 
 crp_status crp_adjoint(crp_sim* h, const crp_objective* obj, double* J, double* grad_amp, double* grad_phase) {
   if (!h) return CRP_ERR_INVALID;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
   return h->s.adjoint(obj, J, grad_amp, grad_phase);
 }
 
@@ -3000,17 +3045,25 @@ crp_status crp_minmax(const crp_sim* h, double* fg_min, double* fg_max, double* 
 
 void* crp_stream(crp_sim* h) { return h ? (void*)h->s.stream : nullptr; }
 
-const char* crp_last_error(const crp_sim* h) { return h ? h->s.err.c_str() : "null handle"; }
+const char* crp_last_error(const crp_sim* h) { return h ? h->s.err.c_str() : crp::noalloc_last_error(); }
 
-void crp_destroy(crp_sim* h) { delete h; }
+void crp_destroy(crp_sim* h) {
+  if (!h) return;
+  DeviceScope dev(h);
+  delete h;
+}
 
 crp_status crp_write_rawdata(crp_sim* h, const char* dir) {
   if (!h || !dir) return CRP_ERR_INVALID;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
   return crp::write_rawdata(h, dir);
 }
 
 crp_status crp_write_sph(crp_sim* h, const char* dir) {
   if (!h || !dir) return CRP_ERR_INVALID;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
   return crp::write_sph(h, dir);
 }
 

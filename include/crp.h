@@ -7,7 +7,9 @@
  * process or throws across this boundary.  A crp_sim owns all of its device
  * memory and its CUDA stream; host buffers passed in are owned by the caller.
  * One crp_sim per host thread at a time (handles are independent of each
- * other; there is no process-global state).
+ * other; there is no process-global state).  A crp_sim lives on the device that
+ * was current at crp_create; its entry points make that device current while
+ * they run and restore the caller's device, so any host thread may drive it.
  *
  * Reference interfaces replaced (paths inside the reference project):
  *   crp_config / crp_config_parse_file  <- Boost program_options keys and
@@ -273,9 +275,12 @@ void* crp_stream(crp_sim* sim);
  * GPU, shared by all calls: calls whose kernels overlap on a GPU race on it and
  * must be ordered (one stream, or events).  crp_void_fraction_noalloc_scratch
  * gives the bytes a call needs; a call that needs more returns
- * CRP_ERR_TOO_LARGE and queues nothing.  The first call on each device looks up
- * the array's device address (cudaGetSymbolAddress, with that device current):
- * make it before any stream capture. */
+ * CRP_ERR_TOO_LARGE and queues nothing (SIZE_MAX from the size query means the
+ * grid alone is too large).  The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress, with that device current): make it
+ * before any stream capture.  The address is cached for the process: after
+ * cudaDeviceReset on a device, do not call this entry point there again.  A
+ * failing call's message is crp_last_error(NULL) on the calling thread. */
 #define CRP_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
 size_t crp_void_fraction_noalloc_scratch(int32_t grid_x, int32_t grid_y, int32_t n);
 crp_status crp_void_fraction_noalloc(const crp_config* cfg, int32_t n, const double* x, const double* y,
@@ -370,6 +375,8 @@ typedef struct crp_objective {
 crp_status crp_set_source_elements(crp_sim* sim, int32_t n, const double* amp, const double* phase);
 crp_status crp_adjoint(crp_sim* sim, const crp_objective* obj, double* J, double* grad_amp, double* grad_phase);
 
+/* Message of the handle's last failed call; with sim == NULL, of the calling
+ * thread's last failed call that takes no handle (crp_void_fraction_noalloc). */
 const char* crp_last_error(const crp_sim* sim);
 const char* crp_status_string(crp_status s);
 void crp_destroy(crp_sim* sim);

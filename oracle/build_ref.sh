@@ -4,17 +4,21 @@
 # oracle/ref_harness.inc.  Test infrastructure only (the checker); nothing in
 # the product links it.  Output goes to oracle/_ref/ only.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
-# Exits 0 without building when the reference tree is absent.
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]
+#   REFERENCE_ROOT defaults to $CRP_REFERENCE, else /root/reference (where the
+#   read-only reference checkout lives on the build machine).  The root used is
+#   written to oracle/_ref/reference_root for the tests that read the
+#   reference's own files.  Exits 0 without building when the tree is absent.
 set -euo pipefail
 here="$(cd "$(dirname "$0")" && pwd)"
-ref="${1:-/root/reference}"
+ref="${1:-${CRP_REFERENCE:-/root/reference}}"
 out="$here/_ref"
 if [[ ! -f "$ref/src/bubble_CUDA.cu" ]]; then
   echo "build_ref: no reference tree at $ref; skipping"
   exit 0
 fi
 mkdir -p "$out/stubs"
+echo "$ref" > "$out/reference_root"
 # Forwarding headers: the reference's quoted includes resolve through these to
 # its inc/ directory, while its <thrust/...> includes keep resolving to CUDA's.
 for h in bubbles.h bubble_CUDA.h bubble_CUDA_kernel.cuh output_styles.h SphDataType.h; do

@@ -39,6 +39,14 @@ void crpo_set_threads(int32_t n);
 int32_t crpo_get_threads(void);
 void crpo_destroy(crpo_sim* sim);
 
+/* Workload inputs built without the product library (oracle/workload.cpp):
+ * the reference's configuration defaults and config-file grammar, and the
+ * seeded [ext] bubble population; same meaning as crp_config_defaults,
+ * crp_config_parse_file and crp_seed_bubbles. */
+crp_status crpo_config_defaults(crp_config* cfg);
+crp_status crpo_config_parse_file(const char* path, crp_config* cfg, char* err, size_t err_len);
+crp_status crpo_seed_bubbles(const crp_config* cfg, double* x, double* y, double* r0, double* n_b);
+
 /* Bubble physics on single inputs, for comparison with the reference's
  * functions (inc/bubble_CUDA_kernel.cuh:227-340).  bp = (R0, PG0, PL0, T0, gam,
  * sig, mu, rho, K0, dt0). */

@@ -49,6 +49,10 @@ def oracle_lib():
             "crpo_solve_pg": (ctypes.c_double, [vp] + [ctypes.c_double] * 7),
             "crpo_host_scalars": (None, [P(crp.Config), vp]),
             "crpo_host_sigma": (ctypes.c_int32, [P(crp.Config), vp, vp, vp, vp, vp, vp]),
+            "crpo_config_defaults": (ctypes.c_int32, [P(crp.Config)]),
+            "crpo_config_parse_file": (ctypes.c_int32, [ctypes.c_char_p, P(crp.Config), ctypes.c_char_p,
+                                                        ctypes.c_size_t]),
+            "crpo_seed_bubbles": (ctypes.c_int32, [P(crp.Config), vp, vp, vp, vp]),
         }
         for n, (r, a) in sig.items():
             f = getattr(lib, n)
@@ -56,6 +60,29 @@ def oracle_lib():
             f.argtypes = a
         _oracle = lib
     return _oracle
+
+
+def oracle_parse_file(path: str) -> crp.Config:
+    """A configuration file parsed by the oracle's own parser on the oracle's
+    defaults (oracle/workload.cpp): no product library involved."""
+    lib = oracle_lib()
+    cfg = crp.Config()
+    lib.crpo_config_defaults(ctypes.byref(cfg))
+    err = ctypes.create_string_buffer(512)
+    st = lib.crpo_config_parse_file(path.encode(), ctypes.byref(cfg), err, 512)
+    if st:
+        raise crp.CrpError(st, err.value.decode())
+    return cfg
+
+
+def oracle_seed_bubbles(cfg: crp.Config) -> crp.Bubbles:
+    """The seeded [ext] bubble population drawn by the oracle's own Philox."""
+    n = cfg.ext_bubble_count
+    arrs = [np.zeros(n) for _ in range(4)]
+    st = oracle_lib().crpo_seed_bubbles(ctypes.byref(cfg), *[_ptr(a) for a in arrs])
+    if st:
+        raise crp.CrpError(st, "crpo_seed_bubbles")
+    return crp.Bubbles(*arrs)
 
 
 class OracleSim:

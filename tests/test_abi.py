@@ -61,20 +61,15 @@ def test_batch_without_device_fails_cleanly():
     assert e.value.status == 10  # CRP_ERR_NO_DEVICE
 
 
-def test_struct_sizes_match_c():
+def test_struct_sizes_match_c(tmp_path):
     """ctypes mirrors have the C layout (offset of the last member + size)."""
-    src = os.path.join(ROOT, "_work_sizes.c")
-    exe = os.path.join(ROOT, "_work_sizes")
+    src = str(tmp_path / "sizes.c")
+    exe = str(tmp_path / "sizes")
     with open(src, "w") as f:
         f.write('#include "crp.h"\n#include <stdio.h>\n#include <stddef.h>\n'
                 'int main(){printf("%zu %zu %zu %zu\\n", sizeof(crp_config), sizeof(crp_stats), '
                 'sizeof(crp_dims), sizeof(crp_bubbles_in));return 0;}\n')
-    try:
-        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
-        sizes = [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
-    finally:
-        for p in (src, exe):
-            if os.path.exists(p):
-                os.remove(p)
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
+    sizes = [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
     assert sizes == [ctypes.sizeof(crp.Config), ctypes.sizeof(crp.Stats), ctypes.sizeof(crp.Dims),
                      ctypes.sizeof(crp.BubblesIn)]

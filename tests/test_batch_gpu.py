@@ -52,3 +52,32 @@ def test_batch_reports_per_simulation_status():
             batch.run([10, 10])
         assert e.value.status == 6  # CRP_ERR_PICARD
         assert batch.sims[1].stats().steps == 10
+
+
+def test_handles_run_from_other_host_threads():
+    """A simulation and a batch created on one host thread and advanced from
+    others (whose current device the library sets from the handle) give the
+    same results as on the creating thread."""
+    import threading
+
+    cfgs = _configs()[:2]
+    with crp.Sim(cfgs[0]) as here:
+        here.step(40)
+        ref = _state(here)
+    errors = []
+    with crp.Sim(cfgs[0]) as sim, crp.Batch(cfgs) as batch:
+        def work():
+            try:
+                sim.step(40)
+                batch.run([40, 40], threads=2)
+            except Exception as e:  # noqa: BLE001 - reported below
+                errors.append(e)
+
+        t = threading.Thread(target=work)
+        t.start()
+        t.join()
+        assert not errors, errors
+        for a, b in zip(_state(sim), ref):
+            assert np.array_equal(a, b)
+        for a, b in zip(_state(batch.sims[0]), ref):
+            assert np.array_equal(a, b)

@@ -7,7 +7,15 @@ import pytest
 import crp
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_SAMPLE = "/root/reference/confs/Sample.txt"
+
+
+def _reference_root():
+    """Root of the reference tree recorded by oracle/build_ref.sh, if it ran here."""
+    p = os.path.join(ROOT, "oracle", "_ref", "reference_root")
+    return open(p).read().strip() if os.path.exists(p) else ""
+
+
+REF_SAMPLE = os.path.join(_reference_root(), "confs", "Sample.txt") if _reference_root() else ""
 
 
 def test_defaults_are_the_reference_defaults():
