@@ -356,6 +356,10 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
   if (lane == 0 && res) atomicMax(a.residual, res);
 }
 
+}  // namespace crp
+#include "fdtd_tma.cuh"
+namespace crp {
+
 // Velocity ghost cells (VelocityBoundaryKernel, inc/bubble_CUDA_kernel.cuh:701-811,
 // the parts outside the faces the update computes).  Each value is written in
 // closed form from computed faces, in the section order of the reference;
@@ -1335,6 +1339,7 @@ struct Scalars {
   int supp[3][4];               // void-fraction supports of the last three steps
   int entered, rebuilt;         // this step ran the Picard loop / rebuilt the bins
   long long launches[4];        // kernels run by completed graph steps, per class
+  int pipe_err;                 // nonzero: an mbarrier wait of the FDTD pass ran out (never cleared)
 };
 
 // Fast2Sum time step (src/bubble_CUDA.cu:208-212), written by the host path.
@@ -1544,6 +1549,11 @@ struct Sim {
   double* scratch = nullptr;  // dense (X+2) x (Y+2) doubles for readback
   double* d_sigma = nullptr;
   double* d_elem = nullptr;  // source elements: amplitude factors, then phase offsets
+  // Tensor maps of every field buffer for fdtd_tma: velocity [vx, vy][buffer],
+  // split pressure [px, py][buffer], void-fraction ring.
+  CUtensorMap tm_v[2][2]{}, tm_p[2][2]{}, tm_fg[3]{};
+  bool fdtd_tma_on = std::getenv("CRP_FDTD_STRIP") == nullptr;
+  int tma_chunk = 64, tma_nchunks = 1, tma_nxb = 1;
   BubbleArrays bub{};
   Bins bins{};
   // Device scalars written by the kernels, read back once per pressure evaluation.
@@ -1719,6 +1729,10 @@ struct Sim {
     pool_bytes = layout(true);
     CRP_CUDA(cudaMalloc(&pool, pool_bytes));
     layout(false);
+    if (fdtd_tma_on) {
+      const crp_status ts = make_tensor_maps();
+      if (ts != CRP_OK) return ts;
+    }
     CRP_CUDA(cudaMemsetAsync(pool, 0, pool_bytes, stream));
     CRP_CUDA(cudaMallocHost(&h_scalars, sizeof(Scalars)));
     std::memset(h_scalars, 0, sizeof(Scalars));
@@ -1789,6 +1803,54 @@ struct Sim {
       CRP_CUDA(cudaMemcpyAsync(fg[fg_c], fg[fg_a], bytes, cudaMemcpyDeviceToDevice, stream));
     }
     CRP_CUDA(cudaStreamSynchronize(stream));
+    return CRP_OK;
+  }
+
+  // Tensor maps (2-D, the whole frame, boxes of kTmaBoxCols x kTmaRows) of
+  // every field buffer, for the TMA-fed FDTD pass.  The encoder is the driver's
+  // cuTensorMapEncodeTiled, reached through the runtime's entry-point query.
+  crp_status make_tensor_maps() {
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    CRP_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (!fn || q != cudaDriverEntryPointSuccess) return fail(CRP_ERR_CUDA, "cuTensorMapEncodeTiled not available");
+    const Encode enc = reinterpret_cast<Encode>(fn);
+    const Frame& f = gp.f;
+    auto make = [&](CUtensorMap* m, void* base, int esz) -> bool {
+      const cuuint64_t dims[2] = {(cuuint64_t)f.pitch, (cuuint64_t)(f.Y + 4)};
+      const cuuint64_t strides[1] = {(cuuint64_t)f.pitch * (cuuint64_t)esz};
+      const cuuint32_t box[2] = {(cuuint32_t)kTmaBoxCols, (cuuint32_t)kTmaRows};
+      const cuuint32_t estr[2] = {1, 1};
+      return enc(m, esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims,
+                 strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    const int fg_esz = mixed ? 4 : 8;
+    bool ok = true;
+    for (int k = 0; k < 2; k++) {
+      ok = ok && make(&tm_v[0][k], vx[k], 8) && make(&tm_v[1][k], vy[k], 8);
+      ok = ok && make(&tm_p[0][k], px[k], 8) && make(&tm_p[1][k], py[k], 8);
+    }
+    for (int k = 0; k < 3; k++) ok = ok && make(&tm_fg[k], fg[k], fg_esz);
+    if (!ok) return fail(CRP_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    // Blocks of kTmaWarps strips by chunks of rows, about two blocks per SM.
+    int dev = 0, sms = 0;
+    CRP_CUDA(cudaGetDevice(&dev));
+    CRP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int strips = (f.X + 29) / 30;
+    tma_nxb = (strips + kTmaWarps - 1) / kTmaWarps;
+    const int target = std::max(1, 2 * sms / tma_nxb);
+    tma_chunk = std::max(2 * kTmaRows, (f.Y + target - 1) / target);
+    tma_nchunks = (f.Y + tma_chunk - 1) / tma_chunk;
+    if (mixed)
+      CRP_CUDA(cudaFuncSetAttribute(fdtd_tma<PrecMixed>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TmaLayout<PrecMixed>::smem_bytes));
+    else
+      CRP_CUDA(cudaFuncSetAttribute(fdtd_tma<PrecFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TmaLayout<PrecFP64>::smem_bytes));
     return CRP_OK;
   }
 
@@ -2008,6 +2070,7 @@ struct Sim {
       prof.resolve();
     }
     crp_status st = CRP_OK;
+    if (h_scalars->pipe_err) return fail(CRP_ERR_CUDA, "an mbarrier wait of the FDTD pass timed out");
     double resimax = __longlong_as_double_host(h_scalars->residual) / gp.P_inf;
     int loop = 0;
     // picard_gate's decision: the first iteration's solve is already queued.
@@ -2339,6 +2402,7 @@ struct Sim {
     for (int q = 0; q < 3; q++) supp[q] = Box{d.supp[q][0], d.supp[q][1], d.supp[q][2], d.supp[q][3]};
     for (int q = 0; q < 4; q++) launches[q] += d.launches[q];
     fill_launch_stats();
+    if (d.pipe_err) return fail(CRP_ERR_CUDA, "an mbarrier wait of the FDTD pass timed out");
     if (d.status) {
       // The failed step ran up to its failure (its buffers rotated); later launches did nothing.
       cur_v = sv, cur_p = sp, fg_a = sa, fg_b = sb, fg_c = sc;
@@ -2426,10 +2490,26 @@ struct Sim {
     fa.tdev = d_scalars->t;
     fa.rho_const = stats.steps == 0 ? 1 : 0;
     fa.residual = d_residual;
-    const int strips = (gp.f.X + kStripCells - 1) / kStripCells;
-    dim3 grid((strips + kStripWarps - 1) / kStripWarps, (gp.f.Y + kStripRows - 1) / kStripRows);
-    dim3 block(32, kStripWarps);
-    cudaError_t e = launch(kClassFdtd, [&] { fdtd_strip<P><<<grid, block, 0, stream>>>(gp, fa); });
+    cudaError_t e;
+    if (fdtd_tma_on) {
+      TmaMaps m;
+      m.m[0] = tm_p[0][cur_p];
+      m.m[1] = tm_p[1][cur_p];
+      m.m[2] = tm_fg[a];
+      m.m[3] = tm_v[0][cur_v];
+      m.m[4] = tm_v[1][cur_v];
+      m.m[5] = tm_fg[b];
+      m.m[6] = tm_fg[c];
+      const dim3 grid(tma_nxb, tma_nchunks), block(32, kTmaWarps + 1);
+      const int smem = TmaLayout<P>::smem_bytes, chunk = tma_chunk;
+      int* perr = &d_scalars->pipe_err;
+      e = launch(kClassFdtd, [&] { fdtd_tma<P><<<grid, block, smem, stream>>>(gp, fa, m, chunk, perr); });
+    } else {
+      const int strips = (gp.f.X + kStripCells - 1) / kStripCells;
+      dim3 grid((strips + kStripWarps - 1) / kStripWarps, (gp.f.Y + kStripRows - 1) / kStripRows);
+      dim3 block(32, kStripWarps);
+      e = launch(kClassFdtd, [&] { fdtd_strip<P><<<grid, block, 0, stream>>>(gp, fa); });
+    }
     if (e != cudaSuccess) return e;
     if (hs.nb > 0) return cudaSuccess;  // bubble_move, which follows, writes the ghost cells
     const int ng = vghost_threads(gp.f);
