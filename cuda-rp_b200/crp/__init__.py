@@ -46,7 +46,7 @@ class Config(ctypes.Structure):
         ("ext_picard_cap", c_int), ("ext_rp_step_cap", c_int), ("ext_bubble_count", c_int),
         ("ext_bubble_seed", ctypes.c_uint64), ("ext_r0_sigma_ln", c_dbl), ("ext_cloud_shape", c_int),
         ("ext_cloud_r", c_dbl), ("ext_cloud_h", c_dbl), ("ext_n_b", c_dbl), ("ext_picard_tol", c_dbl),
-        ("ext_graphs", c_int), ("ext_elements", c_int),
+        ("ext_graphs", c_int), ("ext_elements", c_int), ("ext_rp_scheme", c_int), ("ext_rp_tol", c_dbl),
     ]
 
 

@@ -78,7 +78,7 @@ bool parse_bool(const std::string& v, int32_t* out) {
   return false;
 }
 
-enum Kind { kInt, kDouble, kBool, kU64, kPrecision, kShape };
+enum Kind { kInt, kDouble, kBool, kU64, kPrecision, kShape, kScheme };
 
 struct Key {
   const char* name;
@@ -159,6 +159,8 @@ const Key kKeys[] = {
     K("ext.picard_tol", kDouble, ext_picard_tol),
     K("ext.graphs", kBool, ext_graphs),
     K("ext.elements", kInt, ext_elements),
+    K("ext.rp_scheme", kScheme, ext_rp_scheme),
+    K("ext.rp_tol", kDouble, ext_rp_tol),
 };
 #undef K
 
@@ -187,6 +189,13 @@ bool assign(const Key& k, const std::string& value, crp_config* cfg) {
       if (s == "cylinder" || s == "0") return *p = 0, true;
       if (s == "sphere" || s == "1") return *p = 1, true;
       if (s == "gaussian" || s == "2") return *p = 2, true;
+      return false;
+    }
+    case kScheme: {
+      std::string s = lower(value);
+      int32_t* p = reinterpret_cast<int32_t*>(base);
+      if (s == "ref" || s == "0") return *p = CRP_RP_REF, true;
+      if (s == "rk45" || s == "1") return *p = CRP_RP_RK45, true;
       return false;
     }
   }

@@ -82,7 +82,11 @@ struct BubbleParams {
   double pi, pi4r3;
   double dcx, dcy, dcz;  // delta_coef (src/bubble_CUDA.cu:1469-1471)
   long long step_cap;
+  double rk_rtol;  // relative tolerance of the rk45 scheme
 };
+
+// Default relative tolerance of the rk45 scheme (ext.rp_tol = 0).
+constexpr double kRk45DefaultTol = 1.0e-7;
 
 __host__ __device__ __forceinline__ bool src_pressure(const GridParams& g) { return g.plane_p || g.focused_p; }
 __host__ __device__ __forceinline__ bool src_velocity(const GridParams& g) { return g.plane_v || g.focused_v; }

@@ -1,53 +1,56 @@
-// The fused FDTD pass fed by the tensor memory accelerator (TMA).
+// The fused FDTD pass on tiles staged by the tensor memory accelerator (TMA).
 //
 // Same arithmetic and output as the strip march of fdtd_strip (void-fraction
 // prediction, VelocityKernel with VelocityBoundaryKernel's faces and
 // MixturePressureKernel with its residual, inc/bubble_CUDA_kernel.cuh:622-867),
-// with a different way of getting rows into shared memory.  A block owns
-// kTmaWarps adjacent 30-column strips (120 updated columns) and a chunk of rows;
-// one producer warp streams the seven input arrays of that column range into a
-// ring of kTmaStages stages, each stage kTmaRows rows of all seven arrays,
-// with one 2-D tensor copy (cp.async.bulk.tensor) per array and stage, and
-// signals each stage on an mbarrier with the transaction's byte count.  The
-// consumer warps march their strips up the chunk exactly as fdtd_strip does
-// (row below in registers, neighbours by shuffle) and hand each stage back on
-// a second mbarrier once its rows are read.  Many rows of every array are in
-// flight per block without one load instruction per element and lane, which
-// is what limited the strip march.
+// organised for latency hiding instead of a serial march: one thread per cell.
 //
-// Tensor boxes start at the frame column of logical i = 120 b - 1, so the
-// innermost coordinate is a multiple of 4 elements (16 bytes for both 8- and
-// 4-byte elements) and the box is 124 columns wide (992 or 496 bytes).  Rows
-// and columns outside the frame are filled with zeros by the copy and are
-// never stored.  Every mbarrier wait is bounded: a wait that runs out sets
-// the step's pipeline error word and the block stops; the producer then
-// waits, again bounded, for the copies it issued before it returns.
+// A persistent block of 32 x 16 threads walks a static list of 32 x 16-cell
+// tiles.  For each tile one thread issues seven 2-D tensor copies
+// (cp.async.bulk.tensor) of the tile and a halo (36 x 18 elements: columns
+// i0-2 .. i0+33, rows j0-1 .. j0+16) of the seven input arrays into one of two
+// shared-memory buffers, completing on that buffer's mbarrier; the copies of
+// the next tile are issued before the current one is computed, so one tile's
+// loads are always in flight behind the arithmetic.  The tile is then done in
+// three phases separated by block barriers:
+//   1. p0 = px + py (with the boundary rules of MixtureBoundaryPressureKernel
+//      at the domain's edges) and rho_m = (1 - f_g) rho_inf for the tile and a
+//      one-cell ring, into shared memory;
+//   2. every east face (velocity vx, 33 columns) and north face (vy, 17 rows)
+//      of the tile, each computed once, into shared memory, and stored;
+//   3. the split-pressure update, residual and void-fraction prediction of
+//      every cell.
+// Every thread's work in a phase is independent of the others', so a tile's
+// latency is hidden by the 32 warps of two resident blocks per SM.
+//
+// Tensor boxes start at frame column 32 tx (logical i = 32 tx - 1), a multiple
+// of 4 elements, and are 36 columns wide (288 or 144 bytes): the innermost
+// coordinate and extent of every copy are multiples of 16 bytes.  Rows and
+// columns outside the frame are filled with zeros by the copy and never
+// stored.  Every mbarrier wait is bounded: a wait that runs out sets the
+// step's pipeline error word and the block stops after waiting, again
+// bounded, for the copies it issued.
 #pragma once
 #include <cuda.h>
 
 namespace crp {
 
-constexpr int kTmaWarps = 4;         // consumer warps (30-column strips) per block
-constexpr int kTmaBoxCols = 124;     // columns per tensor box: 30 kTmaWarps + 4
-constexpr int kTmaRows = 4;          // rows per stage
-constexpr int kTmaStages = 4;        // ring depth
-constexpr int kTmaFields = 7;        // pnx, pny, fgA, vx_old, vy_old, fgB, fgC
+constexpr int kTileX = 32;            // cells per tile row (one warp)
+constexpr int kTileY = 16;            // cell rows per tile (one warp each)
+constexpr int kBoxX = kTileX + 4;     // box columns: logical i0-2 .. i0+33
+constexpr int kBoxY = kTileY + 2;     // box rows: logical j0-1 .. j0+16
+constexpr int kHaloX = kTileX + 2;    // p0 / rho columns i0-1 .. i0+32
+constexpr int kTmaFields = 7;         // pnx, pny, fgA, vx_old, vy_old, fgB, fgC
 constexpr unsigned kTmaWaitLimit = 1u << 22;  // polls of one mbarrier wait before it gives up
 
 struct TmaMaps {
   CUtensorMap m[kTmaFields];
 };
 
-__host__ __device__ constexpr int tma_region_bytes(int esz) { return (kTmaBoxCols * kTmaRows * esz + 127) / 128 * 128; }
-
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(unsigned long long* b, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
-  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(b)) : "memory");
 }
 
 __device__ __forceinline__ void mbar_arrive_tx(unsigned long long* b, unsigned bytes) {
@@ -91,221 +94,207 @@ struct ElemBytes<F32> {
   static constexpr int value = 4;
 };
 
-// Shared-memory layout of one stage: the seven arrays' boxes, each padded to
-// 128 bytes, in field order.
+// Shared memory of one block: two buffers of the seven boxes (each padded to
+// 128 bytes), then p0 and rho of the tile and its ring, the east and north
+// faces, and two mbarriers.
 template <typename P>
-struct TmaLayout {
+struct TileLayout {
   // Element bytes of field fld: split pressure (0, 1) and velocity (3, 4) as
   // stored, void fraction (2, 5, 6) 8 or 4.
   __host__ __device__ static constexpr int esz(int fld) {
     return (fld == 2 || fld >= 5) ? ElemBytes<typename P::G>::value
                                   : (fld <= 1 ? ElemBytes<typename P::S>::value : ElemBytes<typename P::V>::value);
   }
+  __host__ __device__ static constexpr int region(int fld) { return (kBoxX * kBoxY * esz(fld) + 127) / 128 * 128; }
   __host__ __device__ static constexpr int offset(int fld) {
     int o = 0;
-    for (int q = 0; q < fld; q++) o += tma_region_bytes(esz(q));
+    for (int q = 0; q < fld; q++) o += region(q);
     return o;
   }
-  static constexpr int stage_bytes = offset(kTmaFields);
-  // Bytes the copies of one stage deliver (the boxes without padding).
+  static constexpr int buf_bytes = offset(kTmaFields);
   __host__ __device__ static constexpr unsigned tx_bytes() {
     unsigned t = 0;
-    for (int q = 0; q < kTmaFields; q++) t += (unsigned)(kTmaBoxCols * kTmaRows * esz(q));
+    for (int q = 0; q < kTmaFields; q++) t += (unsigned)(kBoxX * kBoxY * esz(q));
     return t;
   }
-  static constexpr int bar_bytes = 128;  // 2 kTmaStages mbarriers, padded
-  static constexpr int smem_bytes = bar_bytes + kTmaStages * stage_bytes;
+  static constexpr int p0_off = 2 * buf_bytes;
+  static constexpr int rho_off = p0_off + kBoxY * kHaloX * 8;
+  static constexpr int fx_off = rho_off + kBoxY * kHaloX * 8;
+  static constexpr int fy_off = fx_off + kTileY * (kTileX + 1) * 8;
+  static constexpr int bar_off = fy_off + (kTileY + 1) * kTileX * 8;
+  static constexpr int smem_bytes = bar_off + 16;
 };
 
 template <typename P>
-__global__ void __launch_bounds__(32 * (kTmaWarps + 1), 2)
-    fdtd_tma(const __grid_constant__ GridParams g, const FdtdArgs<P> a, const __grid_constant__ TmaMaps maps,
-             int chunk_rows, int* __restrict__ pipe_err) {
+__global__ void __launch_bounds__(kTileX* kTileY, 2)
+    fdtd_tile(const __grid_constant__ GridParams g, const FdtdArgs<P> a, const __grid_constant__ TmaMaps maps,
+              int ntx, int ntiles, int* __restrict__ pipe_err) {
   using G = typename P::G;
   using S = typename P::S;
   using V = typename P::V;
-  using L = TmaLayout<P>;
-  extern __shared__ __align__(128) unsigned char tma_smem[];
-  unsigned long long* full = reinterpret_cast<unsigned long long*>(tma_smem);
-  unsigned long long* empty = full + kTmaStages;
-  unsigned char* stages = tma_smem + L::bar_bytes;
+  using L = TileLayout<P>;
+  extern __shared__ __align__(128) unsigned char tsm[];
+  double* p0s = reinterpret_cast<double*>(tsm + L::p0_off);   // [kBoxY][kHaloX], rows j0-1.., cols i0-1..
+  double* rhos = reinterpret_cast<double*>(tsm + L::rho_off);
+  double* fx = reinterpret_cast<double*>(tsm + L::fx_off);    // [kTileY][kTileX+1], east faces of i0-1 ..
+  double* fy = reinterpret_cast<double*>(tsm + L::fy_off);    // [kTileY+1][kTileX], north faces of j0-1 ..
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(tsm + L::bar_off);
 
   const Frame& f = g.f;
   const int X = f.X, Y = f.Y;
-  const int warp = threadIdx.y;
-  const int lane = threadIdx.x;
-  const int by = blockIdx.y, cy = (by & 1) ? (int)gridDim.y - 1 - (by >> 1) : (by >> 1);
-  const int j0 = 1 + cy * chunk_rows;
-  const int j1 = min(Y, j0 + chunk_rows - 1);
-  const int nrows = j1 - j0 + 3;  // rows j0-1 .. j1+1
-  const int nst = (nrows + kTmaRows - 1) / kTmaRows;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * kTileX + tx;
+  const double t_prev = a.tdev[0], t_cur = a.tdev[1];
+  const bool src_rows = g.source_row > 0 && src_pressure(g);
 
-  if (warp == 0 && lane == 0) {
-    for (int s = 0; s < kTmaStages; s++) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kTmaWarps);
-    }
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   __syncthreads();
 
-  if (warp == kTmaWarps) {
-    // Producer: one lane issues the copies of every stage of the chunk.
-    if (lane != 0) return;
-    const int x0 = blockIdx.x * (30 * kTmaWarps);  // frame column of logical i = 120 b - 1
-    int issued = 0;
-    bool ok = true;
-    for (int s = 0; s < nst && ok; s++) {
-      const int slot = s % kTmaStages;
-      if (s >= kTmaStages && !mbar_wait(&empty[slot], (unsigned)((s / kTmaStages - 1) & 1))) {
-        atomicOr(pipe_err, 1);
-        ok = false;
-        break;
-      }
-      unsigned char* st = stages + slot * L::stage_bytes;
-      mbar_arrive_tx(&full[slot], L::tx_bytes());
-      const int y = j0 + s * kTmaRows;  // frame row of logical j0 - 1 + s kTmaRows
+  auto issue = [&](int t, int buf) {
+    const int x0 = (t % ntx) * kTileX;         // frame column of logical i0 - 2
+    const int y0 = 1 + (t / ntx) * kTileY;     // frame row of logical j0 - 1
+    unsigned char* dst = tsm + buf * L::buf_bytes;
+    mbar_arrive_tx(&full[buf], L::tx_bytes());
 #pragma unroll
-      for (int q = 0; q < kTmaFields; q++) tma_load_2d(st + L::offset(q), &maps.m[q], x0, y, &full[slot]);
-      issued = s + 1;
-    }
-    // The copies of the last stages are read by the consumers; when they
-    // stopped early, wait (bounded) for every copy still in flight.
-    for (int s = max(0, issued - kTmaStages); s < issued; s++)
-      mbar_wait(&full[s % kTmaStages], (unsigned)((s / kTmaStages) & 1));
-    return;
-  }
+    for (int q = 0; q < kTmaFields; q++) tma_load_2d(dst + L::offset(q), &maps.m[q], x0, y0, &full[buf]);
+  };
 
-  // Consumers.
-  const unsigned full_mask = 0xffffffffu;
-  const int i = (blockIdx.x * kTmaWarps + warp) * 30 + lane;
-  const int col = warp * 30 + lane + 1;  // column of i inside the box
-  const double t_prev = a.tdev[0], t_cur = a.tdev[1];
-  const bool inwin = i <= X + 1;
-  const bool cell = lane >= 1 && lane <= 30 && i <= X;
-  const bool face = lane <= 30 && i <= X;
-  const bool own = inwin && ((lane >= 1 && lane <= 30) || (lane == 0 && i == 0) || (lane == 31 && i == X + 1));
-  const double xm = ((double)i - 0.5) * g.dx;
-  const bool inner_col = i >= 1 && i <= X;
-  const bool src_rows = g.source_row > 0 && src_pressure(g);
-  const unsigned pitch = (unsigned)f.pitch;
-  const unsigned kb = (unsigned)j0 * pitch + (unsigned)(min(i, X + 1) + 1);
-  auto p0_of = [&](int r, double px_, double py_) -> double {
-    if (inner_col && r >= 1 && r <= Y && !(src_rows && r == g.source_row)) return px_ + py_;
-    if (!inwin) return 0.0;
-    return p0_edge(g, a.pnx, a.pny, i, r, t_prev);
-  };
-  auto rho_of = [&](double fa) -> double { return a.rho_const ? g.rho_inf : (1.0 - fa) * g.rho_inf; };
-  auto predict = [&](long k, double fa) -> double {
-    const double v = G::stored(3.0 * fa - 3.0 * a.fgB.get(k) + a.fgC.get(k));
-    a.fgC.put(k, v);
-    return v;
-  };
-  // Element of field fld in chunk row rr (row j0 - 1 + rr).
-  auto at = [&](int rr, int fld) -> const void* {
-    const int slot = (rr / kTmaRows) % kTmaStages;
-    return stages + slot * L::stage_bytes + L::offset(fld) + ((rr % kTmaRows) * kTmaBoxCols + col) * L::esz(fld);
-  };
+  const int first = blockIdx.x;
+  if (tid == 0 && first < ntiles) issue(first, 0);
+  unsigned long long res = 0ull;
+  int k = 0;
   bool ok = true;
-  auto wait_stage = [&](int s) {
-    if (ok && !mbar_wait(&full[s % kTmaStages], (unsigned)((s / kTmaStages) & 1))) {
+  int in_flight = first < ntiles ? 1 : 0;  // tile copies issued and not yet waited for (thread 0's view)
+  for (int t = first; t < ntiles; t += gridDim.x, k++) {
+    const int buf = k & 1;
+    // The other buffer was last read by the previous tile, finished at its
+    // closing barrier: the next tile's copies may go there now.
+    if (tid == 0 && t + (int)gridDim.x < ntiles) {
+      issue(t + gridDim.x, buf ^ 1);
+      in_flight++;
+    }
+    if (!mbar_wait(&full[buf], (unsigned)((k >> 1) & 1))) {
       atomicOr(pipe_err, 1);
       ok = false;
     }
-    ok = __all_sync(full_mask, ok);
-  };
-  auto release_stage = [&](int s) {
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s % kTmaStages]);
-  };
-
-  wait_stage(0);
-  if (!ok) return;
-  double pxc, pyc, fac, p0b, rhob, vyob;
-  {
-    const double pxb = S::staged(at(0, 0)), pyb = S::staged(at(0, 1));
-    const double fab = G::staged(at(0, 2));
-    vyob = V::staged(at(0, 4));
-    pxc = S::staged(at(1, 0));
-    pyc = S::staged(at(1, 1));
-    fac = G::staged(at(1, 2));
-    p0b = p0_of(j0 - 1, pxb, pyb);
-    rhob = rho_of(fab);
-    if (j0 == 1 && own) predict(f.idx(i, 0), fab);
-  }
-  double p0c = p0_of(j0, pxc, pyc), rhoc = rho_of(fac);
-  double vyd = 0.0;
-  if (cell) {
-    double pre_d;
-    vyd = vy_face_value(g, j0 - 1, vyob, p0b, p0c, face_q(g, rhob, rhoc), xm, t_cur, pre_d);
-    if (j0 == 1) {
-      a.vy_new.put(f.idx(i, 0), vyd);
-      if (!g.pml_y0) a.vy_new.put(f.idx(i, -1), pre_d);
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      break;
     }
-  }
+    in_flight--;
+    const unsigned char* box = tsm + buf * L::buf_bytes;
+    // Box element of field fld at logical (i, j).
+    const int i0 = 1 + (t % ntx) * kTileX, j0 = 1 + (t / ntx) * kTileY;
+    auto at = [&](int fld, int i, int j) -> const void* {
+      return box + L::offset(fld) + ((j - j0 + 1) * kBoxX + (i - i0 + 2)) * L::esz(fld);
+    };
 
-  const double vax_e = face ? g.vax[i + 1] : 1.0, vbx_e = face ? g.vbx[i + 1] : 1.0;
-  const double pax_c = cell ? g.pax[i] : 1.0, pbx_c = cell ? g.pbx[i] : 1.0;
-  const double xu_w = cell && g.cyl ? g.xu[i] : 0.0, xu_e = cell && g.cyl ? g.xu[i + 1] : 0.0;
-  const double rxp_c = cell && g.cyl ? g.rxp[i] : 0.0;
-  const bool zero_e = (i == 0 && !g.pml_x0) || (i == X && !g.pml_x1);
+    // Phase 1: p0 and rho over columns i0-1 .. i0+32, rows j0-1 .. j0+16.
+    for (int e = tid; e < kBoxY * kHaloX; e += kTileX * kTileY) {
+      const int r = e / kHaloX, c = e % kHaloX;
+      const int i = i0 - 1 + c, j = j0 - 1 + r;
+      double p0 = 0.0, rho = g.rho_inf;
+      if (i <= X + 1 && j <= Y + 1) {
+        if (i >= 1 && i <= X && j >= 1 && j <= Y && !(src_rows && j == g.source_row))
+          p0 = S::staged(at(0, i, j)) + S::staged(at(1, i, j));
+        else
+          p0 = p0_edge(g, a.pnx, a.pny, i, j, t_prev);
+        if (!a.rho_const) rho = (1.0 - G::staged(at(2, i, j))) * g.rho_inf;
+      }
+      p0s[e] = p0;
+      rhos[e] = rho;
+    }
+    __syncthreads();
 
-  unsigned long long res = 0ull;
-#pragma unroll 1
-  for (int jj = 0; jj < chunk_rows; jj++) {
-    const int j = j0 + jj;
-    if (j > j1) break;
-    const unsigned k = kb + (unsigned)(jj + 1) * pitch;
-    if ((jj + 2) % kTmaRows == 0) {
-      wait_stage((jj + 2) / kTmaRows);
-      if (!ok) return;
+    // Phase 2a: east faces vx(i, j), i in i0-1 .. i0+31, j in j0 .. j0+15.
+    for (int e = tid; e < kTileY * (kTileX + 1); e += kTileX * kTileY) {
+      const int r = e / (kTileX + 1), c = e % (kTileX + 1);
+      const int i = i0 - 1 + c, j = j0 + r;
+      double fe = 0.0;
+      if (i <= X && j <= Y) {
+        const int h = (r + 1) * kHaloX + c;  // cell (i, j) in p0s
+        fe = velocity_face_q(g, V::staged(at(3, i, j)), p0s[h], p0s[h + 1], face_q(g, rhos[h], rhos[h + 1]),
+                             g.vax[i + 1], g.vbx[i + 1]);
+        if ((i == 0 && !g.pml_x0) || (i == X && !g.pml_x1)) fe = 0.0;
+        if (i >= i0 || i == 0) a.vx_new.put(f.idx(i, j), fe);
+      }
+      fx[e] = fe;
     }
-    const double pxn = S::staged(at(jj + 2, 0)), pyn = S::staged(at(jj + 2, 1));
-    const double fan = G::staged(at(jj + 2, 2));
-    const double vxo = V::staged(at(jj + 1, 3)), vyo = V::staged(at(jj + 1, 4));
-    const double fgp = G::stored(3.0 * fac - 3.0 * G::staged(at(jj + 1, 5)) + G::staged(at(jj + 1, 6)));
-    if ((jj + 1) % kTmaRows == kTmaRows - 1) release_stage((jj + 1) / kTmaRows);
-    if (own) a.fgC.put(k, fgp);
-    const double p0n = p0_of(j + 1, pxn, pyn), rhon = rho_of(fan);
-    const double p0r = __shfl_down_sync(full_mask, p0c, 1), rhor = __shfl_down_sync(full_mask, rhoc, 1);
-    double q_e = g.dt_rho, q_n = g.dt_rho, h = 0.0;
-    if (__any_sync(full_mask,
-                   rhoc != g.rho_inf || rhor != g.rho_inf || rhon != g.rho_inf || fgp != 0.0 || fac != 0.0)) {
-      q_e = face_q(g, rhoc, rhor);
-      q_n = face_q(g, rhoc, rhon);
-      h = void_rate_half(g, fgp, fac);
+    // Phase 2b: north faces vy(i, j), j in j0-1 .. j0+15, i in i0 .. i0+31.
+    for (int e = tid; e < (kTileY + 1) * kTileX; e += kTileX * kTileY) {
+      const int r = e / kTileX, c = e % kTileX;
+      const int i = i0 + c, j = j0 - 1 + r;
+      double vn = 0.0;
+      if (i <= X && j <= Y) {
+        const int h = r * kHaloX + c + 1;  // cell (i, j) in p0s
+        double pre;
+        vn = vy_face_value(g, j, V::staged(at(4, i, j)), p0s[h], p0s[h + kHaloX],
+                           face_q(g, rhos[h], rhos[h + kHaloX]), ((double)i - 0.5) * g.dx, t_cur, pre);
+        if (j >= j0) {
+          a.vy_new.put(f.idx(i, j), vn);
+        } else if (j == 0) {
+          a.vy_new.put(f.idx(i, 0), vn);
+          if (!g.pml_y0) a.vy_new.put(f.idx(i, -1), pre);
+        }
+      }
+      fy[e] = vn;
     }
-    double fe = velocity_face_q(g, vxo, p0c, p0r, q_e, vax_e, vbx_e);
-    if (zero_e) fe = 0.0;
-    const double fw = __shfl_up_sync(full_mask, fe, 1);
-    double pre_u;
-    const double vyu = vy_face_value(g, j, vyo, p0c, p0n, q_n, xm, t_cur, pre_u);
-    const double s1x = g.cyl ? (-xu_w * fw + xu_e * fe) * g.rdx * rxp_c : (-fw + fe) * g.rdx;
-    const double s1y = (-vyd + vyu) * g.rdy;
-    const double qx = pressure_component(g, pxc, pax_c, pbx_c, s1x, h);
-    const double qy = pressure_component(g, pyc, g.pay[j], g.pby[j], s1y, h);
-    if (cell) {
-      a.vx_new.put(k, fe);
-      a.vy_new.put(k, vyu);
-      a.px.put(k, qx);
-      a.py.put(k, qy);
+    __syncthreads();
+
+    // Phase 3: the cell (i, j) of this thread.
+    const int i = i0 + tx, j = j0 + ty;
+    if (i <= X && j <= Y) {
+      auto predict_at = [&](int ii, int jj) -> double {
+        const double v = G::stored(3.0 * G::staged(at(2, ii, jj)) - 3.0 * G::staged(at(5, ii, jj)) +
+                                   G::staged(at(6, ii, jj)));
+        a.fgC.put(f.idx(ii, jj), v);
+        return v;
+      };
+      const double fac = G::staged(at(2, i, j));
+      const double fgp = predict_at(i, j);
+      // Ghost columns 0 and X+1 and ghost rows 0 and Y+1 (and the corners)
+      // are predicted by the cells next to them.
+      const bool wl = i == 1, wr = i == X, wb = j == 1, wt = j == Y;
+      if (wl) predict_at(0, j);
+      if (wr) predict_at(X + 1, j);
+      if (wb) predict_at(i, 0);
+      if (wt) predict_at(i, Y + 1);
+      if (wl && wb) predict_at(0, 0);
+      if (wl && wt) predict_at(0, Y + 1);
+      if (wr && wb) predict_at(X + 1, 0);
+      if (wr && wt) predict_at(X + 1, Y + 1);
+      const double hv = void_rate_half(g, fgp, fac);
+      const double fe = fx[ty * (kTileX + 1) + tx + 1], fw = fx[ty * (kTileX + 1) + tx];
+      const double vyu = fy[(ty + 1) * kTileX + tx], vyd = fy[ty * kTileX + tx];
+      const double s1x = g.cyl ? (-g.xu[i] * fw + g.xu[i + 1] * fe) * g.rdx * g.rxp[i] : (-fw + fe) * g.rdx;
+      const double s1y = (-vyd + vyu) * g.rdy;
+      const double qx = pressure_component(g, S::staged(at(0, i, j)), g.pax[i], g.pbx[i], s1x, hv);
+      const double qy = pressure_component(g, S::staged(at(1, i, j)), g.pay[j], g.pby[j], s1y, hv);
+      const long kk = f.idx(i, j);
+      a.px.put(kk, qx);
+      a.py.put(kk, qy);
       double p0new = qx + qy;
-      if (src_rows && j == g.source_row) p0new = source_row_pressure(g, xm, t_cur);
+      if (src_rows && j == g.source_row) p0new = source_row_pressure(g, ((double)i - 0.5) * g.dx, t_cur);
+      const double p0c = p0s[(ty + 1) * kHaloX + tx + 1];
       res = max(res, (unsigned long long)__double_as_longlong(fabs(p0c - p0new)));
-    } else if (lane == 0 && i == 0) {
-      a.vx_new.put(k, fe);
     }
-    vyd = vyu;
-    pxc = pxn;
-    pyc = pyn;
-    fac = fan;
-    p0c = p0n;
-    rhoc = rhon;
+    __syncthreads();
   }
-  if (j1 == Y && own) predict(f.idx(i, Y + 1), fac);
-  for (int o = 16; o > 0; o >>= 1) res = max(res, __shfl_xor_sync(full_mask, res, o));
-  if (lane == 0 && res) atomicMax(a.residual, res);
+  if (!ok && tid == 0) {
+    // Copies issued and not waited for (at most the next tile's): wait,
+    // bounded, so that none lands after the block has exited.
+    for (int q = 0; q < in_flight; q++) {
+      const int kk = k + q;
+      mbar_wait(&full[kk & 1], (unsigned)((kk >> 1) & 1));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) res = max(res, __shfl_xor_sync(0xffffffffu, res, o));
+  if (tx == 0 && res) atomicMax(a.residual, res);
 }
 
 }  // namespace crp

@@ -142,6 +142,15 @@ __device__ __noinline__ double vy_face_special(const GridParams& g, int jf, doub
 // North face jf of a column (VelocityKernel :668-676 with the y sections of
 // VelocityBoundaryKernel): y0 wall or source, [ext] source row, y1 wall.
 // q: dt / mean(rho) of the face (face_q).
+__device__ __forceinline__ double vy_face_value_f(const GridParams& g, int jf, double v_old, double p0a, double p0b,
+                                                  double q, double fa, double fb, double xm, double t_cur,
+                                                  double& pre) {
+  double v = velocity_face_q(g, v_old, p0a, p0b, q, fa, fb);
+  pre = v;
+  if ((jf == 0 && !g.pml_y0) || (g.source_row > 0 && jf == g.source_row)) v = vy_face_special(g, jf, v, xm, t_cur, &pre);
+  if (jf == g.f.Y && !g.pml_y1) v = 0.0;
+  return v;
+}
 __device__ __forceinline__ double vy_face_value(const GridParams& g, int jf, double v_old, double p0a, double p0b,
                                                 double q, double xm, double t_cur, double& pre) {
   double v = velocity_face_q(g, v_old, p0a, p0b, q, g.vay[jf + 1], g.vby[jf + 1]);
@@ -690,8 +699,8 @@ struct RpState {
 // BubbleInterpolationScalarKernel (:361-395) for bubble n, then the set-up of
 // BubbleRadiusKernel from the state stored at the start of the step (:488-504).
 template <typename S>
-__device__ __forceinline__ void rp_begin(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
-                                         const S& px, const S& py, double t_cur, int n, RpState& s) {
+__device__ __forceinline__ double gather_pl(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
+                                           const S& px, const S& py, double t_cur, int n) {
   const Frame& f = g.f;
   const double x = b.x[n], y = b.y[n];
   const int inx = b.ibnx[n], iny = b.ibny[n];
@@ -706,6 +715,13 @@ __device__ __forceinline__ void rp_begin(const GridParams& g, const BubbleParams
       if (i >= 0 && i <= f.X + 1 && j >= 0 && j <= f.Y + 1) PLp += p0_at(g, px, py, i, j, t_cur) * dxw * dyw;
     }
   }
+  return PLp;
+}
+
+template <typename S>
+__device__ __forceinline__ void rp_begin(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
+                                         const S& px, const S& py, double t_cur, int n, RpState& s) {
+  const double PLp = gather_pl(g, bp, b, px, py, t_cur, n);
   b.PL_p[n] = PLp;
   s.r = bubble_r0(bp, b.R0[n]);
   const double dt = g.dt;
@@ -775,6 +791,9 @@ __device__ __forceinline__ void rp_substep_full(const BubbleParams& bp, RpState&
   s.count++;
 }
 
+__device__ __forceinline__ void store_contrib(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
+                                              int n, double Rt);
+
 // Results of BubbleRadiusKernel (:542-550), then the bubble's void-fraction
 // contribution to the four cells of its stencil (VoidFractionReverseLookupKernel,
 // :595-617), stored for the per-cell gather.
@@ -790,12 +809,19 @@ __device__ __forceinline__ void rp_end(const GridParams& g, const BubbleParams& 
   b.re[n] = s.remain;
   b.Q_B[n] = (s.heat + s.vis) / (dt - s.remain + s.re_n);
   b.nsub[n] = (int)min(s.count, (long long)INT32_MAX);
+  store_contrib(g, bp, b, n, s.Rt);
+}
+
+// The bubble's void-fraction contribution to the four cells of its stencil
+// (VoidFractionReverseLookupKernel, :595-617) at radius Rt, stored at its place
+// in the sorted bins for the per-cell gather.
+__device__ __forceinline__ void store_contrib(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
+                                              int n, double Rt) {
   const double x = b.x[n], y = b.y[n];
   const int inx = b.ibnx[n], iny = b.ibny[n];
   const double cx0 = delta_cos_x(bp, g, inx, x), cy0 = delta_cos_y(bp, g, iny, y);
   const double dx0 = delta_w(bp, cx0, 0), dx1 = delta_w(bp, cx0, 1);
   const double dy0 = delta_w(bp, cy0, 0), dy1 = delta_w(bp, cy0, 1);
-  const double Rt = s.Rt;
   const double vol = g.cyl ? bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy / x
                            : bp.pi4r3 * b.n_B[n] * (Rt * Rt * Rt) * g.rdx * g.rdy;
   const int p = b.pos[n];
@@ -865,6 +891,109 @@ __global__ void __launch_bounds__(kRpThreads, rp_min_blocks<P>()) bubble_rp(cons
       } else {
         if (s.remain > 0.0) atomicOr(err, 1);
         rp_end(g, bp, b, n, s);
+        worst = max(worst, s.count);
+        n = -1;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) worst = max(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+  if ((threadIdx.x & 31) == 0 && worst > 0) atomicMax(substep_max, worst);
+}
+
+}  // namespace crp
+#include "rk45.cuh"
+namespace crp {
+
+// Set-up of one bubble's Dormand-Prince integration over the mixture step from
+// the state stored at the start of the step (as rp_begin): the pressure
+// gather, the liquid-pressure polynomial, R, R', PG and the last step size.
+template <typename S>
+__device__ __forceinline__ void rk_begin(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
+                                         const S& px, const S& py, double t_cur, int n, RkState& s) {
+  const double PLp = gather_pl(g, bp, b, px, py, t_cur, n);
+  b.PL_p[n] = PLp;
+  s.r = bubble_r0(bp, b.R0[n]);
+  const double dt = g.dt;
+  s.R = b.R_pn[n];
+  s.V = b.d1_R_n[n];
+  s.PG = b.PG_n[n];
+  s.h = b.dt_n[n];
+  s.t = 0.0;
+  s.tend = dt;
+  s.Q = 0.0;
+  s.count = 0;
+  s.fresh = true;
+  const double PLn = b.PL_n[n], PLm = b.PL_m[n];
+  s.PC0 = PLn + bp.PL0;
+  s.PC1 = 0.5 * (PLp - PLm) / dt;
+  s.PC2 = 0.5 * (PLp + PLm - 2.0 * PLn) / (dt * dt);
+  s.K = 3.0 * (bp.gam - 1.0) * bp.K0 * bp.T0 * s.r.inv_PG0;
+}
+
+// Results of the integration in the arrays the reference scheme fills: the
+// radius at the end of the step (R_t = R_p; R_n likewise, the scheme keeps no
+// older level), R', PG, the step size to start the next mixture step with,
+// no remainder, the mean heat and viscous power, the step attempts; then the
+// void-fraction contributions.
+__device__ __forceinline__ void rk_end(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b, int n,
+                                       const RkState& s) {
+  b.R_t[n] = s.R;
+  b.R_p[n] = s.R;
+  b.R_n[n] = s.R;
+  b.d1_R_p[n] = s.V;
+  b.PG_p[n] = s.PG;
+  b.dt[n] = fmin(s.h, g.dt);
+  b.re[n] = 0.0;
+  b.Q_B[n] = s.Q / g.dt;
+  b.nsub[n] = (int)min(s.count, (long long)INT32_MAX);
+  store_contrib(g, bp, b, n, s.R);
+}
+
+// The radius solve with ext.rp_scheme = rk45: the work queue of bubble_rp,
+// each pass one step attempt of every active lane.
+template <typename P>
+constexpr int rk_min_blocks() {
+  return 3;
+}
+
+template <typename P>
+__global__ void __launch_bounds__(kRpThreads, rk_min_blocks<P>()) bubble_rk45(const __grid_constant__ GridParams g,
+                                                        const __grid_constant__ BubbleParams bp, BubbleArrays b,
+                                                        const typename P::S px, const typename P::S py,
+                                                        const double* __restrict__ tdev,
+                                                        const int* __restrict__ order,
+                                                        int* __restrict__ next, long long* __restrict__ substep_max,
+                                                        int* __restrict__ err) {
+  RkState s;
+  const double t_cur = tdev[1];
+  int n = -1;
+  bool drained = false;
+  long long worst = 0;
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    const unsigned need = __ballot_sync(0xffffffffu, n < 0 && !drained);
+    if (need) {
+      const int leader = __ffs(need) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(next, __popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need & (1u << lane)) {
+        const int q = base + __popc(need & ((1u << lane) - 1u));
+        if (q < b.n) {
+          n = order[q];
+          rk_begin(g, bp, b, px, py, t_cur, n, s);
+        } else {
+          drained = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, n >= 0)) break;
+    if (n >= 0) {
+      if (s.t < s.tend && s.count < bp.step_cap) {
+        if (!rk_attempt<typename P::T>(bp, s, bp.rk_rtol, g.c_inf)) s.count = bp.step_cap;
+      } else {
+        if (s.t < s.tend) atomicOr(err, 1);
+        rk_end(g, bp, b, n, s);
         worst = max(worst, s.count);
         n = -1;
       }
@@ -1552,8 +1681,8 @@ struct Sim {
   // Tensor maps of every field buffer for fdtd_tma: velocity [vx, vy][buffer],
   // split pressure [px, py][buffer], void-fraction ring.
   CUtensorMap tm_v[2][2]{}, tm_p[2][2]{}, tm_fg[3]{};
-  bool fdtd_tma_on = std::getenv("CRP_FDTD_STRIP") == nullptr;
-  int tma_chunk = 64, tma_nchunks = 1, tma_nxb = 1;
+  bool fdtd_tma_on = std::getenv("CRP_FDTD_TILE") != nullptr;
+  int tile_ntx = 1, tile_n = 1, tile_grid = 1;
   BubbleArrays bub{};
   Bins bins{};
   // Device scalars written by the kernels, read back once per pressure evaluation.
@@ -1705,6 +1834,9 @@ struct Sim {
       return fail(CRP_ERR_UNSUPPORTED, "the CUDA path implements simulation.order = 2 and smooth_delta_band = 2");
     if (cfg.ext_precision != CRP_PREC_FP64 && cfg.ext_precision != CRP_PREC_MIXED)
       return fail(CRP_ERR_INVALID, "ext.precision must be fp64 or mixed");
+    if (cfg.ext_rp_scheme != CRP_RP_REF && cfg.ext_rp_scheme != CRP_RP_RK45)
+      return fail(CRP_ERR_INVALID, "ext.rp_scheme must be ref or rk45");
+    if (cfg.ext_rp_tol < 0.0 || !(cfg.ext_rp_tol < 1.0)) return fail(CRP_ERR_INVALID, "ext.rp_tol must be in [0, 1)");
     mixed = cfg.ext_precision == CRP_PREC_MIXED;
     picard_tol = cfg.ext_picard_tol > 0.0 ? cfg.ext_picard_tol : (mixed ? 1.0e-5 : (double)1.0e-7f);
     graphs_on = cfg.ext_graphs != 0;
@@ -1748,10 +1880,13 @@ struct Sim {
       int dev = 0, sms = 0, per_sm = 0;
       CRP_CUDA(cudaGetDevice(&dev));
       CRP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      const bool rk = cfg.ext_rp_scheme == CRP_RP_RK45;
       if (mixed)
-        CRP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bubble_rp<PrecMixed>, kRpThreads, 0));
+        CRP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, rk ? bubble_rk45<PrecMixed> : bubble_rp<PrecMixed>, kRpThreads, 0));
       else
-        CRP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bubble_rp<PrecFP64>, kRpThreads, 0));
+        CRP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, rk ? bubble_rk45<PrecFP64> : bubble_rp<PrecFP64>, kRpThreads, 0));
       rp_grid = std::max(1, std::min(sms * std::max(per_sm, 1), (hs.nb + kRpThreads - 1) / kRpThreads));
       couple_graph_grid = 4 * sms;
     }
@@ -1806,7 +1941,7 @@ struct Sim {
     return CRP_OK;
   }
 
-  // Tensor maps (2-D, the whole frame, boxes of kTmaBoxCols x kTmaRows) of
+  // Tensor maps (2-D, the whole frame, boxes of kBoxX x kBoxY) of
   // every field buffer, for the TMA-fed FDTD pass.  The encoder is the driver's
   // cuTensorMapEncodeTiled, reached through the runtime's entry-point query.
   crp_status make_tensor_maps() {
@@ -1822,7 +1957,7 @@ struct Sim {
     auto make = [&](CUtensorMap* m, void* base, int esz) -> bool {
       const cuuint64_t dims[2] = {(cuuint64_t)f.pitch, (cuuint64_t)(f.Y + 4)};
       const cuuint64_t strides[1] = {(cuuint64_t)f.pitch * (cuuint64_t)esz};
-      const cuuint32_t box[2] = {(cuuint32_t)kTmaBoxCols, (cuuint32_t)kTmaRows};
+      const cuuint32_t box[2] = {(cuuint32_t)kBoxX, (cuuint32_t)kBoxY};
       const cuuint32_t estr[2] = {1, 1};
       return enc(m, esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims,
                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -1836,21 +1971,19 @@ struct Sim {
     }
     for (int k = 0; k < 3; k++) ok = ok && make(&tm_fg[k], fg[k], fg_esz);
     if (!ok) return fail(CRP_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-    // Blocks of kTmaWarps strips by chunks of rows, about two blocks per SM.
+    // Tiles of kTileX x kTileY cells; a persistent grid of two blocks per SM.
     int dev = 0, sms = 0;
     CRP_CUDA(cudaGetDevice(&dev));
     CRP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int strips = (f.X + 29) / 30;
-    tma_nxb = (strips + kTmaWarps - 1) / kTmaWarps;
-    const int target = std::max(1, 2 * sms / tma_nxb);
-    tma_chunk = std::max(2 * kTmaRows, (f.Y + target - 1) / target);
-    tma_nchunks = (f.Y + tma_chunk - 1) / tma_chunk;
+    tile_ntx = (f.X + kTileX - 1) / kTileX;
+    tile_n = tile_ntx * ((f.Y + kTileY - 1) / kTileY);
+    tile_grid = std::max(1, std::min(tile_n, 2 * sms));
     if (mixed)
-      CRP_CUDA(cudaFuncSetAttribute(fdtd_tma<PrecMixed>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    TmaLayout<PrecMixed>::smem_bytes));
+      CRP_CUDA(cudaFuncSetAttribute(fdtd_tile<PrecMixed>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TileLayout<PrecMixed>::smem_bytes));
     else
-      CRP_CUDA(cudaFuncSetAttribute(fdtd_tma<PrecFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    TmaLayout<PrecFP64>::smem_bytes));
+      CRP_CUDA(cudaFuncSetAttribute(fdtd_tile<PrecFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    TileLayout<PrecFP64>::smem_bytes));
     return CRP_OK;
   }
 
@@ -1923,6 +2056,7 @@ struct Sim {
     bp.dcy = d.dcy;
     bp.dcz = d.dcz;
     bp.step_cap = cfg.ext_rp_step_cap;
+    bp.rk_rtol = cfg.ext_rp_tol > 0.0 ? cfg.ext_rp_tol : kRk45DefaultTol;
   }
 
   void set_sigma_pointers() {
@@ -2500,10 +2634,10 @@ struct Sim {
       m.m[4] = tm_v[1][cur_v];
       m.m[5] = tm_fg[b];
       m.m[6] = tm_fg[c];
-      const dim3 grid(tma_nxb, tma_nchunks), block(32, kTmaWarps + 1);
-      const int smem = TmaLayout<P>::smem_bytes, chunk = tma_chunk;
+      const dim3 block(kTileX, kTileY);
+      const int smem = TileLayout<P>::smem_bytes, ntx = tile_ntx, nt = tile_n, grid = tile_grid;
       int* perr = &d_scalars->pipe_err;
-      e = launch(kClassFdtd, [&] { fdtd_tma<P><<<grid, block, smem, stream>>>(gp, fa, m, chunk, perr); });
+      e = launch(kClassFdtd, [&] { fdtd_tile<P><<<grid, block, smem, stream>>>(gp, fa, m, ntx, nt, perr); });
     } else {
       const int strips = (gp.f.X + kStripCells - 1) / kStripCells;
       dim3 grid((strips + kStripWarps - 1) / kStripWarps, (gp.f.Y + kStripRows - 1) / kStripRows);
@@ -2655,6 +2789,11 @@ struct Sim {
   cudaError_t launch_rp() {
     using S = typename P::S;
     const S pxc = view<S>(px[cur_p]), pyc = view<S>(py[cur_p]);
+    if (cfg.ext_rp_scheme == CRP_RP_RK45)
+      return launch(kClassRp, [&] {
+        bubble_rk45<P><<<rp_grid, kRpThreads, 0, stream>>>(gp, bp, bub, pxc, pyc, d_scalars->t, lpt.order, d_next,
+                                                            d_substep_max, d_err);
+      });
     return launch(kClassRp, [&] {
       bubble_rp<P><<<rp_grid, kRpThreads, 0, stream>>>(gp, bp, bub, pxc, pyc, d_scalars->t, lpt.order, d_next,
                                                         d_substep_max, d_err);

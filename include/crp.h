@@ -127,7 +127,23 @@ typedef struct crp_config {
                                 in the axisymmetric geometry), each with an amplitude factor and a
                                 phase offset (crp_set_source_elements; default 1 and 0, which leave
                                 the source unchanged) */
+  int32_t ext_rp_scheme;     /* crp_rp_scheme: integrator of the bubble radius (default: the
+                                reference's three-level variable step) */
+  double ext_rp_tol;         /* CRP_RP_RK45: relative error tolerance per step (0: 1e-7) */
 } crp_config;
+
+/* Integrator of the bubble radius and gas pressure over one mixture step. */
+typedef enum crp_rp_scheme {
+  CRP_RP_REF = 0,   /* the reference's three-level variable-step scheme with its
+                       semi-implicit gas-pressure update (inc/bubble_CUDA_kernel.cuh:227-260,
+                       326-340, 506-539): step limits 1.01 dt, dt0, 1 % radius change,
+                       0.1 R / sqrt|R''| */
+  CRP_RP_RK45 = 1   /* Dormand-Prince 5(4) with embedded error control on (R, R', PG),
+                       the gas pressure from the continuous form of the same thermal
+                       model; each mixture step ends exactly on the step's end.  In the
+                       mixed path the thermal model runs in FP32 except in the stiff
+                       phase (R / R0 < 0.3 or |R'| > 0.1 c_inf), where all of it is FP64 */
+} crp_rp_scheme;
 
 /* Dense host layouts of the readable fields, in the reference's index order:
  * row-major, x fastest, widths and heights from crp_dims. */

@@ -38,7 +38,7 @@
 
 namespace {
 
-enum class T { I32, F64, Bool, U64, Prec, Shape };
+enum class T { I32, F64, Bool, U64, Prec, Shape, Scheme };
 
 struct Slot {
   T type;
@@ -81,6 +81,7 @@ const std::map<std::string, Slot>& registry() {
       S("ext.cloud_r", T::F64, ext_cloud_r), S("ext.cloud_h", T::F64, ext_cloud_h),
       S("ext.n_b", T::F64, ext_n_b), S("ext.picard_tol", T::F64, ext_picard_tol),
       S("ext.graphs", T::Bool, ext_graphs), S("ext.elements", T::I32, ext_elements),
+      S("ext.rp_scheme", T::Scheme, ext_rp_scheme), S("ext.rp_tol", T::F64, ext_rp_tol),
   };
 #undef S
   return m;
@@ -144,6 +145,12 @@ bool store(const Slot& s, const std::string& v, crp_config* cfg) {
     }
     case T::Shape: {
       int k = pick(v, {{"cylinder", "0"}, {"sphere", "1"}, {"gaussian", "2"}});
+      if (k < 0) return false;
+      *reinterpret_cast<int32_t*>(p) = k;
+      return true;
+    }
+    case T::Scheme: {
+      int k = pick(v, {{"ref", "0"}, {"rk45", "1"}});
       if (k < 0) return false;
       *reinterpret_cast<int32_t*>(p) = k;
       return true;
