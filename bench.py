@@ -363,6 +363,27 @@ def driven_sample(sim, args, cells, nb):
     return out
 
 
+def driven_rk45_sample(cfg, bub, args, cells, nb, ref_sim):
+    """The driven sample of the same workload with the radius integrated by the
+    rk45 scheme (ext.rp_scheme = rk45, default tolerance), in the primary
+    precision: a fresh run taken untimed to the sample's start, then the same
+    chunks timed one by one; its radii compared with the reference scheme's run
+    at the same step (the difference is the reference scheme's truncation
+    error, which the rk45 scheme's tolerance bounds far below)."""
+    import crp
+
+    c = crp.Config.from_buffer_copy(cfg)
+    c.ext_rp_scheme = 1
+    with crp.Sim(c, bub) as sim:
+        out = driven_sample(sim, args, cells, nb)
+        out["scheme"] = "rk45"
+        out["rtol"] = c.ext_rp_tol or 1e-6
+        if ref_sim is not None and ref_sim.stats().steps == sim.stats().steps:
+            out["R_t_rel_l2_vs_reference_scheme"] = rel_l2(sim.bubbles("R_t"), ref_sim.bubbles("R_t"))
+            out["p0_rel_l2_vs_reference_scheme"] = rel_l2(sim.field("p0"), ref_sim.field("p0"))
+        return out
+
+
 def max_over_ranks(x, dist):
     """The largest of every rank's x (the job's time is its slowest rank's);
     x itself without a process group.  NCCL reduces a CUDA tensor, gloo a CPU one."""
@@ -574,6 +595,7 @@ def run_ours(args, rank, world, dist):
     e2e = guarded(e2e_run, cfg, bub, args, nb) if rank == 0 and not args.no_e2e else None
     adjoint = guarded(adjoint_cost, cfg) if rank == 0 and world == 1 and not args.no_adjoint else None
     driven = guarded(driven_sample, sim, args, cells, nb) if with_driven else None
+    driven_rk45 = guarded(driven_rk45_sample, cfg, bub, args, cells, nb, sim) if with_driven else None
     focal = None
     if with_driven and all("sim" in r for r in runs.values()) and len(runs) > 1:
         focal = guarded(compare_at, {p: r["sim"] for p, r in runs.items()}, cfg)
@@ -599,7 +621,7 @@ def run_ours(args, rank, world, dist):
         result["config"]["bubbles"] = nb
         if prof_err:
             result["roofline"]["error"] = prof_err["error"]
-        for key, obj in (("driven", driven), ("e2e", e2e), ("adjoint", adjoint)):
+        for key, obj in (("driven", driven), ("driven_rk45", driven_rk45), ("e2e", e2e), ("adjoint", adjoint)):
             if obj is not None:
                 result[key] = obj
         for prec, r in runs.items():

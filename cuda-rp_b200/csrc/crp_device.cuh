@@ -86,7 +86,7 @@ struct BubbleParams {
 };
 
 // Default relative tolerance of the rk45 scheme (ext.rp_tol = 0).
-constexpr double kRk45DefaultTol = 1.0e-7;
+constexpr double kRk45DefaultTol = 1.0e-6;
 
 __host__ __device__ __forceinline__ bool src_pressure(const GridParams& g) { return g.plane_p || g.focused_p; }
 __host__ __device__ __forceinline__ bool src_velocity(const GridParams& g) { return g.plane_v || g.focused_v; }

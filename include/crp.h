@@ -129,7 +129,7 @@ typedef struct crp_config {
                                 the source unchanged) */
   int32_t ext_rp_scheme;     /* crp_rp_scheme: integrator of the bubble radius (default: the
                                 reference's three-level variable step) */
-  double ext_rp_tol;         /* CRP_RP_RK45: relative error tolerance per step (0: 1e-7) */
+  double ext_rp_tol;         /* CRP_RP_RK45: relative error tolerance per step (0: 1e-6) */
 } crp_config;
 
 /* Integrator of the bubble radius and gas pressure over one mixture step. */

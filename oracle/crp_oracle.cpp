@@ -170,6 +170,145 @@ double gas_pressure(double PGn, double Rp, double Rn, double omega, double dt, C
   return (c2 * PGn + c0 * lpr * b.PG0) / c1;
 }
 
+// The reference's sub-step with its step limits scaled down by `refine`
+// (dt0 / refine, 0.01 / refine radius change, 0.1 / refine of R / sqrt|R''|):
+// refine = 1 is rp_substep.  Used only to converge the reference scheme in the
+// single-bubble comparison with the rk45 scheme.
+void rp_substep_refined(double& Rt, double& Rp, double& Rn, double& d1R, double PG, double PL, double& dt,
+                        double& remain, const BubConst& b, double refine) {
+  double Rm = Rn;
+  Rn = Rp;
+  double acc = (PG - PL - 2.0 * b.sig / Rn - 4.0 * b.mu / Rn * d1R) / b.rho - 1.5 * d1R * d1R;
+  double dtm = dt;
+  double dtp = std::min(1.01 * dt, b.dt0 / refine);
+  if (std::fabs(d1R) > kEps) dtp = std::min(dtp, 0.01 / refine * Rn / std::fabs(d1R));
+  if (std::fabs(acc) > kEps) dtp = std::min(dtp, 0.1 / refine * Rn / std::sqrt(std::fabs(acc)));
+  Rt = Rp = (1.0 + dtp / dtm) * Rn - dtp / dtm * Rm + (dtp / Rn) * (0.5 * (dtp + dtm) * acc);
+  d1R = (dtm * dtm * Rp + (-dtm * dtm + dtp * dtp) * Rn - dtp * dtp * Rm) / (dtm * dtp * (dtm + dtp)) +
+        (dtp / Rn) * acc;
+  dt = dtp;
+  if (dtp >= remain) {
+    dtp = remain;
+    Rt = (1.0 + dtp / dtm) * Rn - dtp / dtm * Rm + (dtp / Rn) * (0.5 * (dtp + dtm) * acc);
+  }
+  remain -= dtp;
+}
+
+// ext.rp_scheme = rk45: the same bubble model as a continuous system in
+// (R, R', PG), integrated by the Dormand-Prince 5(4) pair (Dormand & Prince
+// 1980) with embedded error control; the restatement of the CUDA path's
+// scheme (its model and controller are documented in cuda-rp_b200/csrc/rk45.cuh).
+// PG' is the dt -> 0 limit of solvePG (inc/bubble_CUDA_kernel.cuh:326-340),
+// omega and Lp are the reference's thermal model (solveOmegaN, solveLp).
+struct RkD {
+  double R, V, PG, q;
+};
+
+struct RkBubble {
+  const BubConst* k;
+  double K;              // 3 (gam - 1) K0 T0 / PG0
+  double PC0, PC1, PC2;  // liquid pressure PC2 t^2 + PC1 t + PC0, t from the step's start
+  double pi;
+  RkD rhs(double t, double R, double V, double PG) const {
+    const BubConst& b = *k;
+    const double PL = PC2 * t * t + PC1 * t + PC0;
+    RkD d;
+    d.R = V;
+    d.V = ((PG - PL - 2.0 * b.sig / R - 4.0 * b.mu / R * V) / b.rho - 1.5 * V * V) / R;
+    Cplx alpha;
+    const double omega = thermal_omega(alpha, PG, R, b);
+    const Cplx lp = thermal_lp(alpha, R);
+    const double den = lp.re * lp.re + lp.im * lp.im;
+    const double Lr = lp.re / den, Liw = lp.im / den / omega;
+    const double x = R / b.R0;
+    const double x3 = x * x * x;
+    const double KR = K / R;
+    const double num = -3.0 * b.gam * PG * V / R + KR * (Lr * (b.PG0 - x3 * PG) + Liw * 3.0 * x * x * V / b.R0 * PG);
+    d.PG = num / (1.0 - KR * Liw * x3);
+    const double R3 = R * R * R;
+    const double dTdr = b.T0 / (b.PG0 * b.R03) * (Lr * (b.PG0 * b.R03 - PG * R3) + Liw * (R3 * d.PG + 3.0 * R * R * V * PG));
+    d.q = -4.0 * pi * R * R * b.K0 * dTdr + 16.0 * pi * b.mu * R * V * V;
+    return d;
+  }
+};
+
+struct RkRun {
+  double R, V, PG, h, t, tend, Q;
+  int64_t count;
+};
+
+// Integrates over [t, tend]; false when the step cap is reached or the step
+// size collapses.
+bool rk45_run(const RkBubble& m, RkRun& s, double rtol, int64_t cap) {
+  const double c2 = 1.0 / 5.0, c3 = 3.0 / 10.0, c4 = 4.0 / 5.0, c5 = 8.0 / 9.0;
+  const double a21 = 1.0 / 5.0;
+  const double a31 = 3.0 / 40.0, a32 = 9.0 / 40.0;
+  const double a41 = 44.0 / 45.0, a42 = -56.0 / 15.0, a43 = 32.0 / 9.0;
+  const double a51 = 19372.0 / 6561.0, a52 = -25360.0 / 2187.0, a53 = 64448.0 / 6561.0, a54 = -212.0 / 729.0;
+  const double a61 = 9017.0 / 3168.0, a62 = -355.0 / 33.0, a63 = 46732.0 / 5247.0, a64 = 49.0 / 176.0,
+               a65 = -5103.0 / 18656.0;
+  const double b1 = 35.0 / 384.0, b3 = 500.0 / 1113.0, b4 = 125.0 / 192.0, b5 = -2187.0 / 6784.0, b6 = 11.0 / 84.0;
+  const double e1 = 71.0 / 57600.0, e3 = -71.0 / 16695.0, e4 = 71.0 / 1920.0, e5 = -17253.0 / 339200.0,
+               e6 = 22.0 / 525.0, e7 = -1.0 / 40.0;
+  RkD k1 = m.rhs(s.t, s.R, s.V, s.PG);
+  while (s.t < s.tend) {
+    if (s.count >= cap) return false;
+    const double rem = s.tend - s.t;
+    double h = s.h;
+    bool last = false;
+    if (h >= rem || 1.01 * h >= rem) {
+      h = rem;
+      last = true;
+    }
+    s.count++;
+    const double t = s.t;
+    const RkD k2 = m.rhs(t + c2 * h, s.R + h * (a21 * k1.R), s.V + h * (a21 * k1.V), s.PG + h * (a21 * k1.PG));
+    const RkD k3 = m.rhs(t + c3 * h, s.R + h * (a31 * k1.R + a32 * k2.R), s.V + h * (a31 * k1.V + a32 * k2.V),
+                         s.PG + h * (a31 * k1.PG + a32 * k2.PG));
+    const RkD k4 = m.rhs(t + c4 * h, s.R + h * (a41 * k1.R + a42 * k2.R + a43 * k3.R),
+                         s.V + h * (a41 * k1.V + a42 * k2.V + a43 * k3.V),
+                         s.PG + h * (a41 * k1.PG + a42 * k2.PG + a43 * k3.PG));
+    const RkD k5 = m.rhs(t + c5 * h, s.R + h * (a51 * k1.R + a52 * k2.R + a53 * k3.R + a54 * k4.R),
+                         s.V + h * (a51 * k1.V + a52 * k2.V + a53 * k3.V + a54 * k4.V),
+                         s.PG + h * (a51 * k1.PG + a52 * k2.PG + a53 * k3.PG + a54 * k4.PG));
+    const RkD k6 = m.rhs(t + h, s.R + h * (a61 * k1.R + a62 * k2.R + a63 * k3.R + a64 * k4.R + a65 * k5.R),
+                         s.V + h * (a61 * k1.V + a62 * k2.V + a63 * k3.V + a64 * k4.V + a65 * k5.V),
+                         s.PG + h * (a61 * k1.PG + a62 * k2.PG + a63 * k3.PG + a64 * k4.PG + a65 * k5.PG));
+    const double Rn = s.R + h * (b1 * k1.R + b3 * k3.R + b4 * k4.R + b5 * k5.R + b6 * k6.R);
+    const double Vn = s.V + h * (b1 * k1.V + b3 * k3.V + b4 * k4.V + b5 * k5.V + b6 * k6.V);
+    const double PGn = s.PG + h * (b1 * k1.PG + b3 * k3.PG + b4 * k4.PG + b5 * k5.PG + b6 * k6.PG);
+    const bool finite = Rn > 0.0 && PGn > 0.0 && std::isfinite(Rn) && std::isfinite(Vn) && std::isfinite(PGn);
+    RkD k7{0.0, 0.0, 0.0, 0.0};
+    double err = 1.0e30;
+    if (finite) {
+      k7 = m.rhs(t + h, Rn, Vn, PGn);
+      const double eR = h * (e1 * k1.R + e3 * k3.R + e4 * k4.R + e5 * k5.R + e6 * k6.R + e7 * k7.R);
+      const double eV = h * (e1 * k1.V + e3 * k3.V + e4 * k4.V + e5 * k5.V + e6 * k6.V + e7 * k7.V);
+      const double eP = h * (e1 * k1.PG + e3 * k3.PG + e4 * k4.PG + e5 * k5.PG + e6 * k6.PG + e7 * k7.PG);
+      const double sR = rtol * std::max(std::fabs(s.R), std::fabs(Rn));
+      const double sV = rtol * (std::max(std::fabs(s.V), std::fabs(Vn)) + 1.0);
+      const double sP = rtol * std::max(std::fabs(s.PG), std::fabs(PGn));
+      err = std::max(std::fabs(eR) / sR, std::max(std::fabs(eV) / sV, std::fabs(eP) / sP));
+      if (!std::isfinite(err)) err = 1.0e30;
+    }
+    double fac = err > 0.0 ? 0.9 * std::pow(err, -0.2) : 5.0;
+    if (err <= 1.0) {
+      s.Q += h * (b1 * k1.q + b3 * k3.q + b4 * k4.q + b5 * k5.q + b6 * k6.q);
+      s.R = Rn;
+      s.V = Vn;
+      s.PG = PGn;
+      k1 = k7;
+      s.t = last ? s.tend : t + h;
+      fac = std::min(5.0, std::max(0.2, fac));
+      s.h = last ? std::max(s.h, h * fac) : h * fac;
+    } else {
+      s.h = h * std::min(1.0, std::max(0.2, fac));
+    }
+    if (!(s.h > 1.0e-22)) return false;
+  }
+  return true;
+}
+
 // -------------------------------------------------------------------------
 // array_index_t and init_array, inc/bubble_CUDA.h:59-69, src/bubble_CUDA.cu:561-597.
 struct Index {
@@ -843,6 +982,7 @@ struct crpo_sim {
     const int64_t cap = cfg.ext_rp_step_cap;
     int64_t worst = 0;
     bool capped = false;
+    if (cfg.ext_rp_scheme == CRP_RP_RK45) return bubble_radii_rk45();
 #pragma omp parallel for schedule(dynamic, 64) reduction(max : worst) reduction(|| : capped)
     for (int b = 0; b < nb; b++) {
       const BubConst& k = bc[b];
@@ -886,6 +1026,39 @@ struct crpo_sim {
       Q_B[b] = (heat + vis) / (dt - remain + re_n[b]);
       nsub[b] = (int)std::min<int64_t>(count, INT32_MAX);
       worst = std::max(worst, count);
+    }
+    return capped ? -1 : worst;
+  }
+
+  // The radius solve with ext.rp_scheme = rk45 (rk45_run): from the state at
+  // the start of the step (R_pn, d1_R_n, PG_n, last step size dt_n) to the
+  // step's end exactly; results in the arrays the reference scheme fills.
+  int64_t bubble_radii_rk45() {
+    const double dt = d.dt;
+    const int64_t cap = cfg.ext_rp_step_cap;
+    const double rtol = cfg.ext_rp_tol > 0.0 ? cfg.ext_rp_tol : 1.0e-6;
+    int64_t worst = 0;
+    bool capped = false;
+#pragma omp parallel for schedule(dynamic, 64) reduction(max : worst) reduction(|| : capped)
+    for (int b = 0; b < nb; b++) {
+      const BubConst& k = bc[b];
+      RkBubble m;
+      m.k = &k;
+      m.K = 3.0 * (k.gam - 1.0) * k.K0 * k.T0 / k.PG0;
+      m.PC0 = PL_n[b] + k.PL0;
+      m.PC1 = 0.5 * (PL_p[b] - PL_m[b]) / dt;
+      m.PC2 = 0.5 * (PL_p[b] + PL_m[b] - 2.0 * PL_n[b]) / (dt * dt);
+      m.pi = d.pi;
+      RkRun s{R_pn[b], d1_R_n[b], PG_n[b], dt_n[b], 0.0, dt, 0.0, 0};
+      if (!rk45_run(m, s, rtol, cap)) capped = true;
+      R_t[b] = R_p[b] = R_n[b] = s.R;
+      d1_R_p[b] = s.V;
+      PG_p[b] = s.PG;
+      dtb[b] = std::min(s.h, dt);
+      re[b] = 0.0;
+      Q_B[b] = s.Q / dt;
+      nsub[b] = (int)std::min<int64_t>(s.count, INT32_MAX);
+      worst = std::max(worst, s.count);
     }
     return capped ? -1 : worst;
   }
@@ -1274,6 +1447,54 @@ int64_t crpo_bubble_history(const double* bp, double R_init, double dt_mix, doub
       if (total > 100000000) return -1;
     }
     re = remain;
+    R_out[s] = Rt;
+    PG_out[s] = PGp;
+  }
+  return total;
+}
+
+int64_t crpo_bubble_drive(const double* bp, double R_init, double dt_mix, double p_amp, double omega_drive,
+                          int32_t nsteps, int32_t scheme, double param, double* R_out, double* PG_out) {
+  // One bubble from rest at R_init under a liquid pressure PL0 + p_amp sin(w t),
+  // entering each mixture step as the quadratic through its values at the
+  // step's start, end and the start of the previous step (the simulation's
+  // PL_m, PL_n, PL_p).  scheme 0: the reference scheme with its limits scaled
+  // down by param (rp_substep_refined, param >= 1); scheme 1: rk45 at rtol = param.
+  BubConst b = bub_from(bp);
+  const double pi = std::acos(-1.0);
+  double Rt = R_init, Rp = R_init, Rn = R_init, d1R = 0.0, PGp = b.PG0 * std::pow(b.R0 / R_init, 3.0 * b.gam),
+         dtL = b.dt0, re = 0.0;
+  int64_t total = 0;
+  auto pl = [&](int s) { return p_amp * std::sin(omega_drive * (double)s * dt_mix); };
+  for (int s = 0; s < nsteps; s++) {
+    const double PLm = pl(s - 1), PLn = pl(s), PLp = pl(s + 1);
+    const double PC0 = PLn + b.PL0, PC1 = 0.5 * (PLp - PLm) / dt_mix,
+                 PC2 = 0.5 * (PLp + PLm - 2.0 * PLn) / (dt_mix * dt_mix);
+    if (scheme == 1) {
+      RkBubble m{&b, 3.0 * (b.gam - 1.0) * b.K0 * b.T0 / b.PG0, PC0, PC1, PC2, pi};
+      RkRun r{Rp, d1R, PGp, dtL, 0.0, dt_mix, 0.0, 0};
+      if (!rk45_run(m, r, param, 100000000)) return -1;
+      Rt = Rp = Rn = r.R;
+      d1R = r.V;
+      PGp = r.PG;
+      dtL = std::min(r.h, dt_mix);
+      total += r.count;
+    } else {
+      double remain = re + dt_mix, time = -re;
+      while (remain > 0.0) {
+        double PGn = PGp;
+        double PL = PC2 * time * time + PC1 * time + PC0;
+        rp_substep_refined(Rt, Rp, Rn, d1R, PGn, PL, dtL, remain, b, param);
+        time = time + dtL;
+        Cplx alpha;
+        double omega = thermal_omega(alpha, PGn, Rn, b);
+        Cplx lp = thermal_lp(alpha, Rn);
+        PGp = gas_pressure(PGn, Rp, Rn, omega, dtL, lp, b);
+        total++;
+        if (total > 100000000) return -1;
+      }
+      re = remain;
+    }
     R_out[s] = Rt;
     PG_out[s] = PGp;
   }

@@ -61,6 +61,13 @@ double crpo_solve_pg(const double* bp, double PGn, double Rp, double Rn, double 
  * total number of sub-steps (-1 if it exceeded 1e8). */
 int64_t crpo_bubble_history(const double* bp, double R_init, double dt_mix, double dpl, int32_t nsteps, double* R_out,
                             double* PG_out);
+/* One bubble from rest at R_init driven by a liquid pressure P0 + p_amp
+ * sin(omega_drive t) for nsteps mixture steps of dt_mix, with the reference's
+ * sub-step scheme (scheme 0, its step limits divided by param >= 1) or the
+ * rk45 scheme (scheme 1, rtol = param).  R_out/PG_out get R_t and PG after each
+ * step.  Returns the total number of steps (-1 on failure). */
+int64_t crpo_bubble_drive(const double* bp, double R_init, double dt_mix, double p_amp, double omega_drive,
+                          int32_t nsteps, int32_t scheme, double param, double* R_out, double* PG_out);
 /* Derived scalars in the order of crp_ref_host_scalars (oracle/ref_harness.inc). */
 void crpo_host_scalars(const crp_config* cfg, double* out);
 /* PML profiles and cylindrical metrics: mx[i1m], my[j1m], nx[i2n], ny[j2n], xu[i2n], rxp[i2m]. */

@@ -1,0 +1,78 @@
+"""The rk45 radius scheme (ext.rp_scheme = rk45) in the oracle, on CPU.
+
+A single bubble driven by a sinusoidal liquid pressure (crpo_bubble_drive):
+the Dormand-Prince integration converges at the rate its tolerance sets, and
+the reference's own three-level scheme, with its step limits refined, converges
+towards the same solution (the two integrate the same model; rk45.cuh and the
+oracle document the continuous form of the gas-pressure update).  An
+unforced bubble at equilibrium stays at R0.  A coupled simulation with the
+scheme runs and its radii stay near the reference scheme's, which are first
+order accurate."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import _bind as B
+
+R0, P0, SIG, GAM, MU, RHO, K0, T0 = 3e-6, 101325.0, 0.0725, 1.4, 1e-3, 998.0, 26.2e-3, 293.15
+DT = 1.3495e-8  # mixture step of the 1024 x 2048 workload
+BP = np.array([R0, P0 + 2 * SIG / R0, P0, T0, GAM, SIG, MU, RHO, K0, 0.1 * DT])
+
+
+def drive(scheme, param, amp, steps):
+    f = B.oracle_lib().crpo_bubble_drive
+    f.restype = ctypes.c_int64
+    f.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                  ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+    R, PG = np.zeros(steps), np.zeros(steps)
+    n = f(BP.ctypes.data, R0, DT, amp, 2 * np.pi * 1e6, steps, scheme, param, R.ctypes.data, PG.ctypes.data)
+    assert n > 0
+    return R, PG, n
+
+
+@pytest.mark.parametrize("amp", [2e5, 1e6])
+def test_rk45_converges_at_its_tolerance(amp):
+    best, best_pg, _ = drive(1, 1e-12, amp, 300)
+    assert best.max() > 3 * R0 and best.min() < 0.4 * R0  # a driven growth and collapse
+    prev = np.inf
+    for tol in (1e-5, 1e-6, 1e-7, 1e-8):
+        R, PG, _ = drive(1, tol, amp, 300)
+        err = np.abs(R - best).max() / best.max()
+        assert err < 100 * tol, (tol, err)
+        assert err < prev
+        prev = err
+        assert np.abs(PG - best_pg).max() / best_pg.max() < 1000 * tol
+
+
+def test_reference_scheme_converges_to_rk45():
+    amp = 1e6
+    best, _, _ = drive(1, 1e-12, amp, 300)
+    errs = []
+    for refine in (1, 4, 16):
+        R, _, _ = drive(0, refine, amp, 300)
+        errs.append(np.abs(R - best).max() / best.max())
+    # First order: each four-fold refinement cuts the error by about four.
+    assert errs[0] > errs[1] > errs[2]
+    assert errs[2] < 0.03 and errs[0] / errs[2] > 8
+
+
+def test_rk45_equilibrium_bubble_stays():
+    R, PG, n = drive(1, 1e-7, 0.0, 200)
+    assert np.abs(R - R0).max() / R0 < 1e-10
+    assert n == 200 or n < 400  # one or two steps per mixture step at rest
+
+
+def test_rk45_simulation_runs_close_to_reference_scheme():
+    cfg = B.small_config()
+    ref = B.OracleSim(cfg)
+    cfg_rk = B.small_config(ext_rp_scheme=1)
+    rk = B.OracleSim(cfg_rk)
+    ref.step(150)
+    rk.step(150)
+    a, b = rk.bubbles("R_t"), ref.bubbles("R_t")
+    assert np.all(np.isfinite(a))
+    assert np.abs(a - b).max() / np.abs(b).max() < 0.05
+    # Far fewer steps per mixture step than the reference's sub-steps.
+    assert rk.stats().rp_substeps_max < ref.stats().rp_substeps_max
+    assert np.all(rk.bubbles("re") == 0.0)
