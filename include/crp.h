@@ -141,8 +141,9 @@ typedef enum crp_rp_scheme {
   CRP_RP_RK45 = 1   /* Dormand-Prince 5(4) with embedded error control on (R, R', PG),
                        the gas pressure from the continuous form of the same thermal
                        model; each mixture step ends exactly on the step's end.  In the
-                       mixed path the thermal model runs in FP32 except in the stiff
-                       phase (R / R0 < 0.3 or |R'| > 0.1 c_inf), where all of it is FP64 */
+                       mixed path the thermal model runs in FP32 only near equilibrium
+                       (|R / R0 - 1| <= 1e-3); in the stiff phase (R / R0 < 0.3 or
+                       |R'| > 0.1 c_inf) and elsewhere all of it is FP64 */
 } crp_rp_scheme;
 
 /* Dense host layouts of the readable fields, in the reference's index order:

@@ -45,7 +45,10 @@ def rel_err(a, b, floor):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), floor))
 
 
-def _compare(gpu, cpu, tol):
+def _compare(gpu, cpu, tol, loose=None):
+    """Every field and bubble quantity within tol of the oracle (relative max
+    error with the FLOOR of each); quantities in `loose` within their own bound."""
+    loose = loose or {}
     worst = {}
     fields = FIELDS + (["T"] if gpu._keep[0].dbg_T else [])
     for k in fields:
@@ -59,7 +62,7 @@ def _compare(gpu, cpu, tol):
         for k in ("ibn_x", "ibn_y", "ibm_x", "ibm_y"):
             assert np.array_equal(gpu.bubbles(k), cpu.bubbles(k)), k
     print({k: f"{v:.2e}" for k, v in worst.items()})
-    bad = {k: v for k, v in worst.items() if not v <= tol}
+    bad = {k: v for k, v in worst.items() if not v <= loose.get(k, tol)}
     assert not bad, bad
 
 

@@ -30,7 +30,12 @@ def test_rk45_fp64_matches_oracle(name):
         gs, cs = gpu.stats(), cpu.stats()
         print(name, "picard", gs.picard_total, cs.picard_total, "steps max", gs.rp_substeps_max, cs.rp_substeps_max)
         assert abs(gs.picard_total - cs.picard_total) <= max(2, cs.picard_total // 50)
-        _compare(gpu, cpu, TOL_FP64)
+        # The next trial step size comes from the error estimate, a difference of
+        # stage combinations that cancels to ~1e-7 of the stages: its rounding
+        # moves the proposed step by up to a few 1e-4 (measured 2e-4) while the
+        # state it produces agrees to 1e-10.  It is a controller quantity,
+        # compared more loosely than the state.
+        _compare(gpu, cpu, TOL_FP64, loose={"bub_dt": 1e-2})
         if gpu.dims.num_bubbles:
             assert np.all(gpu.bubbles("re") == 0.0)
             assert abs(gs.rp_substeps_max - cs.rp_substeps_max) <= max(2, cs.rp_substeps_max // 20)
