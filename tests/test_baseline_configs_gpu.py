@@ -1,0 +1,149 @@
+"""Parity on the benchmark's own configurations, not only on small grids.
+
+Configuration 1 (axisym_256x512: 256 x 512 axisymmetric grid, 4096 seeded
+bubbles, 0.5 MPa focused burst) is run from t = 0 on the CUDA path in FP64 and
+in the mixed form, and on the FP64 oracle, in lockstep, until each stops.  The
+drive grows the bubble cloud until the mixture model stops converging; the
+oracle does the same, so the CUDA path must stop at the same step.
+
+Measured (one B200, 16 host cores for the oracle), relative to the oracle:
+FP64 p0 ~1e-15 through the quiet phase, 8e-12 (R_t 2e-10) at the focal arrival
+(step 1000, focal pressure 1.9 MPa), then growing about tenfold per ten steps
+once the cloud is driven (R/R0 > 20): 5e-8 at step 1100, 1e-3 at 1200; both
+stop with CRP_ERR_PICARD at step 1220.  The mixed form's focal-pressure error
+is 5e-7 at the focal arrival and 4e-5 fifty steps later (the 1e-4 target), and
+grows past it from step 1060; it stops at step 1172 (its Picard threshold is
+1e-5, since FP32 storage of f_g leaves a residual floor near 7e-7).
+
+Configuration 2 (axisym_1024x2048, 262144 bubbles) is compared over a bounded
+window from t = 0, the oracle's time being about 0.1 s per step.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import _bind as B
+import crp
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CONF = os.path.join(ROOT, "cuda-rp_b200", "configs")
+TOL = 1e-9
+FOCAL_ARRIVAL = 1000  # mixture step at which the burst reaches the focus (40 mm / 1482 m/s / dt)
+
+
+def rel_l2(a, b):
+    n = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / n) if n > 0 else float(np.linalg.norm(a))
+
+
+def rel_max(a, b, floor):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), floor))
+
+
+def focal_mask(dims, cfg, radius=2e-3):
+    fy = cfg.tr_focal_dist * 0.5 * np.sqrt(3.0)
+    ii, jj = np.meshgrid(np.arange(dims.i1m), np.arange(dims.j1m))
+    return np.hypot((ii - 0.5) * dims.dx, (jj - 0.5) * dims.dy - fy) <= radius
+
+
+@pytest.fixture(scope="module")
+def cfg1_run():
+    """Lockstep run of configuration 1: errors at checkpoints and the steps at
+    which each path stopped."""
+    path = os.path.join(CONF, "axisym_256x512.conf")
+    cfg = crp.parse_file(path)
+    bub = crp.seed_bubbles(cfg)
+    ocfg = B.oracle_parse_file(path)
+    oracle = B.OracleSim(ocfg, B.oracle_seed_bubbles(ocfg), threads=os.cpu_count() or 1)
+    mcfg = crp.Config.from_buffer_copy(cfg)
+    mcfg.ext_precision = 1
+    sims = {"fp64": crp.Sim(cfg, bub), "mixed": crp.Sim(mcfg, bub), "oracle": oracle}
+    mask = focal_mask(sims["fp64"].dims, cfg)
+    stopped, status, records = {}, {}, {}
+    checkpoints = [500, FOCAL_ARRIVAL, 1050, 1100]
+    step = 0
+    try:
+        while len(stopped) < 3 and step < 1400:
+            n = 100 if step < 900 else 10
+            for name, s in sims.items():
+                if name in stopped:
+                    continue
+                try:
+                    s.step(n)
+                except crp.CrpError as e:
+                    stopped[name] = int(s.stats().steps) + 1
+                    status[name] = e.status
+            step += n
+            if step in checkpoints and "oracle" not in stopped:
+                po, vo, ro = oracle.field("p0"), oracle.field("vx"), oracle.bubbles("R_t")
+                rec = {"picard_oracle": int(oracle.stats().picard_total)}
+                for name in ("fp64", "mixed"):
+                    if name in stopped:
+                        continue
+                    s = sims[name]
+                    p = s.field("p0")
+                    rec[name] = {"p0": rel_max(p, po, 1e-3), "vx": rel_max(s.field("vx"), vo, 1e-9),
+                                 "R_t": rel_max(s.bubbles("R_t"), ro, 1e-9), "focal_l2": rel_l2(p[mask], po[mask]),
+                                 "picard": int(s.stats().picard_total)}
+                records[step] = rec
+    finally:
+        for name in ("fp64", "mixed"):
+            sims[name].close()
+        oracle.close()
+    print("cfg1 checkpoints", records, "stopped", stopped)
+    return {"records": records, "stopped": stopped, "status": status}
+
+
+def test_cfg1_fp64_matches_oracle_through_focal_arrival(cfg1_run):
+    for step in (500, FOCAL_ARRIVAL):
+        r = cfg1_run["records"][step]["fp64"]
+        assert r["p0"] < TOL and r["vx"] < TOL and r["R_t"] < TOL, (step, r)
+        assert r["picard"] == cfg1_run["records"][step]["picard_oracle"]
+
+
+def test_cfg1_driven_phase_stays_close_until_the_cloud_amplifies(cfg1_run):
+    # 100 steps after the arrival the driven cloud has amplified rounding
+    # differences by about 1e3 (measured 5e-8); still far below the physics.
+    r = cfg1_run["records"][1100]["fp64"]
+    assert r["p0"] < 1e-5 and r["R_t"] < 1e-5, r
+    assert abs(r["picard"] - cfg1_run["records"][1100]["picard_oracle"]) <= 2
+
+
+def test_cfg1_cuda_and_oracle_stop_at_the_same_step(cfg1_run):
+    st, code = cfg1_run["stopped"], cfg1_run["status"]
+    assert "fp64" in st and "oracle" in st, st
+    assert code["fp64"] == 6 and code["oracle"] == 6  # CRP_ERR_PICARD
+    assert st["fp64"] == st["oracle"], st
+
+
+def test_cfg1_mixed_focal_error_at_arrival(cfg1_run):
+    for step in (FOCAL_ARRIVAL, 1050):
+        r = cfg1_run["records"][step]["mixed"]
+        assert r["focal_l2"] < 1e-4, (step, r)
+
+
+def test_cfg2_fp64_window_matches_oracle():
+    path = os.path.join(CONF, "axisym_1024x2048.conf")
+    cfg = crp.parse_file(path)
+    ocfg = B.oracle_parse_file(path)
+    oracle = B.OracleSim(ocfg, B.oracle_seed_bubbles(ocfg), threads=os.cpu_count() or 1)
+    try:
+        with crp.Sim(cfg, crp.seed_bubbles(cfg)) as gpu:
+            # The first steps' pressure is a ramped source of millipascals; the
+            # comparison starts once it has grown (floor 1 Pa for p0).
+            for n in (60, 60):
+                gpu.step(n)
+                oracle.step(n)
+                errs = {"p0": rel_max(gpu.field("p0"), oracle.field("p0"), 1.0),
+                        "vx": rel_max(gpu.field("vx"), oracle.field("vx"), 1e-9),
+                        "vy": rel_max(gpu.field("vy"), oracle.field("vy"), 1e-9),
+                        "f_g": rel_max(gpu.field("f_g"), oracle.field("f_g"), 1e-12),
+                        "R_t": rel_max(gpu.bubbles("R_t"), oracle.bubbles("R_t"), 1e-9)}
+                print("cfg2 step", gpu.stats().steps, errs)
+                assert all(v < TOL for v in errs.values()), errs
+                assert gpu.stats().picard_total == oracle.stats().picard_total
+    finally:
+        oracle.close()
