@@ -199,13 +199,13 @@ constexpr int kStripRows = 8;    // rows per chunk (measured best of 4-16 at 102
 constexpr int kStripStages = 4;  // ring slots (rows) per warp; a smaller ring leaves more L1 (measured)
 constexpr int kStripFields = 7;  // pnx, pny, fgA, vx_old, vy_old, fgB, fgC
 
-template <typename P>
-__global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_constant__ GridParams g,
+template <typename P, int STAGES = kStripStages, int ROWS = kStripRows, int MINB = 4>
+__global__ void __launch_bounds__(32 * kStripWarps, MINB) fdtd_strip(const __grid_constant__ GridParams g,
                                                                const FdtdArgs<P> a) {
   using G = typename P::G;
   using S = typename P::S;
   using V = typename P::V;
-  __shared__ __align__(16) double ring[kStripWarps][kStripStages][kStripFields][32];
+  __shared__ __align__(16) double ring[kStripWarps][STAGES][kStripFields][32];
   const Frame& f = g.f;
   const int X = f.X, Y = f.Y;
   const unsigned full = 0xffffffffu;
@@ -222,8 +222,8 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
   // that the PML bands at both y ends (the slowest chunks: general updates
   // with divisions) start first and the cheap interior chunks fill the tail.
   const int by = blockIdx.y, cy = (by & 1) ? (int)gridDim.y - 1 - (by >> 1) : (by >> 1);
-  const int j0 = 1 + cy * kStripRows;
-  const int j1 = min(Y, j0 + kStripRows - 1);
+  const int j0 = 1 + cy * ROWS;
+  const int j1 = min(Y, j0 + ROWS - 1);
   const double xm = ((double)i - 0.5) * g.dx;
   const bool inner_col = i >= 1 && i <= X;
   const bool src_rows = g.source_row > 0 && src_pressure(g);
@@ -243,14 +243,14 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
   };
   // Ring slot of field fld of chunk row rr (row j0 - 1 + rr); each lane only
   // touches its own column.
-  auto slot = [&](int rr, int fld) -> double* { return &ring[threadIdx.y][rr % kStripStages][fld][lane]; };
+  auto slot = [&](int rr, int fld) -> double* { return &ring[threadIdx.y][rr % STAGES][fld][lane]; };
   // Queue the copies of chunk row rr: pnx, pny, fgA for rows j0-1..j1+1,
   // vy_old for j0-1..j1, vx_old, fgB, fgC for j0..j1.  One commit group per
   // row, empty past the chunk, so that a fixed wait count always means "the
   // next row landed".
   auto issue = [&](int rr) {
     const int r = j0 - 1 + rr;
-    if (rr <= kStripRows + 1 && r <= j1 + 1) {
+    if (rr <= ROWS + 1 && r <= j1 + 1) {
       const unsigned k = kb + (unsigned)rr * pitch;
       a.pnx.stage(slot(rr, 0), k);
       a.pny.stage(slot(rr, 1), k);
@@ -267,8 +267,8 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
     __pipeline_commit();
   };
 #pragma unroll
-  for (int rr = 0; rr < kStripStages; rr++) issue(rr);
-  __pipeline_wait_prior(kStripStages - 2);  // rows j0-1 and j0 have landed
+  for (int rr = 0; rr < STAGES; rr++) issue(rr);
+  __pipeline_wait_prior(STAGES - 2);  // rows j0-1 and j0 have landed
 
   // Row below the chunk and the chunk's first row.
   double pxc, pyc, fac, p0b, rhob, vyob;
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
     rhob = rho_of(fab);
     if (j0 == 1 && own) predict(f.idx(i, 0), fab);
   }
-  issue(kStripStages);  // reuses the slot of row j0-1
+  issue(STAGES);  // reuses the slot of row j0-1
   double p0c = p0_of(j0, pxc, pyc), rhoc = rho_of(fac);
   double vyd = 0.0;
   if (cell) {
@@ -311,11 +311,11 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
   // across the warp too.
   unsigned long long res = 0ull;  // max |dp0| as a bit pattern (NaN sorts above every number)
 #pragma unroll 1
-  for (int jj = 0; jj < kStripRows; jj++) {
+  for (int jj = 0; jj < ROWS; jj++) {
     const int j = j0 + jj;
     if (j > j1) break;
     const unsigned k = kb + (unsigned)(jj + 1) * pitch;  // (i, j) for every lane that stores
-    __pipeline_wait_prior(kStripStages - 2);              // row j+1 has landed
+    __pipeline_wait_prior(STAGES - 2);              // row j+1 has landed
     const double pxn = S::staged(slot(jj + 2, 0)), pyn = S::staged(slot(jj + 2, 1));
     const double fan = G::staged(slot(jj + 2, 2));
     const double vxo = V::staged(slot(jj + 1, 3)), vyo = V::staged(slot(jj + 1, 4));
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(32 * kStripWarps, 4) fdtd_strip(const __grid_c
     fac = fan;
     p0c = p0n;
     rhoc = rhon;
-    issue(jj + 1 + kStripStages);  // reuses the slot of row j
+    issue(jj + 1 + STAGES);  // reuses the slot of row j
   }
   if (j1 == Y && own) predict(f.idx(i, Y + 1), fac);
   // Warp maximum, one atomic per warp with a nonzero residual (no block
@@ -1681,8 +1681,7 @@ struct Sim {
   // Tensor maps of every field buffer for fdtd_tma: velocity [vx, vy][buffer],
   // split pressure [px, py][buffer], void-fraction ring.
   CUtensorMap tm_v[2][2]{}, tm_p[2][2]{}, tm_fg[3]{};
-  bool fdtd_tma_on = std::getenv("CRP_FDTD_TILE") != nullptr;
-  int tile_ntx = 1, tile_n = 1, tile_grid = 1;
+  bool fdtd_tma_on = std::getenv("CRP_FDTD_TILE") != nullptr;  int tile_ntx = 1, tile_n = 1, tile_grid = 1;
   BubbleArrays bub{};
   Bins bins{};
   // Device scalars written by the kernels, read back once per pressure evaluation.
@@ -2640,8 +2639,8 @@ struct Sim {
       e = launch(kClassFdtd, [&] { fdtd_tile<P><<<grid, block, smem, stream>>>(gp, fa, m, ntx, nt, perr); });
     } else {
       const int strips = (gp.f.X + kStripCells - 1) / kStripCells;
-      dim3 grid((strips + kStripWarps - 1) / kStripWarps, (gp.f.Y + kStripRows - 1) / kStripRows);
       dim3 block(32, kStripWarps);
+      dim3 grid((strips + kStripWarps - 1) / kStripWarps, (gp.f.Y + kStripRows - 1) / kStripRows);
       e = launch(kClassFdtd, [&] { fdtd_strip<P><<<grid, block, 0, stream>>>(gp, fa); });
     }
     if (e != cudaSuccess) return e;
