@@ -47,12 +47,20 @@ class Config(ctypes.Structure):
         ("ext_bubble_seed", ctypes.c_uint64), ("ext_r0_sigma_ln", c_dbl), ("ext_cloud_shape", c_int),
         ("ext_cloud_r", c_dbl), ("ext_cloud_h", c_dbl), ("ext_n_b", c_dbl), ("ext_picard_tol", c_dbl),
         ("ext_graphs", c_int), ("ext_elements", c_int), ("ext_rp_scheme", c_int), ("ext_rp_tol", c_dbl),
+        ("ext_grid_z", c_int), ("ext_grid_lz", c_dbl), ("ext_pml_z0", c_int), ("ext_pml_z1", c_int),
+        ("ext_array_elements", c_int), ("ext_array_radius", c_dbl), ("ext_array_focus_dx", c_dbl),
+        ("ext_array_seed", ctypes.c_uint64), ("ext_array_phases", c_int),
     ]
 
 
 class Dims(ctypes.Structure):
     _fields_ = [("i1m", c_int), ("j1m", c_int), ("i2m", c_int), ("j2m", c_int), ("i2n", c_int),
                 ("j2n", c_int), ("num_bubbles", c_int), ("dx", c_dbl), ("dy", c_dbl), ("dt", c_dbl)]
+
+
+class Dims3(ctypes.Structure):
+    _fields_ = [("nx", c_int), ("ny", c_int), ("nz", c_int), ("num_bubbles", c_int), ("dx", c_dbl), ("dy", c_dbl),
+                ("dz", c_dbl), ("dt", c_dbl), ("source_cells", c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -84,14 +92,15 @@ class OutputPlan(ctypes.Structure):
 
 class BubblesIn(ctypes.Structure):
     _fields_ = [("n", c_int), ("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("r0", ctypes.c_void_p),
-                ("n_b", ctypes.c_void_p)]
+                ("n_b", ctypes.c_void_p), ("z", ctypes.c_void_p)]
 
 
 FIELDS = {"p0": 0, "px": 1, "py": 2, "pnx": 3, "pny": 4, "vx": 5, "vy": 6, "f_g": 7, "f_gn": 8, "T": 11,
-          "f_gm": 9, "rho_m": 10}
+          "f_gm": 9, "rho_m": 10, "vz": 12, "pz": 13}
 BUBBLE_FIELDS = {"x": 0, "y": 1, "R_t": 2, "R_p": 3, "R_n": 4, "d1_R_p": 5, "PG_p": 6, "PL_p": 7,
                  "PL_n": 8, "PL_m": 9, "dt": 10, "re": 11, "Q_B": 12, "n_B": 13, "R0": 14, "v_x": 15,
-                 "v_y": 16, "ibm_x": 17, "ibm_y": 18, "ibn_x": 19, "ibn_y": 20, "substeps": 21}
+                 "v_y": 16, "ibm_x": 17, "ibm_y": 18, "ibn_x": 19, "ibn_y": 20, "substeps": 21,
+                 "z": 22, "v_z": 23, "ibm_z": 24, "ibn_z": 25}
 
 
 class CrpError(RuntimeError):
@@ -109,6 +118,12 @@ def field_shape(dims, name: str) -> tuple[int, int]:
     if name == "vy":
         return dims.j2n, dims.i2m
     return dims.j2m, dims.i2m
+
+
+def field_shape3(d3, name: str) -> tuple[int, int, int]:
+    """(depth, height, width) of a 3-D field's dense array (x fastest)."""
+    nz, ny, nx = d3.nz, d3.ny, d3.nx
+    return {"vx": (nz, ny, nx + 1), "vy": (nz, ny + 1, nx), "vz": (nz + 1, ny, nx)}.get(name, (nz, ny, nx))
 
 
 def _ptr(a: np.ndarray) -> ctypes.c_void_p:
@@ -134,6 +149,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "crp_config_parse_file": (c_int, [ctypes.c_char_p, P(Config), ctypes.c_char_p, ctypes.c_size_t]),
         "crp_config_parse_string": (c_int, [ctypes.c_char_p, P(Config), ctypes.c_char_p, ctypes.c_size_t]),
         "crp_seed_bubbles": (c_int, [P(Config), vp, vp, vp, vp]),
+        "crp_seed_bubbles3": (c_int, [P(Config), vp, vp, vp, vp, vp]),
+        "crp_get_dims3": (c_int, [vp, P(Dims3)]),
         "crp_create": (c_int, [P(Config), P(BubblesIn), vp, P(vp)]),
         "crp_step": (c_int, [vp, c_int]),
         "crp_get_dims": (c_int, [vp, P(Dims)]),
@@ -200,11 +217,14 @@ class Bubbles:
     y: np.ndarray
     r0: np.ndarray
     n_b: np.ndarray
+    z: np.ndarray | None = None  # 3-D grids only
 
     def as_c(self) -> BubblesIn:
-        for a in (self.x, self.y, self.r0, self.n_b):
+        arrays = (self.x, self.y, self.r0, self.n_b) + ((self.z,) if self.z is not None else ())
+        for a in arrays:
             assert a.dtype == np.float64 and a.flags.c_contiguous
-        return BubblesIn(len(self.x), _ptr(self.x), _ptr(self.y), _ptr(self.r0), _ptr(self.n_b))
+        return BubblesIn(len(self.x), _ptr(self.x), _ptr(self.y), _ptr(self.r0), _ptr(self.n_b),
+                         _ptr(self.z) if self.z is not None else None)
 
 
 def seed_bubbles(cfg: Config) -> Bubbles:
@@ -214,6 +234,15 @@ def seed_bubbles(cfg: Config) -> Bubbles:
     if st:
         raise CrpError(st, "crp_seed_bubbles")
     return Bubbles(*arrs)
+
+
+def seed_bubbles3(cfg: Config) -> Bubbles:
+    n = cfg.ext_bubble_count
+    x, y, z, r0, nb = (np.zeros(n) for _ in range(5))
+    st = load().crp_seed_bubbles3(ctypes.byref(cfg), _ptr(x), _ptr(y), _ptr(z), _ptr(r0), _ptr(nb))
+    if st:
+        raise CrpError(st, "crp_seed_bubbles3")
+    return Bubbles(x, y, r0, nb, z)
 
 
 class Sim:
@@ -231,6 +260,10 @@ class Sim:
         self.h = h
         self.dims = Dims()
         self._check(self.lib.crp_get_dims(self.h, ctypes.byref(self.dims)))
+        self.dims3 = None
+        if cfg.ext_grid_z > 0:
+            self.dims3 = Dims3()
+            self._check(self.lib.crp_get_dims3(self.h, ctypes.byref(self.dims3)))
 
     def _check(self, st: int):
         if st:
@@ -248,7 +281,7 @@ class Sim:
     def field(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
         """Dense copy of a field; into `out` (float64, C-contiguous, the field's
         shape) when given, e.g. a pinned host buffer."""
-        shape = field_shape(self.dims, name)
+        shape = field_shape3(self.dims3, name) if self.dims3 is not None else field_shape(self.dims, name)
         if out is None:
             out = np.empty(shape, dtype=np.float64)
         assert out.shape == shape and out.dtype == np.float64 and out.flags.c_contiguous
@@ -345,6 +378,7 @@ class _BatchSim(Sim):
         self.h = ctypes.c_void_p(h)
         self.dims = Dims()
         self._check(self.lib.crp_get_dims(self.h, ctypes.byref(self.dims)))
+        self.dims3 = None
 
     def close(self):
         self.h = None

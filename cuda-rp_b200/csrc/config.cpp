@@ -161,6 +161,15 @@ const Key kKeys[] = {
     K("ext.elements", kInt, ext_elements),
     K("ext.rp_scheme", kScheme, ext_rp_scheme),
     K("ext.rp_tol", kDouble, ext_rp_tol),
+    K("ext.grid_z", kInt, ext_grid_z),
+    K("ext.grid_lz", kDouble, ext_grid_lz),
+    K("ext.pml_z0", kBool, ext_pml_z0),
+    K("ext.pml_z1", kBool, ext_pml_z1),
+    K("ext.array_elements", kInt, ext_array_elements),
+    K("ext.array_radius", kDouble, ext_array_radius),
+    K("ext.array_focus_dx", kDouble, ext_array_focus_dx),
+    K("ext.array_seed", kU64, ext_array_seed),
+    K("ext.array_phases", kInt, ext_array_phases),
 };
 #undef K
 
@@ -370,6 +379,57 @@ crp_status crp_seed_bubbles(const crp_config* cfg, double* x, double* y, double*
   return CRP_OK;
 }
 
+crp_status crp_seed_bubbles3(const crp_config* cfg, double* x, double* y, double* z, double* r0, double* n_b) {
+  if (!cfg || !x || !y || !z || !r0 || !n_b || cfg->ext_bubble_count <= 0 || cfg->ext_grid_z <= 0)
+    return CRP_ERR_INVALID;
+  const double pi = std::acos(-1.0);
+  // The cloud sits at the bowl's focus: the grid's centre moved by focus_dx along x.
+  const double cx = 0.5 * cfg->grid_lx + cfg->ext_array_focus_dx, cy = 0.5 * cfg->grid_ly,
+               cz = 0.5 * cfg->ext_grid_lz;
+  const double R = cfg->ext_cloud_r;
+  Philox g{(uint32_t)cfg->ext_bubble_seed, (uint32_t)(cfg->ext_bubble_seed >> 32)};
+  for (int32_t k = 0; k < cfg->ext_bubble_count; k++) {
+    uint32_t a[4], b[4];
+    g.block((uint64_t)k, 0u, a);
+    g.block((uint64_t)k, 1u, b);
+    double ox, oy, oz;
+    switch (cfg->ext_cloud_shape) {
+      case 1: {  // ball
+        const double rs = R * std::cbrt(unit(a[0]));
+        const double ct = 2.0 * unit(a[1]) - 1.0;
+        const double st = std::sqrt(std::max(0.0, 1.0 - ct * ct));
+        const double ph = 2.0 * pi * unit(a[2]);
+        ox = rs * st * std::cos(ph);
+        oy = rs * st * std::sin(ph);
+        oz = rs * ct;
+        break;
+      }
+      case 2: {  // Gaussian per axis
+        const double rad = std::sqrt(-2.0 * std::log(unit(a[0])));
+        ox = R * rad * std::cos(2.0 * pi * unit(a[1]));
+        oy = R * rad * std::sin(2.0 * pi * unit(a[1]));
+        oz = R * std::sqrt(-2.0 * std::log(unit(b[2]))) * std::cos(2.0 * pi * unit(b[3]));
+        break;
+      }
+      default: {  // cylinder along z, area-uniform in the radius
+        const double rr = R * std::sqrt(unit(a[0]));
+        const double ph = 2.0 * pi * unit(a[2]);
+        ox = rr * std::cos(ph);
+        oy = rr * std::sin(ph);
+        oz = (unit(a[1]) - 0.5) * cfg->ext_cloud_h;
+        break;
+      }
+    }
+    const double nrm = std::sqrt(-2.0 * std::log(unit(b[0]))) * std::cos(2.0 * pi * unit(b[1]));
+    x[k] = cx + ox;
+    y[k] = cy + oy;
+    z[k] = cz + oz;
+    r0[k] = cfg->bub_R0 * std::exp(cfg->ext_r0_sigma_ln * nrm);
+    n_b[k] = cfg->ext_n_b;
+  }
+  return CRP_OK;
+}
+
 const char* crp_status_string(crp_status s) {
   switch (s) {
     case CRP_OK: return "ok";
@@ -389,3 +449,11 @@ const char* crp_status_string(crp_status s) {
 }
 
 }  // extern "C"
+
+namespace crp {
+// One Philox-4x32-10 block of the seeding's generator (the 3-D source's seeded phases).
+void philox_block(uint64_t seed, uint64_t counter, uint32_t stream, uint32_t out[4]) {
+  Philox g{(uint32_t)seed, (uint32_t)(seed >> 32)};
+  g.block(counter, stream, out);
+}
+}  // namespace crp

@@ -35,8 +35,10 @@
 
 #include "crp.h"
 #include "crp_device.cuh"
+#include "radius.cuh"
 #include "adjoint.cuh"
 #include "crp_host.h"
+#include "sim3d.h"
 
 namespace crp {
 
@@ -688,13 +690,7 @@ __global__ void bin_sort(const int* __restrict__ start, int* __restrict__ idx, i
   }
 }
 
-// Per-bubble state of BubbleRadiusKernel (inc/bubble_CUDA_kernel.cuh:471-554)
-// while its sub-steps run.
-struct RpState {
-  double Rt, Rp, Rn, d1Rp, PGp, dtL, remain, time, PC0, PC1, PC2, heat, vis, re_n;
-  BubbleR0 r;
-  long long count;
-};
+// RpState, thermal_model and rp_substep_full live in radius.cuh (shared with the 3-D path).
 
 // BubbleInterpolationScalarKernel (:361-395) for bubble n, then the set-up of
 // BubbleRadiusKernel from the state stored at the start of the step (:488-504).
@@ -743,53 +739,6 @@ __device__ __forceinline__ void rp_begin(const GridParams& g, const BubbleParams
   s.count = 0;
 }
 
-// One pass of the sub-step loop of BubbleRadiusKernel (:506-539).  T is the
-// real type of the thermal model (omega_N, alpha_N, Lp_N); everything else is FP64.
-template <typename T>
-__device__ __forceinline__ void thermal_model(const BubbleParams& bp, const RpState& s, double PGn, double& omega,
-                                              C64& lp) {
-  Cx<T> alpha_t;
-  ThermalConst<T> c;
-  if constexpr (sizeof(T) == sizeof(double))
-    c = thermal_const64(bp, s.r);
-  else
-    c = thermal_const32(bp, s.r);
-  omega = (double)omega_n<T>(alpha_t, (T)PGn, (T)s.Rn, c);
-  const Cx<T> lp_t = lp_n<T>(alpha_t, (T)s.Rn, c.cut2);
-  lp = C64{(double)lp_t.re, (double)lp_t.im};
-}
-
-// Relative radius excursion |R/R0 - 1| above which the mixed path evaluates
-// the thermal model in FP64: FP32 is accurate for the small oscillations of a
-// quiet bubble, and its rounding is amplified once the bubble is driven.
-constexpr double kThermalFp64Excursion = 1.0e-3;
-
-template <typename T>
-__device__ __forceinline__ void rp_substep_full(const BubbleParams& bp, RpState& s) {
-  const double PGn = s.PGp;
-  const double PL = s.PC2 * s.time * s.time + s.PC1 * s.time + s.PC0;
-  rp_substep(s.Rt, s.Rp, s.Rn, s.d1Rp, PGn, PL, s.dtL, s.remain, bp);
-  s.time = s.time + s.dtL;
-  double omega;
-  C64 lp;
-  if (sizeof(T) == sizeof(double) || fabs(s.Rn - s.r.R0) > kThermalFp64Excursion * s.r.R0)
-    thermal_model<double>(bp, s, PGn, omega, lp);
-  else
-    thermal_model<T>(bp, s, PGn, omega, lp);
-  const double den = lp.re * lp.re + lp.im * lp.im;
-  const double inv_wdt = 1.0 / (omega * s.dtL);
-  s.PGp = gas_pressure(PGn, s.Rp, s.Rn, inv_wdt, s.dtL, den, lp, bp, s.r);
-  const double inv_den = 1.0 / den;  // for the heat flux only, off the chain to the next sub-step
-  const double Rp = s.Rp, Rn = s.Rn, PGp = s.PGp;
-  const double s0 = 0.5 * (Rp + Rn);
-  const double s1 = inv_den * s.r.T0_PG0R03;
-  const double dTdr = lp.re * s1 * (s.r.PG0 * s.r.R03 - 0.5 * (PGp + PGn) * s0 * s0 * s0) +
-                      lp.im * s1 * (PGp * Rp * Rp * Rp - PGn * Rn * Rn * Rn) * inv_wdt;
-  s.heat -= 4.0 * bp.pi * Rp * Rp * bp.K0 * dTdr * s.dtL;
-  // 4 pi Rp^2 (4 mu d1Rp / Rp) d1Rp dt, with Rp^2 / Rp cancelled.
-  s.vis += 4.0 * bp.pi * Rp * 4.0 * bp.mu * s.d1Rp * s.d1Rp * s.dtL;
-  s.count++;
-}
 
 __device__ __forceinline__ void store_contrib(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
                                               int n, double Rt);
@@ -3101,6 +3050,12 @@ cudaError_t Sim::launch_couple(bool pressure) {
 // ---------------------------------------------------------------------------
 struct crp_sim {
   crp::Sim s;
+  crp::Sim3Impl* s3 = nullptr;  // a 3-D grid (ext.grid_z > 0) runs here instead of s
+  std::string err3;
+  ~crp_sim() {
+    if (s3) crp::sim3_destroy(s3);
+  }
+  int device() const { return s3 ? crp::sim3_device(s3) : s.device; }
 };
 
 namespace crp {
@@ -3115,8 +3070,8 @@ class DeviceScope {
  public:
   explicit DeviceScope(const crp_sim* h) {
     if (cudaGetDevice(&prev_) != cudaSuccess) prev_ = -1;
-    if (h && prev_ != h->s.device) {
-      ok_ = cudaSetDevice(h->s.device) == cudaSuccess;
+    if (h && prev_ != h->device()) {
+      ok_ = cudaSetDevice(h->device()) == cudaSuccess;
       switched_ = ok_;
     }
   }
@@ -3139,6 +3094,16 @@ crp_status crp_create(const crp_config* cfg, const crp_bubbles_in* bubbles, void
   *out = nullptr;
   crp_sim* h = new (std::nothrow) crp_sim();
   if (!h) return CRP_ERR_ALLOC;
+  if (cfg->ext_grid_z > 0) {
+    const crp_status st3 = crp::sim3_create(cfg, bubbles, stream, &h->s3, &h->err3);
+    if (st3 != CRP_OK) {
+      fprintf(stderr, "crp_create: %s\n", h->err3.c_str());
+      delete h;
+      return st3;
+    }
+    *out = h;
+    return CRP_OK;
+  }
   crp_status st = h->s.create(*cfg, bubbles, stream);
   if (st != CRP_OK) {
     fprintf(stderr, "crp_create: %s\n", h->s.err.c_str());
@@ -3153,11 +3118,24 @@ crp_status crp_step(crp_sim* h, int32_t n) {
   if (!h || n < 0) return CRP_ERR_INVALID;
   DeviceScope dev(h);
   if (!dev.ok()) return CRP_ERR_CUDA;
+  if (h->s3) return crp::sim3_step(h->s3, n);
   return h->s.step_n(n);
+}
+
+crp_status crp_get_dims3(const crp_sim* h, crp_dims3* d) {
+  if (!h || !d || !h->s3) return CRP_ERR_INVALID;
+  crp::sim3_dims(h->s3, d);
+  return CRP_OK;
 }
 
 crp_status crp_get_dims(const crp_sim* h, crp_dims* d) {
   if (!h || !d) return CRP_ERR_INVALID;
+  if (h->s3) {
+    crp_dims3 d3;
+    crp::sim3_dims(h->s3, &d3);
+    *d = crp_dims{d3.nx, d3.ny, d3.nx, d3.ny, d3.nx + 1, d3.ny + 1, d3.num_bubbles, d3.dx, d3.dy, d3.dt};
+    return CRP_OK;
+  }
   const crp::Frame& f = h->s.gp.f;
   d->i1m = f.X + 2;
   d->j1m = f.Y + 2;
@@ -3174,12 +3152,17 @@ crp_status crp_get_dims(const crp_sim* h, crp_dims* d) {
 
 crp_status crp_get_stats(const crp_sim* h, crp_stats* st) {
   if (!h || !st) return CRP_ERR_INVALID;
+  if (h->s3) {
+    *st = crp::sim3_stats(h->s3);
+    return CRP_OK;
+  }
   *st = h->s.stats;
   return CRP_OK;
 }
 
 crp_status crp_set_profiling(crp_sim* h, int32_t enable) {
   if (!h) return CRP_ERR_INVALID;
+  if (h->s3) return enable ? CRP_ERR_UNSUPPORTED : CRP_OK;
   DeviceScope dev(h);
   if (!dev.ok()) return CRP_ERR_CUDA;
   if (cudaStreamSynchronize(h->s.stream) != cudaSuccess) return CRP_ERR_CUDA;
@@ -3193,6 +3176,7 @@ crp_status crp_read_field(crp_sim* h, crp_field f, double* host) {
   if (!h || !host) return CRP_ERR_INVALID;
   DeviceScope dev(h);
   if (!dev.ok()) return CRP_ERR_CUDA;
+  if (h->s3) return crp::sim3_read_field(h->s3, f, host);
   return h->s.read_field(f, host);
 }
 
@@ -3200,6 +3184,7 @@ crp_status crp_read_bubbles(crp_sim* h, crp_bubble_field w, double* host) {
   if (!h || !host) return CRP_ERR_INVALID;
   DeviceScope dev(h);
   if (!dev.ok()) return CRP_ERR_CUDA;
+  if (h->s3) return crp::sim3_read_bubbles(h->s3, w, host);
   return h->s.read_bubbles(w, host);
 }
 
@@ -3235,11 +3220,13 @@ crp_status crp_set_source_elements(crp_sim* h, int32_t n, const double* amp, con
   if (!h) return CRP_ERR_INVALID;
   DeviceScope dev(h);
   if (!dev.ok()) return CRP_ERR_CUDA;
+  if (h->s3) return crp::sim3_set_elements(h->s3, n, amp, phase);
   return h->s.set_source_elements(n, amp, phase);
 }
 
 crp_status crp_adjoint(crp_sim* h, const crp_objective* obj, double* J, double* grad_amp, double* grad_phase) {
   if (!h) return CRP_ERR_INVALID;
+  if (h->s3) return CRP_ERR_UNSUPPORTED;
   DeviceScope dev(h);
   if (!dev.ok()) return CRP_ERR_CUDA;
   return h->s.adjoint(obj, J, grad_amp, grad_phase);
@@ -3261,9 +3248,12 @@ crp_status crp_minmax(const crp_sim* h, double* fg_min, double* fg_max, double* 
   return CRP_OK;
 }
 
-void* crp_stream(crp_sim* h) { return h ? (void*)h->s.stream : nullptr; }
+void* crp_stream(crp_sim* h) { return h ? (h->s3 ? crp::sim3_stream(h->s3) : (void*)h->s.stream) : nullptr; }
 
-const char* crp_last_error(const crp_sim* h) { return h ? h->s.err.c_str() : crp::noalloc_last_error(); }
+const char* crp_last_error(const crp_sim* h) {
+  if (!h) return crp::noalloc_last_error();
+  return h->s3 ? crp::sim3_error(h->s3) : h->s.err.c_str();
+}
 
 void crp_destroy(crp_sim* h) {
   if (!h) return;
@@ -3273,6 +3263,7 @@ void crp_destroy(crp_sim* h) {
 
 crp_status crp_write_rawdata(crp_sim* h, const char* dir) {
   if (!h || !dir) return CRP_ERR_INVALID;
+  if (h->s3) return CRP_ERR_UNSUPPORTED;
   DeviceScope dev(h);
   if (!dev.ok()) return CRP_ERR_CUDA;
   return crp::write_rawdata(h, dir);
@@ -3280,6 +3271,7 @@ crp_status crp_write_rawdata(crp_sim* h, const char* dir) {
 
 crp_status crp_write_sph(crp_sim* h, const char* dir) {
   if (!h || !dir) return CRP_ERR_INVALID;
+  if (h->s3) return CRP_ERR_UNSUPPORTED;
   DeviceScope dev(h);
   if (!dev.ok()) return CRP_ERR_CUDA;
   return crp::write_sph(h, dir);

@@ -130,6 +130,19 @@ typedef struct crp_config {
   int32_t ext_rp_scheme;     /* crp_rp_scheme: integrator of the bubble radius (default: the
                                 reference's three-level variable step) */
   double ext_rp_tol;         /* CRP_RP_RK45: relative error tolerance per step (0: 1e-6) */
+  /* 3-D Cartesian grid (no counterpart in the reference, which is 2-D): with
+     ext_grid_z > 0 the grid is grid_x x grid_y x ext_grid_z cells of
+     lx/x x ly/y x lz/z, planar (transducer.cylindrical off), with a PML on all
+     six faces (pml.x0..y1 and ext.pml_z0/z1 must all be on), bubbles in 3-D,
+     and the hemispherical array below as its source. */
+  int32_t ext_grid_z;
+  double ext_grid_lz;
+  int32_t ext_pml_z0, ext_pml_z1;
+  int32_t ext_array_elements;  /* elements of the hemispherical bowl (3-D source) */
+  double ext_array_radius;     /* [m] bowl radius about the grid's centre; opens towards +z */
+  double ext_array_focus_dx;   /* [m] focus offset from the centre along x (the bowl's phases focus there) */
+  uint64_t ext_array_seed;     /* seed of the phases when ext_array_phases = 1 */
+  int32_t ext_array_phases;    /* 0: focusing phases omega |x_e - focus| / c; 1: seeded, uniform in [0, 2 pi) */
 } crp_config;
 
 /* Integrator of the bubble radius and gas pressure over one mixture step. */
@@ -160,7 +173,11 @@ typedef enum crp_field {
   CRP_FIELD_FGN = 8,   /* i2m x j2m, previous step */
   CRP_FIELD_FGM = 9,   /* i2m x j2m, two steps back */
   CRP_FIELD_RHO_M = 10, /* i1m x j1m, mixture density as the next velocity update sees it */
-  CRP_FIELD_T = 11      /* i2m x j2m, mixture temperature rise over T_inf (debug.T = 1 only) */
+  CRP_FIELD_T = 11,     /* i2m x j2m, mixture temperature rise over T_inf (debug.T = 1 only) */
+  /* 3-D grids: cell fields are (Z+2) planes of (Y+2) x (X+2), x fastest; vx is
+     (Z+2) x (Y+2) x (X+3), vy (Z+2) x (Y+3) x (X+2), vz (Z+3) x (Y+2) x (X+2). */
+  CRP_FIELD_VZ = 12,    /* 3-D only */
+  CRP_FIELD_PZ = 13     /* 3-D only: the z split component of the pressure */
 } crp_field;
 
 typedef enum crp_bubble_field {
@@ -169,7 +186,8 @@ typedef enum crp_bubble_field {
   CRP_BUB_DT = 10, CRP_BUB_RE = 11, CRP_BUB_Q_B = 12, CRP_BUB_N_B = 13, CRP_BUB_R0 = 14,
   CRP_BUB_VX = 15, CRP_BUB_VY = 16,
   CRP_BUB_IBM_X = 17, CRP_BUB_IBM_Y = 18, CRP_BUB_IBN_X = 19, CRP_BUB_IBN_Y = 20,
-  CRP_BUB_SUBSTEPS = 21  /* RP sub-steps of the bubble's last radius solve */
+  CRP_BUB_SUBSTEPS = 21, /* RP sub-steps of the bubble's last radius solve */
+  CRP_BUB_Z = 22, CRP_BUB_VZ = 23, CRP_BUB_IBM_Z = 24, CRP_BUB_IBN_Z = 25  /* 3-D only */
 } crp_bubble_field;
 
 typedef struct crp_dims {
@@ -177,6 +195,15 @@ typedef struct crp_dims {
   int32_t num_bubbles;
   double dx, dy, dt;
 } crp_dims;
+
+/* crp_dims of a 3-D grid: cells per axis with ghost layers (X+2, Y+2, Z+2),
+ * the bubble count, the spacings, the step, and the cells of the bowl source. */
+typedef struct crp_dims3 {
+  int32_t nx, ny, nz;
+  int32_t num_bubbles;
+  double dx, dy, dz, dt;
+  int32_t source_cells;
+} crp_dims3;
 
 typedef struct crp_stats {
   int64_t steps;               /* mixture steps taken */
@@ -212,6 +239,7 @@ typedef struct crp_bubbles_in {
   const double* y;
   const double* r0;
   const double* n_b;
+  const double* z;  /* 3-D grids only (NULL otherwise) */
 } crp_bubbles_in;
 
 typedef struct crp_sim crp_sim;
@@ -231,6 +259,12 @@ crp_status crp_config_parse_string(const char* text, crp_config* cfg, char* err,
  * by ext_bubble_seed. */
 crp_status crp_seed_bubbles(const crp_config* cfg, double* x, double* y, double* r0, double* n_b);
 
+/* The same for a 3-D grid (ext_grid_z > 0): positions around the bowl's focus
+ * (the grid's centre plus ext_array_focus_dx along x) in a cylinder along z
+ * (radius cloud_r about the focus line, length cloud_h), a ball of radius
+ * cloud_r, or a Gaussian cloud of standard deviation cloud_r per axis. */
+crp_status crp_seed_bubbles3(const crp_config* cfg, double* x, double* y, double* z, double* r0, double* n_b);
+
 /* Build the simulation on the current CUDA device.  bubbles may be NULL (the
  * reference's lattice seeding, or ext seeding when ext_bubble_count > 0).
  * stream may be NULL (a stream is created) or a cudaStream_t to run on. */
@@ -240,6 +274,8 @@ crp_status crp_create(const crp_config* cfg, const crp_bubbles_in* bubbles, void
 crp_status crp_step(crp_sim* sim, int32_t n);
 
 crp_status crp_get_dims(const crp_sim* sim, crp_dims* dims);
+/* Dimensions of a 3-D simulation (CRP_ERR_INVALID for a 2-D one). */
+crp_status crp_get_dims3(const crp_sim* sim, crp_dims3* dims);
 crp_status crp_get_stats(const crp_sim* sim, crp_stats* stats);
 
 /* Copy one field into a dense host array (layout above). */

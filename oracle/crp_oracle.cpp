@@ -1517,3 +1517,11 @@ crp_status crpo_host_sigma(const crp_config* cfg, double* mx, double* my, double
 }
 
 }  // extern "C"
+
+// The 3-D Cartesian extension.
+namespace {
+void philox_block(uint64_t seed, uint64_t counter, uint32_t stream, uint32_t out[4]) {
+  crpo_philox_block(seed, counter, stream, out);
+}
+}  // namespace
+#include "oracle3d.inc"

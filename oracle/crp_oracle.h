@@ -46,6 +46,22 @@ void crpo_destroy(crpo_sim* sim);
 crp_status crpo_config_defaults(crp_config* cfg);
 crp_status crpo_config_parse_file(const char* path, crp_config* cfg, char* err, size_t err_len);
 crp_status crpo_seed_bubbles(const crp_config* cfg, double* x, double* y, double* r0, double* n_b);
+crp_status crpo_seed_bubbles3(const crp_config* cfg, double* x, double* y, double* z, double* r0, double* n_b);
+/* One Philox-4x32-10 block (key seed, counter, stream word), as the seeding draws. */
+void crpo_philox_block(uint64_t seed, uint64_t counter, uint32_t stream, uint32_t out[4]);
+
+/* The 3-D Cartesian extension (ext_grid_z > 0; oracle/oracle3d.inc states its
+ * discretisation).  Dense layouts as crp_read_field documents for 3-D grids. */
+typedef struct crpo3_sim crpo3_sim;
+crp_status crpo3_create(const crp_config* cfg, const crp_bubbles_in* bubbles, crpo3_sim** out);
+crp_status crpo3_step(crpo3_sim* sim, int32_t n);
+crp_status crpo3_set_source_elements(crpo3_sim* sim, int32_t n, const double* amp, const double* phase);
+crp_status crpo3_get_stats(const crpo3_sim* sim, crp_stats* stats);
+int32_t crpo3_num_bubbles(const crpo3_sim* sim);
+int32_t crpo3_num_source_cells(const crpo3_sim* sim);
+crp_status crpo3_read_field(crpo3_sim* sim, crp_field field, double* host);
+crp_status crpo3_read_bubbles(crpo3_sim* sim, crp_bubble_field what, double* host);
+void crpo3_destroy(crpo3_sim* sim);
 
 /* Bubble physics on single inputs, for comparison with the reference's
  * functions (inc/bubble_CUDA_kernel.cuh:227-340).  bp = (R0, PG0, PL0, T0, gam,

@@ -82,6 +82,11 @@ const std::map<std::string, Slot>& registry() {
       S("ext.n_b", T::F64, ext_n_b), S("ext.picard_tol", T::F64, ext_picard_tol),
       S("ext.graphs", T::Bool, ext_graphs), S("ext.elements", T::I32, ext_elements),
       S("ext.rp_scheme", T::Scheme, ext_rp_scheme), S("ext.rp_tol", T::F64, ext_rp_tol),
+      S("ext.grid_z", T::I32, ext_grid_z), S("ext.grid_lz", T::F64, ext_grid_lz),
+      S("ext.pml_z0", T::Bool, ext_pml_z0), S("ext.pml_z1", T::Bool, ext_pml_z1),
+      S("ext.array_elements", T::I32, ext_array_elements), S("ext.array_radius", T::F64, ext_array_radius),
+      S("ext.array_focus_dx", T::F64, ext_array_focus_dx), S("ext.array_seed", T::U64, ext_array_seed),
+      S("ext.array_phases", T::I32, ext_array_phases),
   };
 #undef S
   return m;
@@ -283,6 +288,55 @@ crp_status crpo_seed_bubbles(const crp_config* cfg, double* x, double* y, double
     n_b[k] = cfg->ext_n_b;
   }
   return CRP_OK;
+}
+
+// 3-D cloud about the bowl's focus (grid centre + ext_array_focus_dx along x):
+// cylinder along z (area-uniform radius), ball, or Gaussian per axis; the
+// same two Philox blocks per bubble as the 2-D seeding.
+crp_status crpo_seed_bubbles3(const crp_config* cfg, double* x, double* y, double* z, double* r0, double* n_b) {
+  if (!cfg || !x || !y || !z || !r0 || !n_b || cfg->ext_bubble_count <= 0 || cfg->ext_grid_z <= 0)
+    return CRP_ERR_INVALID;
+  const double two_pi = 2.0 * std::acos(-1.0);
+  const double fx = 0.5 * cfg->grid_lx + cfg->ext_array_focus_dx, fy = 0.5 * cfg->grid_ly,
+               fz = 0.5 * cfg->ext_grid_lz;
+  const double R = cfg->ext_cloud_r;
+  for (int32_t k = 0; k < cfg->ext_bubble_count; k++) {
+    uint32_t w[4], v[4];
+    philox4x32(cfg->ext_bubble_seed, (uint64_t)k, 0u, w);
+    philox4x32(cfg->ext_bubble_seed, (uint64_t)k, 1u, v);
+    double ox, oy, oz;
+    if (cfg->ext_cloud_shape == 1) {
+      const double rad = R * std::cbrt(open01(w[0]));
+      const double cth = 2.0 * open01(w[1]) - 1.0;
+      const double sth = std::sqrt(std::max(0.0, 1.0 - cth * cth));
+      const double ph = two_pi * open01(w[2]);
+      ox = rad * sth * std::cos(ph);
+      oy = rad * sth * std::sin(ph);
+      oz = rad * cth;
+    } else if (cfg->ext_cloud_shape == 2) {
+      const double m = std::sqrt(-2.0 * std::log(open01(w[0])));
+      ox = R * m * std::cos(two_pi * open01(w[1]));
+      oy = R * m * std::sin(two_pi * open01(w[1]));
+      oz = R * std::sqrt(-2.0 * std::log(open01(v[2]))) * std::cos(two_pi * open01(v[3]));
+    } else {
+      const double rr = R * std::sqrt(open01(w[0]));
+      const double ph = two_pi * open01(w[2]);
+      ox = rr * std::cos(ph);
+      oy = rr * std::sin(ph);
+      oz = (open01(w[1]) - 0.5) * cfg->ext_cloud_h;
+    }
+    const double gauss = std::sqrt(-2.0 * std::log(open01(v[0]))) * std::cos(two_pi * open01(v[1]));
+    x[k] = fx + ox;
+    y[k] = fy + oy;
+    z[k] = fz + oz;
+    r0[k] = cfg->bub_R0 * std::exp(cfg->ext_r0_sigma_ln * gauss);
+    n_b[k] = cfg->ext_n_b;
+  }
+  return CRP_OK;
+}
+
+void crpo_philox_block(uint64_t seed, uint64_t counter, uint32_t stream, uint32_t out[4]) {
+  philox4x32(seed, counter, stream, out);
 }
 
 }  // extern "C"

@@ -53,6 +53,16 @@ def oracle_lib():
             "crpo_config_parse_file": (ctypes.c_int32, [ctypes.c_char_p, P(crp.Config), ctypes.c_char_p,
                                                         ctypes.c_size_t]),
             "crpo_seed_bubbles": (ctypes.c_int32, [P(crp.Config), vp, vp, vp, vp]),
+            "crpo_seed_bubbles3": (ctypes.c_int32, [P(crp.Config), vp, vp, vp, vp, vp]),
+            "crpo3_create": (ctypes.c_int32, [P(crp.Config), P(crp.BubblesIn), P(vp)]),
+            "crpo3_step": (ctypes.c_int32, [vp, ctypes.c_int32]),
+            "crpo3_set_source_elements": (ctypes.c_int32, [vp, ctypes.c_int32, vp, vp]),
+            "crpo3_get_stats": (ctypes.c_int32, [vp, P(crp.Stats)]),
+            "crpo3_num_bubbles": (ctypes.c_int32, [vp]),
+            "crpo3_num_source_cells": (ctypes.c_int32, [vp]),
+            "crpo3_read_field": (ctypes.c_int32, [vp, ctypes.c_int32, vp]),
+            "crpo3_read_bubbles": (ctypes.c_int32, [vp, ctypes.c_int32, vp]),
+            "crpo3_destroy": (None, [vp]),
         }
         for n, (r, a) in sig.items():
             f = getattr(lib, n)
@@ -83,6 +93,74 @@ def oracle_seed_bubbles(cfg: crp.Config) -> crp.Bubbles:
     if st:
         raise crp.CrpError(st, "crpo_seed_bubbles")
     return crp.Bubbles(*arrs)
+
+
+def oracle_seed_bubbles3(cfg: crp.Config) -> crp.Bubbles:
+    """The seeded 3-D bubble population drawn by the oracle's own Philox."""
+    n = cfg.ext_bubble_count
+    x, y, z, r0, nb = (np.zeros(n) for _ in range(5))
+    st = oracle_lib().crpo_seed_bubbles3(ctypes.byref(cfg), *[_ptr(a) for a in (x, y, z, r0, nb)])
+    if st:
+        raise crp.CrpError(st, "crpo_seed_bubbles3")
+    return crp.Bubbles(x, y, r0, nb, z)
+
+
+class OracleSim3:
+    """The 3-D oracle (ext_grid_z > 0) with the surface of crp.Sim."""
+
+    def __init__(self, cfg: crp.Config, bubbles: crp.Bubbles | None = None, threads: int = 0):
+        self.lib = oracle_lib()
+        if threads:
+            self.lib.crpo_set_threads(threads)
+        self._keep = (cfg, bubbles)
+        h = vp()
+        bin_ = bubbles.as_c() if bubbles is not None else None
+        st = self.lib.crpo3_create(ctypes.byref(cfg), ctypes.byref(bin_) if bin_ is not None else None,
+                                   ctypes.byref(h))
+        if st:
+            raise crp.CrpError(st, "crpo3_create")
+        self.h = h
+        self.dims3 = crp.Dims3()
+        self.dims3.nx, self.dims3.ny, self.dims3.nz = cfg.grid_x + 2, cfg.grid_y + 2, cfg.ext_grid_z + 2
+        self.dims3.num_bubbles = self.lib.crpo3_num_bubbles(self.h)
+        self.dims3.source_cells = self.lib.crpo3_num_source_cells(self.h)
+
+    def step(self, n=1):
+        st = self.lib.crpo3_step(self.h, n)
+        if st:
+            raise crp.CrpError(st, "crpo3_step")
+
+    def set_source_elements(self, amp, phase):
+        a = np.ascontiguousarray(amp, dtype=np.float64)
+        p = np.ascontiguousarray(phase, dtype=np.float64)
+        st = self.lib.crpo3_set_source_elements(self.h, int(a.size), _ptr(a), _ptr(p))
+        if st:
+            raise crp.CrpError(st, "crpo3_set_source_elements")
+
+    def stats(self):
+        s = crp.Stats()
+        self.lib.crpo3_get_stats(self.h, ctypes.byref(s))
+        return s
+
+    def field(self, name):
+        out = np.empty(crp.field_shape3(self.dims3, name))
+        st = self.lib.crpo3_read_field(self.h, crp.FIELDS[name], _ptr(out))
+        assert st == 0, st
+        return out
+
+    def bubbles(self, name):
+        out = np.empty(self.dims3.num_bubbles)
+        st = self.lib.crpo3_read_bubbles(self.h, crp.BUBBLE_FIELDS[name], _ptr(out))
+        assert st == 0, st
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.crpo3_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 class OracleSim:
