@@ -61,18 +61,32 @@ import numpy as np  # noqa: E402
 # largest bubble radius leaves R0 by more than 1 %), measured with the FP64
 # path; the Picard loop of both workloads stops converging about 500 and 300
 # steps later (steps 2187 and 1219).
-DRIVEN_START = {"axisym_1024x2048": 1700, "axisym_256x512": 900, "sweep_64": 500}
+DRIVEN_START = {"axisym_1024x2048": 1700, "axisym_256x512": 900, "sweep_64": 500,
+                # 3-D: the burst from the bowl reaches the cloud's inner bubbles
+                "cart3d_384": 150, "cart3d_256": 200}
 # Timed windows end here (see the module docstring).
 QUIET_END = dict(DRIVEN_START)
-MAX_CHUNK = {"axisym_1024x2048": 100, "axisym_256x512": 100, "sweep_64": 25}
+MAX_CHUNK = {"axisym_1024x2048": 100, "axisym_256x512": 100, "sweep_64": 25, "cart3d_384": 25, "cart3d_256": 25}
 WORKLOADS = {
     "axisym_1024x2048": os.path.join(PKG, "configs", "axisym_1024x2048.conf"),
     "axisym_256x512": os.path.join(PKG, "configs", "axisym_256x512.conf"),
+    "cart3d_384": os.path.join(PKG, "configs", "cart3d_384.conf"),
+    "cart3d_256": os.path.join(PKG, "configs", "cart3d_256.conf"),
 }
 # Compulsory HBM traffic of the fused FDTD pass per cell: FP64
 # reads px, py, vx, vy, f_g, f_gn, f_gm and writes px, py, vx, vy, predicted f_g;
 # mixed stores each velocity/pressure value as two FP32 words and f_g as FP32.
 BYTES_PER_CELL = {"fp64": 96, "mixed": 80}
+# 3-D: vz and pz besides, each read and written.
+BYTES_PER_CELL_3D = {"fp64": 128, "mixed": 112}
+
+
+def is3d(cfg):
+    return cfg.ext_grid_z > 0
+
+
+def cell_count(cfg):
+    return cfg.grid_x * cfg.grid_y * (cfg.ext_grid_z if is3d(cfg) else 1)
 DTYPE = {"fp64": "f64", "mixed": "f32 fields + f32 compensation (f64 arithmetic), f32 void fraction, "
                                   "f32 thermal model while |R/R0-1| <= 1e-3, f64 RP"}
 
@@ -173,10 +187,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic(workload, precision):
-    """DRAM bytes (read + write) of one fdtd_strip launch from the committed ncu
-    summary of this workload and precision, or None when there is none."""
-    p = os.path.join(ROOT, "profiles", f"fdtd_strip_{workload}_{precision}.md")
+def grid_of(cfg):
+    return [cfg.grid_x, cfg.grid_y] + ([cfg.ext_grid_z] if is3d(cfg) else [])
+
+
+def traffic(kernel, workload, precision):
+    """DRAM bytes (read + write) of one launch of the FDTD kernel from the
+    committed ncu summary of this workload and precision, or None when there is none."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}_{precision}.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -191,7 +209,8 @@ def load_workload(name):
     import crp
 
     cfg = crp.parse_file(WORKLOADS[name])
-    bub = crp.seed_bubbles(cfg) if cfg.ext_bubble_count > 0 else None
+    seed = crp.seed_bubbles3 if is3d(cfg) else crp.seed_bubbles
+    bub = seed(cfg) if cfg.ext_bubble_count > 0 else None
     return cfg, bub
 
 
@@ -201,15 +220,22 @@ def load_workload_oracle(name):
     import _bind as B
 
     cfg = B.oracle_parse_file(WORKLOADS[name])
-    bub = B.oracle_seed_bubbles(cfg) if cfg.ext_bubble_count > 0 else None
+    seed = B.oracle_seed_bubbles3 if is3d(cfg) else B.oracle_seed_bubbles
+    bub = seed(cfg) if cfg.ext_bubble_count > 0 else None
     return cfg, bub
+
+
+def oracle_sim(cfg, bub, threads):
+    import _bind as B
+
+    return (B.OracleSim3 if is3d(cfg) else B.OracleSim)(cfg, bub, threads=threads)
 
 
 def cpu_baseline(cfg, bub, seconds, threads):
     """Oracle on the host cores: returns (cell-updates/s, steps, wall s, oracle sim)."""
     import _bind as B
 
-    o = B.OracleSim(cfg, bub, threads=threads)
+    o = oracle_sim(cfg, bub, threads)
     t0 = time.perf_counter()
     o.step(1)
     t1 = time.perf_counter()
@@ -217,7 +243,7 @@ def cpu_baseline(cfg, bub, seconds, threads):
     t2 = time.perf_counter()
     o.step(n)
     t3 = time.perf_counter()
-    rate = cfg.grid_x * cfg.grid_y * n / (t3 - t2)
+    rate = cell_count(cfg) * n / (t3 - t2)
     return rate, n + 1, t3 - t2, o
 
 
@@ -245,7 +271,7 @@ def reference_sample(args, world):
     else:
         cfg, bub = load_workload_oracle(args.workload)
     threads = os.cpu_count() or 1
-    o = B.OracleSim(cfg, bub, threads=threads)
+    o = oracle_sim(cfg, bub, threads)
     start = args.window[0]
     pre = max(0, start - args.warmup)
     o.step(pre) if pre else None
@@ -255,7 +281,8 @@ def reference_sample(args, world):
     for _ in range(args.steps):
         o.step(1)
     dt = time.perf_counter() - t0
-    cells = cfg.grid_x * cfg.grid_y
+    cells = cell_count(cfg)
+    nb_ref = o.dims3.num_bubbles if is3d(cfg) else o.dims.num_bubbles
     value = cells * args.steps / dt / 1e6
     t_start = int(o.stats().steps) - args.steps
     sample = (f"mixture steps {t_start}-{t_start + args.steps} of {args.workload} (untimed from t=0 to step "
@@ -264,9 +291,9 @@ def reference_sample(args, world):
         "impl": "reference", "metric": "Mcell-upd/s", "value": value, "unit": "Mcell-upd/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bubbles, Philox-4x32-10)",
-        "config": {"workload": args.workload, "grid": [cfg.grid_x, cfg.grid_y], "bubbles": o.dims.num_bubbles,
+        "config": {"workload": args.workload, "grid": grid_of(cfg), "bubbles": nb_ref,
                    "mixture_steps_per_step": 1, "window_start": t_start, "precision": "fp64"},
-        "bubble_steps_per_s": o.dims.num_bubbles * args.steps / dt,
+        "bubble_steps_per_s": nb_ref * args.steps / dt,
         "cpu_baseline": {"value": value, "unit": "Mcell-upd/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "Mcell-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -502,8 +529,12 @@ def e2e_run(cfg, bub, args, nb):
             t[...] = a
         return t
 
-    bub_pinned = crp.Bubbles(*(pinned(a) for a in (bub.x, bub.y, bub.r0, bub.n_b))) if bub is not None else None
-    p0_host = pinned((cfg.grid_y + 2, cfg.grid_x + 2))
+    bub_pinned = None
+    if bub is not None:
+        bub_pinned = crp.Bubbles(*(pinned(a) for a in (bub.x, bub.y, bub.r0, bub.n_b)),
+                                 pinned(bub.z) if bub.z is not None else None)
+    p0_shape = (cfg.ext_grid_z + 2, cfg.grid_y + 2, cfg.grid_x + 2) if is3d(cfg) else (cfg.grid_y + 2, cfg.grid_x + 2)
+    p0_host = pinned(p0_shape)
     r_host = pinned((nb,)) if nb > 0 else None
     n_steps = args.warmup + args.steps
     t_steps = t_read = 0.0
@@ -521,9 +552,9 @@ def e2e_run(cfg, bub, args, nb):
             t_steps += tb - ta
             t_read += time.perf_counter() - tb
         wall = time.perf_counter() - t0
-    h2d = 4 * 8 * nb
-    return {"value": cfg.grid_x * cfg.grid_y * n_steps * args.chunk / wall / 1e6, "unit": "Mcell-upd/s",
-            "h2d_bytes_per_step": h2d // n_steps, "d2h_bytes_per_step": 8 * (d.i1m * d.j1m + nb),
+    h2d = (5 if is3d(cfg) else 4) * 8 * nb
+    return {"value": cell_count(cfg) * n_steps * args.chunk / wall / 1e6, "unit": "Mcell-upd/s",
+            "h2d_bytes_per_step": h2d // n_steps, "d2h_bytes_per_step": 8 * (int(np.prod(p0_shape)) + nb),
             "seconds": {"create": t_create, "steps": t_steps, "read_back": t_read, "total": wall},
             "mixture_steps": [0, n_steps * args.chunk],
             "note": "wall clock: crp_create (seeded bubbles uploaded from pinned host memory) + the warm-up and "
@@ -548,14 +579,14 @@ def run_ours(args, rank, world, dist):
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
     cfg, bub = load_workload(args.workload)
-    cells = cfg.grid_x * cfg.grid_y
+    cells = cell_count(cfg)
     S = args.chunk
     mix_steps = args.steps * S
     base = {
         "metric": "Mcell-upd/s", "unit": "Mcell-upd/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "data": "synthetic (seeded bubbles, Philox-4x32-10)",
-        "config": {"workload": args.workload, "grid": [cfg.grid_x, cfg.grid_y],
+        "config": {"workload": args.workload, "grid": grid_of(cfg),
                    "mixture_steps_per_step": S, "window": list(args.window), "precision": args.primary,
                    "parallelism": f"replicas x{world}", "l2": "state > L2 (no flush needed)"},
     }
@@ -574,7 +605,7 @@ def run_ours(args, rank, world, dist):
                 r["sim"].close()
         return dict(base, value=None, error=f"{primary} path: {run['error']}", dtype=DTYPE[primary])
     sim = run["sim"]
-    nb = sim.dims.num_bubbles
+    nb = sim.dims3.num_bubbles if is3d(cfg) else sim.dims.num_bubbles
     ms, s0, s1 = run["ms"], run["s0"], run["s1"]
     value = job_rate(cells * mix_steps, world, ms) / 1e6
     # The other path's simulation stays open when a driven sample follows: the
@@ -593,14 +624,16 @@ def run_ours(args, rank, world, dist):
     prof = {k: (getattr(p1s, k) - getattr(p0s, k)) for k in ("ms_fdtd", "ms_rp", "ms_couple", "ms_other")}
 
     e2e = guarded(e2e_run, cfg, bub, args, nb) if rank == 0 and not args.no_e2e else None
-    adjoint = guarded(adjoint_cost, cfg) if rank == 0 and world == 1 and not args.no_adjoint else None
+    adjoint = (guarded(adjoint_cost, cfg) if rank == 0 and world == 1 and not args.no_adjoint and not is3d(cfg)
+               else None)
     driven = guarded(driven_sample, sim, args, cells, nb) if with_driven else None
     driven_rk45 = guarded(driven_rk45_sample, cfg, bub, args, cells, nb, sim) if with_driven else None
     focal = None
-    if with_driven and all("sim" in r for r in runs.values()) and len(runs) > 1:
+    if with_driven and all("sim" in r for r in runs.values()) and len(runs) > 1 and not is3d(cfg):
         focal = guarded(compare_at, {p: r["sim"] for p, r in runs.items()}, cfg)
     hbm, kind = peaks()
-    bpc = BYTES_PER_CELL[primary]
+    bpc = (BYTES_PER_CELL_3D if is3d(cfg) else BYTES_PER_CELL)[primary]
+    kernel = "fdtd3" if is3d(cfg) else "fdtd_strip"
     achieved = bpc * cells / (fdtd_ms * 1e-3) / 1e9 if n_fdtd else None
     result = None
     if rank == 0:
@@ -610,9 +643,9 @@ def run_ours(args, rank, world, dist):
             "bubble_steps_per_s": nb * mix_steps * world / (ms * 1e-3),
             "picard_iterations_per_step": (s1.picard_total - s0.picard_total) / mix_steps,
             "gpu_launches": int(s1.kernel_launches - s0.kernel_launches),
-            "roofline": {"kernel": "fdtd_strip", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "roofline": {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm if achieved else None, "peak_kind": kind,
-                         "traffic": traffic(args.workload, primary), "bytes_per_cell": bpc,
+                         "traffic": traffic(kernel, args.workload, primary), "bytes_per_cell": bpc,
                          "ms_per_launch": fdtd_ms if n_fdtd else None,
                          "launches": int(n_fdtd)},
             "kernel_ms_per_chunk": prof,

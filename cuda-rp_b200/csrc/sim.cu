@@ -3162,7 +3162,7 @@ crp_status crp_get_stats(const crp_sim* h, crp_stats* st) {
 
 crp_status crp_set_profiling(crp_sim* h, int32_t enable) {
   if (!h) return CRP_ERR_INVALID;
-  if (h->s3) return enable ? CRP_ERR_UNSUPPORTED : CRP_OK;
+  if (h->s3) return crp::sim3_set_profiling(h->s3, enable);
   DeviceScope dev(h);
   if (!dev.ok()) return CRP_ERR_CUDA;
   if (cudaStreamSynchronize(h->s.stream) != cudaSuccess) return CRP_ERR_CUDA;

@@ -753,6 +753,17 @@ struct Sim3Impl {
   int supp[3][6];
   crp_stats stats{};
   int64_t launches = 0;
+  // Profiling (crp_set_profiling): events around the FDTD launch of a step.
+  bool prof_on = false, prof_pending = false;
+  cudaEvent_t ev_f0 = nullptr, ev_f1 = nullptr;
+  crp_status set_profiling(bool on) {
+    if (on && !ev_f0) {
+      if (cudaEventCreate(&ev_f0) != cudaSuccess || cudaEventCreate(&ev_f1) != cudaSuccess)
+        return CRP_ERR_CUDA;
+    }
+    prof_on = on;
+    return CRP_OK;
+  }
 
   crp_status fail(crp_status s, const char* what, cudaError_t e = cudaSuccess) {
     err = what;
@@ -850,6 +861,8 @@ F32 Sim3Impl::view<F32>(void* p) const {
 }
 
 Sim3Impl::~Sim3Impl() {
+  if (ev_f0) cudaEventDestroy(ev_f0);
+  if (ev_f1) cudaEventDestroy(ev_f1);
   if (pool) cudaFree(pool);
   if (h_sc) cudaFreeHost(h_sc);
   if (own_stream && stream) cudaStreamDestroy(stream);
@@ -1199,9 +1212,15 @@ crp_status Sim3Impl::launch_fdtd() {
   const dim3 block(d3::kTX, d3::kTY);
   const dim3 grid((g.f.X + 1 + d3::kCX - 1) / d3::kCX + 1, (g.f.Y + 1 + d3::kCY - 1) / d3::kCY + 1,
                   (g.f.Z + d3::kZChunk - 1) / d3::kZChunk);
+  if (prof_on) C3(cudaEventRecord(ev_f0, stream));
   d3::fdtd3<P><<<grid, block, 0, stream>>>(g, a);
   C3(cudaGetLastError());
+  if (prof_on) {
+    C3(cudaEventRecord(ev_f1, stream));
+    prof_pending = true;
+  }
   launches++;
+  stats.fdtd_launches++;
   return CRP_OK;
 }
 
@@ -1288,6 +1307,12 @@ crp_status Sim3Impl::step_once() {
   }
   C3(cudaMemcpyAsync(h_sc, d_sc, sizeof(d3::Scalars3), cudaMemcpyDeviceToHost, stream));
   C3(cudaStreamSynchronize(stream));
+  if (prof_pending) {
+    float ms = 0.0f;
+    C3(cudaEventElapsedTime(&ms, ev_f0, ev_f1));
+    stats.ms_fdtd += ms;
+    prof_pending = false;
+  }
   double res = as_double(h_sc->residual) / g.P_inf;
   int loop = 0;
   int bnow[6] = {1, 1, 1, 0, 0, 0};
@@ -1471,6 +1496,7 @@ void sim3_dims(const Sim3Impl* s, crp_dims3* d) {
 }
 const crp_stats& sim3_stats(const Sim3Impl* s) { return s->stats; }
 const char* sim3_error(const Sim3Impl* s) { return s->err.c_str(); }
+crp_status sim3_set_profiling(Sim3Impl* s, int on) { return s->set_profiling(on != 0); }
 void* sim3_stream(Sim3Impl* s) { return (void*)s->stream; }
 int sim3_device(const Sim3Impl* s) { return s->device; }
 

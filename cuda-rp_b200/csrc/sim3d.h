@@ -18,6 +18,7 @@ crp_status sim3_set_elements(Sim3Impl* s, int n, const double* amp, const double
 void sim3_dims(const Sim3Impl* s, crp_dims3* d);
 const crp_stats& sim3_stats(const Sim3Impl* s);
 const char* sim3_error(const Sim3Impl* s);
+crp_status sim3_set_profiling(Sim3Impl* s, int on);
 void* sim3_stream(Sim3Impl* s);
 int sim3_device(const Sim3Impl* s);
 
