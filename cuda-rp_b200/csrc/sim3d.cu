@@ -112,13 +112,21 @@ struct Fdtd3Args {
 constexpr int kTX = 32, kTY = 8;   // threads per block
 constexpr int kCX = 30, kCY = 6;   // cells updated per block
 constexpr int kZChunk = 32;        // planes per block
+constexpr int kStages3 = 4;        // ring slots (planes) per thread
+constexpr int kFields3 = 9;        // pnx, pny, pnz, fgA, vx_old, vy_old, vz_old, fgB, fgC
+constexpr size_t kRing3Bytes = sizeof(double) * kStages3 * kFields3 * kTX * kTY;
 
+// Each thread's inputs of plane k0 - 1 + r are staged in ring slot r % kStages3
+// (dynamic shared memory, one 8-byte element per thread and field) by
+// asynchronous copies issued kStages3 - 2 planes ahead, so the loads of the
+// next planes are in flight while a plane is computed.
 template <typename P>
 __global__ void __launch_bounds__(kTX* kTY, 2) fdtd3(const __grid_constant__ Grid3 g, const Fdtd3Args<P> a) {
   using G = typename P::G;
   using S = typename P::S;
   using V = typename P::V;
   __shared__ double s_p0[2][kTY][kTX], s_rho[2][kTY][kTX], s_vy[2][kTY][kTX];
+  extern __shared__ __align__(16) double ring3[];  // [kStages3][kFields3][kTY * kTX]
   const Frame3& f = g.f;
   const int X = f.X, Y = f.Y, Z = f.Z;
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -128,8 +136,7 @@ __global__ void __launch_bounds__(kTX* kTY, 2) fdtd3(const __grid_constant__ Gri
   const int il = min(i, X + 1), jl = min(j, Y + 1);  // loads of threads past the window repeat the edge
   const double t_cur = a.tdev[1];
   const unsigned full = 0xffffffffu;
-  auto p0_at = [&](long q) { return a.pnx.get(q) + a.pny.get(q) + a.pnz.get(q); };
-  auto rho_at = [&](long q) { return a.rho_const ? g.rho_inf : (1.0 - a.fgA.get(q)) * g.rho_inf; };
+  auto rho_of = [&](double fa) { return a.rho_const ? g.rho_inf : (1.0 - fa) * g.rho_inf; };
   auto predict = [&](int ii, int jj, int kk) {
     const long q = f.idx(ii, jj, kk);
     const double v = G::stored(3.0 * a.fgA.get(q) - 3.0 * a.fgB.get(q) + a.fgC.get(q));
@@ -139,30 +146,70 @@ __global__ void __launch_bounds__(kTX* kTY, 2) fdtd3(const __grid_constant__ Gri
   const double vax = g.vax[il + 1], vbx = g.vbx[il + 1], vay = g.vay[jl + 1], vby = g.vby[jl + 1];
   const double pax = g.pax[il], pbx = g.pbx[il], pay = g.pay[jl], pby = g.pby[jl];
 
-  // The face below the first plane, vz(i, j, k0 - 1).
-  long q = f.idx(il, jl, k0 - 1);
-  double p0c = p0_at(q), rhoc = rho_at(q);
-  const double vz_old_b = a.vz_old.get(q);
-  q = f.idx(il, jl, k0);
-  double p0n = p0_at(q), rhon = rho_at(q);
-  double fb = face3(vz_old_b, p0c, p0n, face_q3(g, rhoc, rhon), g.rdz, g.vaz[k0], g.vbz[k0]);
-  if (k0 == 1 && upd) a.vz_new.put(f.idx(i, j, 0), fb);
-  double pxc = a.pnx.get(q), pyc = a.pny.get(q), pzc = a.pnz.get(q), fac = a.fgA.get(q);
-  p0c = p0n;
-  rhoc = rhon;
+  const int tid = ty * kTX + tx;
+  auto slot = [&](int r, int fld) -> double* { return &ring3[((r % kStages3) * kFields3 + fld) * (kTX * kTY) + tid]; };
+  const long qb = f.idx(il, jl, k0 - 1), plane = (long)(Y + 4) * f.pitch;
+  // Queue the copies of plane kk = k0 - 1 + r: pnx, pny, pnz, fgA for planes
+  // k0-1..k1+1, vz_old for k0-1..k1, vx_old, vy_old, fgB, fgC for k0..k1.  One
+  // commit group per plane, empty past the chunk, so that a fixed wait count
+  // always means "the next plane landed".
+  auto issue = [&](int r) {
+    const int kk = k0 - 1 + r;
+    if (kk <= k1 + 1) {
+      const long q = qb + r * plane;
+      a.pnx.stage(slot(r, 0), q);
+      a.pny.stage(slot(r, 1), q);
+      a.pnz.stage(slot(r, 2), q);
+      a.fgA.stage(slot(r, 3), q);
+      if (kk <= k1) {
+        a.vz_old.stage(slot(r, 6), q);
+        if (r >= 1) {
+          a.vx_old.stage(slot(r, 4), q);
+          a.vy_old.stage(slot(r, 5), q);
+          a.fgB.stage(slot(r, 7), q);
+          a.fgC.stage(slot(r, 8), q);
+        }
+      }
+    }
+    __pipeline_commit();
+  };
+#pragma unroll
+  for (int r = 0; r < kStages3; r++) issue(r);
+  __pipeline_wait_prior(kStages3 - 2);  // planes k0 - 1 and k0 have landed
+
+  // The face below the first plane, vz(i, j, k0 - 1), from planes k0 - 1 and k0.
+  double p0c, rhoc, fb, pxc, pyc, pzc, fac;
+  {
+    const double pxb = S::staged(slot(0, 0)), pyb = S::staged(slot(0, 1)), pzb = S::staged(slot(0, 2));
+    const double fab = G::staged(slot(0, 3)), vz_old_b = V::staged(slot(0, 6));
+    pxc = S::staged(slot(1, 0));
+    pyc = S::staged(slot(1, 1));
+    pzc = S::staged(slot(1, 2));
+    fac = G::staged(slot(1, 3));
+    const double p0b = pxb + pyb + pzb, rhob = rho_of(fab);
+    p0c = pxc + pyc + pzc;
+    rhoc = rho_of(fac);
+    fb = face3(vz_old_b, p0b, p0c, face_q3(g, rhob, rhoc), g.rdz, g.vaz[k0], g.vbz[k0]);
+    if (k0 == 1 && upd) a.vz_new.put(f.idx(i, j, 0), fb);
+  }
+  issue(kStages3);  // reuses the slot of plane k0 - 1
+  int src_e = g.src[qb + plane];  // source element + 1 of plane k0
   unsigned long long res = 0ull;
   int buf = 0;
 #pragma unroll 1
   for (int k = k0; k <= k1; k++) {
-    const long qc = f.idx(il, jl, k), qn = qc + (long)(Y + 4) * f.pitch;
+    const int r = k - k0 + 1;
+    __pipeline_wait_prior(kStages3 - 2);  // plane k + 1 has landed
     // Next plane.
-    const double pxn = a.pnx.get(qn), pyn = a.pny.get(qn), pzn = a.pnz.get(qn);
-    const double fan = a.fgA.get(qn);
-    p0n = pxn + pyn + pzn;
-    rhon = a.rho_const ? g.rho_inf : (1.0 - fan) * g.rho_inf;
+    const double pxn = S::staged(slot(r + 1, 0)), pyn = S::staged(slot(r + 1, 1)), pzn = S::staged(slot(r + 1, 2));
+    const double fan = G::staged(slot(r + 1, 3));
+    const double p0n = pxn + pyn + pzn, rhon = rho_of(fan);
     // This plane's old faces and void-fraction history.
-    const double vxo = a.vx_old.get(qc), vyo = a.vy_old.get(qc), vzo = a.vz_old.get(qc);
-    const double fgB = a.fgB.get(qc), fgC = a.fgC.get(qc);
+    const double vxo = V::staged(slot(r, 4)), vyo = V::staged(slot(r, 5)), vzo = V::staged(slot(r, 6));
+    const double fgB = G::staged(slot(r, 7)), fgC = G::staged(slot(r, 8));
+    issue(r + kStages3);  // reuses the slot of plane k
+    const int e = src_e;
+    if (k < k1) src_e = g.src[qb + (long)(r + 1) * plane];
     s_p0[buf][ty][tx] = p0c;
     s_rho[buf][ty][tx] = rhoc;
     __syncthreads();
@@ -201,7 +248,6 @@ __global__ void __launch_bounds__(kTX* kTY, 2) fdtd3(const __grid_constant__ Gri
       const double qy = pyc * pay - g.s3p * ((-fs + fn) * g.rdy + h) * pby;
       const double qz = pzc * g.paz[k] - g.s3p * ((-fb + ft) * g.rdz + h) * g.pbz[k];
       double p0new = qx + qy + qz;
-      const int e = g.src[o];
       if (e > 0) {
         p0new = element_pressure(g, e - 1, t_cur);
         a.px.put(o, p0new);
@@ -490,7 +536,6 @@ __global__ void __launch_bounds__(kRpThreads3) radius3(const __grid_constant__ G
                                                        const __grid_constant__ BubbleParams bp, Bub3 b,
                                                        const typename P::S px, const typename P::S py,
                                                        const typename P::S pz, Scalars3* sc) {
-  const double t_cur = sc->t[1];
   const double dt = g.dt;
   RpState s;
   RkState r;
@@ -706,12 +751,14 @@ struct P64 {
   using S = F64;
   using G = F64;
   using T = double;
+  static constexpr int kIndex = 0;
 };
 struct PMix {
   using V = F32c;
   using S = F32c;
   using G = F32;
   using T = float;
+  static constexpr int kIndex = 1;
 };
 
 }  // namespace d3
@@ -755,6 +802,7 @@ struct Sim3Impl {
   int64_t launches = 0;
   // Profiling (crp_set_profiling): events around the FDTD launch of a step.
   bool prof_on = false, prof_pending = false;
+  bool fdtd_smem_set[2] = {false, false};  // fdtd3's dynamic shared memory limit raised (FP64, mixed)
   cudaEvent_t ev_f0 = nullptr, ev_f1 = nullptr;
   crp_status set_profiling(bool on) {
     if (on && !ev_f0) {
@@ -1212,8 +1260,12 @@ crp_status Sim3Impl::launch_fdtd() {
   const dim3 block(d3::kTX, d3::kTY);
   const dim3 grid((g.f.X + 1 + d3::kCX - 1) / d3::kCX + 1, (g.f.Y + 1 + d3::kCY - 1) / d3::kCY + 1,
                   (g.f.Z + d3::kZChunk - 1) / d3::kZChunk);
+  if (!fdtd_smem_set[P::kIndex]) {
+    C3(cudaFuncSetAttribute(d3::fdtd3<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d3::kRing3Bytes));
+    fdtd_smem_set[P::kIndex] = true;
+  }
   if (prof_on) C3(cudaEventRecord(ev_f0, stream));
-  d3::fdtd3<P><<<grid, block, 0, stream>>>(g, a);
+  d3::fdtd3<P><<<grid, block, d3::kRing3Bytes, stream>>>(g, a);
   C3(cudaGetLastError());
   if (prof_on) {
     C3(cudaEventRecord(ev_f1, stream));
