@@ -49,7 +49,7 @@ class Config(ctypes.Structure):
         ("ext_graphs", c_int), ("ext_elements", c_int), ("ext_rp_scheme", c_int), ("ext_rp_tol", c_dbl),
         ("ext_grid_z", c_int), ("ext_grid_lz", c_dbl), ("ext_pml_z0", c_int), ("ext_pml_z1", c_int),
         ("ext_array_elements", c_int), ("ext_array_radius", c_dbl), ("ext_array_focus_dx", c_dbl),
-        ("ext_array_seed", ctypes.c_uint64), ("ext_array_phases", c_int),
+        ("ext_array_seed", ctypes.c_uint64), ("ext_array_phases", c_int), ("ext_rp_reuse", c_int),
     ]
 
 
@@ -69,7 +69,7 @@ class Stats(ctypes.Structure):
                 ("residual_last", c_dbl), ("kernel_launches", ctypes.c_int64), ("fdtd_launches", ctypes.c_int64),
                 ("rp_launches", ctypes.c_int64), ("couple_launches", ctypes.c_int64),
                 ("ms_fdtd", c_dbl), ("ms_rp", c_dbl), ("ms_couple", c_dbl), ("ms_other", c_dbl),
-                ("picard_stalls", ctypes.c_int64)]
+                ("picard_stalls", ctypes.c_int64), ("rp_reused", ctypes.c_int64)]
 
 
 PROGRESS = ctypes.CFUNCTYPE(None, ctypes.c_int64, c_dbl, ctypes.c_void_p)

@@ -170,6 +170,7 @@ const Key kKeys[] = {
     K("ext.array_focus_dx", kDouble, ext_array_focus_dx),
     K("ext.array_seed", kU64, ext_array_seed),
     K("ext.array_phases", kInt, ext_array_phases),
+    K("ext.rp_reuse", kBool, ext_rp_reuse),
 };
 #undef K
 
@@ -312,6 +313,7 @@ crp_status crp_config_defaults(crp_config* cfg) {
   cfg->ext_p_inf = 0.1e6;
   cfg->ext_precision = CRP_PREC_FP64;
   cfg->ext_picard_cap = 1000;
+  cfg->ext_rp_reuse = 1;
   cfg->ext_graphs = 0;
   cfg->ext_elements = 0;
   cfg->ext_rp_step_cap = 1000000;

@@ -83,6 +83,7 @@ struct BubbleParams {
   double dcx, dcy, dcz;  // delta_coef (src/bubble_CUDA.cu:1469-1471)
   long long step_cap;
   double rk_rtol;  // relative tolerance of the rk45 scheme
+  int reuse;       // ext.rp_reuse: keep a bubble's last solve of the step while its gathered pressure is unchanged
 };
 
 // Default relative tolerance of the rk45 scheme (ext.rp_tol = 0).

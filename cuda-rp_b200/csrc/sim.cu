@@ -714,10 +714,15 @@ __device__ __forceinline__ double gather_pl(const GridParams& g, const BubblePar
   return PLp;
 }
 
+// With `reuse` (a radius solve of this step has completed with the current
+// bins), a bubble whose gathered pressure has the bit pattern of the last
+// solve's is not set up: every input of its solve is unchanged, so its stored
+// results are what the solve would write; returns false for it.
 template <typename S>
-__device__ __forceinline__ void rp_begin(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
-                                         const S& px, const S& py, double t_cur, int n, RpState& s) {
+__device__ __forceinline__ bool rp_begin(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
+                                         const S& px, const S& py, double t_cur, int n, RpState& s, bool reuse) {
   const double PLp = gather_pl(g, bp, b, px, py, t_cur, n);
+  if (reuse && __double_as_longlong(PLp) == __double_as_longlong(b.PL_p[n])) return false;
   b.PL_p[n] = PLp;
   s.r = bubble_r0(bp, b.R0[n]);
   const double dt = g.dt;
@@ -737,6 +742,7 @@ __device__ __forceinline__ void rp_begin(const GridParams& g, const BubbleParams
   s.heat = 0.0;
   s.vis = 0.0;
   s.count = 0;
+  return true;
 }
 
 
@@ -800,6 +806,12 @@ constexpr int rp_min_blocks() {
   return sizeof(typename P::T) == sizeof(double) ? 6 : 5;
 }
 
+// Solves kept by rp_begin/rk_begin, summed per warp into one counter.
+__device__ __forceinline__ void count_kept(unsigned long long kept, unsigned long long* reused) {
+  for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+  if ((threadIdx.x & 31) == 0 && kept) atomicAdd(reused, kept);
+}
+
 template <typename P>
 __global__ void __launch_bounds__(kRpThreads, rp_min_blocks<P>()) bubble_rp(const __grid_constant__ GridParams g,
                                                         const __grid_constant__ BubbleParams bp, BubbleArrays b,
@@ -807,12 +819,15 @@ __global__ void __launch_bounds__(kRpThreads, rp_min_blocks<P>()) bubble_rp(cons
                                                         const double* __restrict__ tdev,
                                                         const int* __restrict__ order,
                                                         int* __restrict__ next, long long* __restrict__ substep_max,
-                                                        int* __restrict__ err) {
+                                                        int* __restrict__ err, const int* __restrict__ solved,
+                                                        unsigned long long* __restrict__ reused) {
   RpState s;
   const double t_cur = tdev[1];
+  const bool reuse = bp.reuse && *solved > 0;
   int n = -1;
   bool drained = false;
   long long worst = 0;
+  unsigned long long kept = 0;
   const int lane = threadIdx.x & 31;
   for (;;) {
     // Lanes without a bubble claim the next ones from the queue together:
@@ -827,13 +842,16 @@ __global__ void __launch_bounds__(kRpThreads, rp_min_blocks<P>()) bubble_rp(cons
         const int q = base + __popc(need & ((1u << lane) - 1u));
         if (q < b.n) {
           n = order[q];
-          rp_begin(g, bp, b, px, py, t_cur, n, s);
+          if (!rp_begin(g, bp, b, px, py, t_cur, n, s, reuse)) {
+            n = -1;
+            kept++;
+          }
         } else {
           drained = true;
         }
       }
     }
-    if (!__any_sync(0xffffffffu, n >= 0)) break;
+    if (!__any_sync(0xffffffffu, n >= 0 || !drained)) break;
     if (n >= 0) {
       if (s.remain > 0.0 && s.count < bp.step_cap) {
         rp_substep_full<typename P::T>(bp, s);
@@ -847,6 +865,7 @@ __global__ void __launch_bounds__(kRpThreads, rp_min_blocks<P>()) bubble_rp(cons
   }
   for (int o = 16; o > 0; o >>= 1) worst = max(worst, __shfl_xor_sync(0xffffffffu, worst, o));
   if ((threadIdx.x & 31) == 0 && worst > 0) atomicMax(substep_max, worst);
+  count_kept(kept, reused);
 }
 
 }  // namespace crp
@@ -856,10 +875,12 @@ namespace crp {
 // Set-up of one bubble's Dormand-Prince integration over the mixture step from
 // the state stored at the start of the step (as rp_begin): the pressure
 // gather, the liquid-pressure polynomial, R, R', PG and the last step size.
+// `reuse` as in rp_begin.
 template <typename S>
-__device__ __forceinline__ void rk_begin(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
-                                         const S& px, const S& py, double t_cur, int n, RkState& s) {
+__device__ __forceinline__ bool rk_begin(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
+                                         const S& px, const S& py, double t_cur, int n, RkState& s, bool reuse) {
   const double PLp = gather_pl(g, bp, b, px, py, t_cur, n);
+  if (reuse && __double_as_longlong(PLp) == __double_as_longlong(b.PL_p[n])) return false;
   b.PL_p[n] = PLp;
   s.r = bubble_r0(bp, b.R0[n]);
   const double dt = g.dt;
@@ -877,6 +898,7 @@ __device__ __forceinline__ void rk_begin(const GridParams& g, const BubbleParams
   s.PC1 = 0.5 * (PLp - PLm) / dt;
   s.PC2 = 0.5 * (PLp + PLm - 2.0 * PLn) / (dt * dt);
   s.K = 3.0 * (bp.gam - 1.0) * bp.K0 * bp.T0 * s.r.inv_PG0;
+  return true;
 }
 
 // Results of the integration in the arrays the reference scheme fills: the
@@ -912,12 +934,15 @@ __global__ void __launch_bounds__(kRpThreads, rk_min_blocks<P>()) bubble_rk45(co
                                                         const double* __restrict__ tdev,
                                                         const int* __restrict__ order,
                                                         int* __restrict__ next, long long* __restrict__ substep_max,
-                                                        int* __restrict__ err) {
+                                                        int* __restrict__ err, const int* __restrict__ solved,
+                                                        unsigned long long* __restrict__ reused) {
   RkState s;
   const double t_cur = tdev[1];
+  const bool reuse = bp.reuse && *solved > 0;
   int n = -1;
   bool drained = false;
   long long worst = 0;
+  unsigned long long kept = 0;
   const int lane = threadIdx.x & 31;
   for (;;) {
     const unsigned need = __ballot_sync(0xffffffffu, n < 0 && !drained);
@@ -930,13 +955,16 @@ __global__ void __launch_bounds__(kRpThreads, rk_min_blocks<P>()) bubble_rk45(co
         const int q = base + __popc(need & ((1u << lane) - 1u));
         if (q < b.n) {
           n = order[q];
-          rk_begin(g, bp, b, px, py, t_cur, n, s);
+          if (!rk_begin(g, bp, b, px, py, t_cur, n, s, reuse)) {
+            n = -1;
+            kept++;
+          }
         } else {
           drained = true;
         }
       }
     }
-    if (!__any_sync(0xffffffffu, n >= 0)) break;
+    if (!__any_sync(0xffffffffu, n >= 0 || !drained)) break;
     if (n >= 0) {
       if (s.t < s.tend && s.count < bp.step_cap) {
         if (!rk_attempt<typename P::T>(bp, s, bp.rk_rtol, g.c_inf)) s.count = bp.step_cap;
@@ -950,6 +978,7 @@ __global__ void __launch_bounds__(kRpThreads, rk_min_blocks<P>()) bubble_rk45(co
   }
   for (int o = 16; o > 0; o >>= 1) worst = max(worst, __shfl_xor_sync(0xffffffffu, worst, o));
   if ((threadIdx.x & 31) == 0 && worst > 0) atomicMax(substep_max, worst);
+  count_kept(kept, reused);
 }
 
 // Work order for the next radius solves: bubbles bucketed by the binary
@@ -1411,7 +1440,9 @@ struct Scalars {
   long long steps, picard_total, stalls;
   int picard_last, picard_max;
   int status;                   // crp_status of the first failure (0: none)
-  int loop;                     // Picard iterations of this step
+  int loop;                     // Picard iterations of this step completed (both paths; the radius
+                                // solves keep unchanged bubbles' results from the second on)
+  unsigned long long reused;    // radius solves kept (ext.rp_reuse), summed over the handle's life
   int stale;                    // bins need a rebuild
   int bnow[4], box[4];          // bubbles' cell box, coupling box
   int supp[3][4];               // void-fraction supports of the last three steps
@@ -1430,12 +1461,14 @@ __global__ void set_time(Scalars* s, double t_prev, double t, double carry) {
   s->residual = 0ull;
   s->moved = 0;
   for (int k = 0; k < 4; k++) s->bbox[k] = 0;
+  s->loop = 0;
 }
 // Start of a Picard iteration of a host-driven step: residual and work-queue
-// head cleared.
-__global__ void picard_begin(Scalars* s) {
+// head cleared; `done` iterations of this step have completed.
+__global__ void picard_begin(Scalars* s, int done) {
   s->residual = 0ull;
   s->next = 0;
+  s->loop = done;
 }
 // The first Picard iteration's start, launched with the radius solve before the
 // host has read the prediction's residual: the iteration runs when the host
@@ -1445,6 +1478,7 @@ __global__ void picard_begin(Scalars* s) {
 // bubble; the host then rebuilds the bins and starts the loop itself, or skips it.
 __global__ void picard_gate(Scalars* s, double P_inf, double tol, int n) {
   const double r = __longlong_as_double((long long)s->residual) / P_inf;
+  s->loop = 0;
   if (r > tol && s->moved == 0) {
     s->residual = 0ull;
     s->next = 0;
@@ -2005,6 +2039,7 @@ struct Sim {
     bp.dcz = d.dcz;
     bp.step_cap = cfg.ext_rp_step_cap;
     bp.rk_rtol = cfg.ext_rp_tol > 0.0 ? cfg.ext_rp_tol : kRk45DefaultTol;
+    bp.reuse = cfg.ext_rp_reuse ? 1 : 0;
   }
 
   void set_sigma_pointers() {
@@ -2171,7 +2206,7 @@ struct Sim {
         if (loop >= cfg.ext_picard_cap) return fail(CRP_ERR_PICARD, "Picard iteration cap reached");
         loop++;
         if (!(first_queued && loop == 1)) {
-          CRP_CUDA(launch(kClassOther, [&] { picard_begin<<<1, 1, 0, stream>>>(d_scalars); }));
+          CRP_CUDA(launch(kClassOther, [&] { picard_begin<<<1, 1, 0, stream>>>(d_scalars, loop - 1); }));
           CRP_CUDA(mixed ? launch_rp<PrecMixed>() : launch_rp<PrecFP64>());
         }
         CRP_CUDA(launch_couple(true));
@@ -2212,6 +2247,7 @@ struct Sim {
     stats.picard_max = std::max(stats.picard_max, loop);
     stats.residual_last = resimax;
     stats.rp_substeps_max = h_scalars->substep_max;
+    stats.rp_reused = (int64_t)h_scalars->reused;
     fill_launch_stats();
     return CRP_OK;
   }
@@ -2423,6 +2459,7 @@ struct Sim {
     h.steps = stats.steps;
     h.picard_total = stats.picard_total;
     h.stalls = stats.picard_stalls;
+    h.reused = (unsigned long long)stats.rp_reused;
     h.picard_last = stats.picard_last;
     h.picard_max = stats.picard_max;
     h.res_last = stats.residual_last;
@@ -2476,6 +2513,7 @@ struct Sim {
     stats.time = tstep;
     stats.picard_total = d.picard_total;
     stats.picard_stalls = d.stalls;
+    stats.rp_reused = (int64_t)d.reused;
     stats.picard_last = d.picard_last;
     stats.picard_max = d.picard_max;
     stats.residual_last = d.res_last;
@@ -2740,11 +2778,12 @@ struct Sim {
     if (cfg.ext_rp_scheme == CRP_RP_RK45)
       return launch(kClassRp, [&] {
         bubble_rk45<P><<<rp_grid, kRpThreads, 0, stream>>>(gp, bp, bub, pxc, pyc, d_scalars->t, lpt.order, d_next,
-                                                            d_substep_max, d_err);
+                                                            d_substep_max, d_err, &d_scalars->loop,
+                                                            &d_scalars->reused);
       });
     return launch(kClassRp, [&] {
       bubble_rp<P><<<rp_grid, kRpThreads, 0, stream>>>(gp, bp, bub, pxc, pyc, d_scalars->t, lpt.order, d_next,
-                                                        d_substep_max, d_err);
+                                                        d_substep_max, d_err, &d_scalars->loop, &d_scalars->reused);
     });
   }
 

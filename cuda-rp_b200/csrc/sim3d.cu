@@ -294,6 +294,7 @@ struct Scalars3 {
   int moved;
   int box[6];  // bubbles' ibn box: min x, y, z, max x, y, z
   double t[2];
+  unsigned long long reused;  // radius solves kept (ext.rp_reuse), summed over the handle's life
 };
 
 __global__ void set_time3(Scalars3* s, double t_prev, double t) {
@@ -530,18 +531,22 @@ constexpr int kRpThreads3 = 128;
 
 // The radius solves: the reference scheme's sub-steps (rp_substep_full) or
 // the rk45 scheme (rk_attempt), from the state stored at the step's start,
-// persistent lanes claiming bubbles from a queue.
+// persistent lanes claiming bubbles from a queue.  With `reuse` (a solve of
+// this step has completed), a bubble whose gathered pressure has the bit
+// pattern of the last solve's keeps that solve's results: every input of its
+// solve is unchanged.
 template <typename P, bool RK>
 __global__ void __launch_bounds__(kRpThreads3) radius3(const __grid_constant__ Grid3 g,
                                                        const __grid_constant__ BubbleParams bp, Bub3 b,
                                                        const typename P::S px, const typename P::S py,
-                                                       const typename P::S pz, Scalars3* sc) {
+                                                       const typename P::S pz, Scalars3* sc, int reuse) {
   const double dt = g.dt;
   RpState s;
   RkState r;
   int n = -1;
   bool drained = false;
   long long worst = 0;
+  unsigned long long kept = 0;
   const int lane = threadIdx.x & 31;
   for (;;) {
     const unsigned need = __ballot_sync(0xffffffffu, n < 0 && !drained);
@@ -552,9 +557,13 @@ __global__ void __launch_bounds__(kRpThreads3) radius3(const __grid_constant__ G
       base = __shfl_sync(0xffffffffu, base, leader);
       if (need & (1u << lane)) {
         const int q = base + __popc(need & ((1u << lane) - 1u));
-        if (q < b.n) {
+        const double PLp = q < b.n ? gather_pl3(g, bp, b, px, py, pz, q) : 0.0;
+        if (q >= b.n) {
+          drained = true;
+        } else if (reuse && __double_as_longlong(PLp) == __double_as_longlong(b.PL_p[q])) {
+          kept++;
+        } else {
           n = q;
-          const double PLp = gather_pl3(g, bp, b, px, py, pz, n);
           b.PL_p[n] = PLp;
           const double PLn = b.PL_n[n], PLm = b.PL_m[n];
           const double PC0 = PLn + bp.PL0, PC1 = 0.5 * (PLp - PLm) / dt,
@@ -592,12 +601,10 @@ __global__ void __launch_bounds__(kRpThreads3) radius3(const __grid_constant__ G
             s.vis = 0.0;
             s.count = 0;
           }
-        } else {
-          drained = true;
         }
       }
     }
-    if (!__any_sync(0xffffffffu, n >= 0)) break;
+    if (!__any_sync(0xffffffffu, n >= 0 || !drained)) break;
     if (n < 0) continue;
     if (RK) {
       if (r.t < r.tend && r.count < bp.step_cap) {
@@ -636,6 +643,8 @@ __global__ void __launch_bounds__(kRpThreads3) radius3(const __grid_constant__ G
   }
   for (int o = 16; o > 0; o >>= 1) worst = max(worst, __shfl_xor_sync(0xffffffffu, worst, o));
   if (lane == 0 && worst > 0) atomicMax(&sc->substep_max, worst);
+  for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+  if (lane == 0 && kept) atomicAdd(&sc->reused, kept);
 }
 
 template <typename P>
@@ -879,7 +888,7 @@ struct Sim3Impl {
   template <typename P>
   crp_status launch_move();
   template <typename P>
-  crp_status launch_radius();
+  crp_status launch_radius(int done);
   template <typename P>
   crp_status launch_couple(bool gather, bool pressure, const int box[6]);
   crp_status build_bins();
@@ -1134,6 +1143,7 @@ crp_status Sim3Impl::create(const crp_config& c, const crp_bubbles_in* bin, void
   bp.dcz = 2.0 * pi / 2.0 * g.rdy;
   bp.step_cap = c.ext_rp_step_cap;
   bp.rk_rtol = c.ext_rp_tol > 0.0 ? c.ext_rp_tol : kRk45DefaultTol;
+  bp.reuse = c.ext_rp_reuse ? 1 : 0;
   for (int q = 0; q < 3; q++) supp[q][0] = supp[q][1] = supp[q][2] = 1, supp[q][3] = supp[q][4] = supp[q][5] = 0;
   if (nb > 0) {
     std::vector<double> zeros(nb, 0.0), dt0(nb, bp.dt0), pg0(nb);
@@ -1287,15 +1297,16 @@ crp_status Sim3Impl::launch_move() {
 }
 
 template <typename P>
-crp_status Sim3Impl::launch_radius() {
+crp_status Sim3Impl::launch_radius(int done) {
   using S = typename P::S;
+  const int reuse = bp.reuse && done > 0 ? 1 : 0;
   C3(cudaMemsetAsync(&d_sc->next, 0, sizeof(int), stream));
   if (cfg.ext_rp_scheme == CRP_RP_RK45)
     d3::radius3<P, true><<<rp_grid, d3::kRpThreads3, 0, stream>>>(g, bp, bub, view<S>(px[cur_p]), view<S>(py[cur_p]),
-                                                                   view<S>(pz[cur_p]), d_sc);
+                                                                   view<S>(pz[cur_p]), d_sc, reuse);
   else
     d3::radius3<P, false><<<rp_grid, d3::kRpThreads3, 0, stream>>>(g, bp, bub, view<S>(px[cur_p]),
-                                                                    view<S>(py[cur_p]), view<S>(pz[cur_p]), d_sc);
+                                                                    view<S>(py[cur_p]), view<S>(pz[cur_p]), d_sc, reuse);
   C3(cudaGetLastError());
   launches++;
   return CRP_OK;
@@ -1385,7 +1396,7 @@ crp_status Sim3Impl::step_once() {
       if (loop >= cfg.ext_picard_cap) return fail(CRP_ERR_PICARD, "Picard iteration cap reached");
       loop++;
       C3(cudaMemsetAsync(&d_sc->residual, 0, sizeof(unsigned long long), stream));
-      st = mixed ? launch_radius<d3::PMix>() : launch_radius<d3::P64>();
+      st = mixed ? launch_radius<d3::PMix>(loop - 1) : launch_radius<d3::P64>(loop - 1);
       if (st != CRP_OK) return st;
       st = mixed ? launch_couple<d3::PMix>(true, true, box) : launch_couple<d3::P64>(true, true, box);
       if (st != CRP_OK) return st;
@@ -1418,6 +1429,7 @@ crp_status Sim3Impl::step_once() {
   stats.picard_max = std::max(stats.picard_max, loop);
   stats.residual_last = res;
   stats.rp_substeps_max = h_sc->substep_max;
+  stats.rp_reused = (int64_t)h_sc->reused;
   stats.kernel_launches = launches;
   return CRP_OK;
 }

@@ -143,6 +143,11 @@ typedef struct crp_config {
   double ext_array_focus_dx;   /* [m] focus offset from the centre along x (the bowl's phases focus there) */
   uint64_t ext_array_seed;     /* seed of the phases when ext_array_phases = 1 */
   int32_t ext_array_phases;    /* 0: focusing phases omega |x_e - focus| / c; 1: seeded, uniform in [0, 2 pi) */
+  int32_t ext_rp_reuse;        /* 1 (default): a Picard iteration after a step's first re-solves only
+                                  the bubbles whose gathered liquid pressure changed (bit pattern) since
+                                  the last solve and keeps the others' results, which are bit for bit
+                                  what a re-solve returns; 0: every bubble every iteration, as the
+                                  reference (src/bubble_CUDA.cu:239-276) */
 } crp_config;
 
 /* Integrator of the bubble radius and gas pressure over one mixture step. */
@@ -223,6 +228,10 @@ typedef struct crp_stats {
    * stopped falling (less than halved by an iteration, from the third on)
    * while below CRP_MIXED_STALL_RESIDUAL.  Always 0 in the FP64 path. */
   int64_t picard_stalls;
+  /* Bubble radius solves that a Picard iteration kept from the previous one
+   * (ext.rp_reuse: the bubble's gathered liquid pressure was unchanged),
+   * summed over all steps.  The oracle re-solves every bubble (always 0). */
+  int64_t rp_reused;
 } crp_stats;
 
 /* Residual (max |dp0| / P_inf) below which the mixed path accepts a stagnating

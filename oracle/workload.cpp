@@ -86,7 +86,7 @@ const std::map<std::string, Slot>& registry() {
       S("ext.pml_z0", T::Bool, ext_pml_z0), S("ext.pml_z1", T::Bool, ext_pml_z1),
       S("ext.array_elements", T::I32, ext_array_elements), S("ext.array_radius", T::F64, ext_array_radius),
       S("ext.array_focus_dx", T::F64, ext_array_focus_dx), S("ext.array_seed", T::U64, ext_array_seed),
-      S("ext.array_phases", T::I32, ext_array_phases),
+      S("ext.array_phases", T::I32, ext_array_phases), S("ext.rp_reuse", T::Bool, ext_rp_reuse),
   };
 #undef S
   return m;
@@ -215,6 +215,7 @@ crp_status crpo_config_defaults(crp_config* cfg) {
   cfg->ext_c_inf = 1500.0;
   cfg->ext_p_inf = 1.0e5;
   cfg->ext_picard_cap = 1000;
+  cfg->ext_rp_reuse = 1;
   cfg->ext_rp_step_cap = 1000000;
   cfg->ext_n_b = 1.0;
   return CRP_OK;
