@@ -772,6 +772,29 @@ def run_sweep(args, rank, world):
         batch_done = [0] * n
         run(args.warmup * args.chunk)
         batch_done = [s.stats().steps for s in batch.sims]
+        # Per-simulation error against the FP64 oracle after the warm-up steps,
+        # on four simulations (smallest and largest grid, most bubbles,
+        # strongest drive; oracle seeding and parser, all host cores).
+        oracle_err = {}
+        if not args.no_cpu_baseline:
+            import _bind as B
+
+            ocfgs, _ = sweep_configs(B.oracle_parse_file)
+            picks = sorted({min(range(n), key=lambda k: cfgs[k].grid_x), max(range(n), key=lambda k: cfgs[k].grid_x),
+                            max(range(n), key=lambda k: cfgs[k].ext_bubble_count),
+                            max(range(n), key=lambda k: cfgs[k].tr_amp)})
+            for k in picks:
+                if k in failed:
+                    continue
+                o = oracle_sim(ocfgs[k], B.oracle_seed_bubbles(ocfgs[k]), os.cpu_count() or 1)
+                o.step(batch_done[k])
+                oracle_err[str(k)] = {"grid": [cfgs[k].grid_x, cfgs[k].grid_y], "bubbles": cfgs[k].ext_bubble_count,
+                                      "at_step": batch_done[k], **state_error(batch.sims[k], o)}
+        # The autotuner (untimed): candidate settings timed on the batch itself,
+        # every simulation's state restored after each trial.
+        t0 = time.perf_counter()
+        best, tried = batch.tune(trial_steps=10)
+        tune_s = time.perf_counter() - t0
         s0 = [s.stats() for s in batch.sims]
         e0 = [torch.cuda.Event(enable_timing=True) for _ in range(n)]
         e1 = [torch.cuda.Event(enable_timing=True) for _ in range(n)]
@@ -800,10 +823,13 @@ def run_sweep(args, rank, world):
                        "cells": int(sum(c.grid_x * c.grid_y for c in cfgs)),
                        "bubbles": int(sum(sim.dims.num_bubbles for sim in batch.sims)),
                        "mixture_steps_per_step": args.chunk, "window": list(args.window),
-                       "nominal_steps": [min(nominal), max(nominal)], "parallelism": "concurrent streams x64",
+                       "nominal_steps": [min(nominal), max(nominal)],
+                       "parallelism": f"concurrent streams x{n}, {best.as_dict()['mode']} (autotuned)",
                        "l2": "state > L2 (no flush needed)"},
             "bubble_steps_per_s": bub_steps / (ms * 1e-3), "gpu_launches": int(launches),
             "failed_simulations": failed, "wall_s": wall, "clocks": clk.summary(),
+            "tuning": {"chosen": best.as_dict(), "tried": [t.as_dict() for t in tried], "seconds": tune_s},
+            "oracle_error": oracle_err,
         }
 
 

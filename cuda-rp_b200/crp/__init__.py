@@ -63,6 +63,23 @@ class Dims3(ctypes.Structure):
                 ("dz", c_dbl), ("dt", c_dbl), ("source_cells", c_int)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("fdtd_rows", c_int), ("rp_blocks", c_int), ("rp_blocks_max", c_int)]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("mode", c_int), ("threads", c_int), ("blocking", c_int), ("fdtd_rows", c_int),
+                ("rp_bubbles_per_lane", c_int), ("ms_per_step", c_dbl)]
+
+    def as_dict(self) -> dict:
+        return {"mode": ["threads", "graphs"][self.mode], "threads": self.threads, "blocking": self.blocking,
+                "fdtd_rows": self.fdtd_rows, "rp_bubbles_per_lane": self.rp_bubbles_per_lane,
+                "ms_per_step": self.ms_per_step}
+
+
+BATCH_THREADS, BATCH_GRAPHS = 0, 1
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_int64), ("time", c_dbl), ("picard_total", ctypes.c_int64),
                 ("picard_last", c_int), ("picard_max", c_int), ("rp_substeps_max", ctypes.c_int64),
@@ -178,6 +195,15 @@ def load(path: str | None = None) -> ctypes.CDLL:
         "crp_batch_count": (c_int, [vp]),
         "crp_batch_sim": (vp, [vp, c_int]),
         "crp_batch_destroy": (None, [vp]),
+        "crp_state_bytes": (ctypes.c_size_t, [vp]),
+        "crp_save_state": (c_int, [vp, P(vp)]),
+        "crp_load_state": (c_int, [vp, vp]),
+        "crp_state_free": (None, [vp]),
+        "crp_get_tuning": (c_int, [vp, P(Tuning)]),
+        "crp_set_tuning": (c_int, [vp, P(Tuning)]),
+        "crp_batch_get_tuning": (c_int, [vp, P(BatchTuning)]),
+        "crp_batch_set_tuning": (c_int, [vp, P(BatchTuning)]),
+        "crp_batch_tune": (c_int, [vp, c_int, P(BatchTuning), P(BatchTuning), c_int, P(c_int)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)
@@ -278,6 +304,26 @@ class Sim:
         self._check(self.lib.crp_get_stats(self.h, ctypes.byref(s)))
         return s
 
+    def save_state(self, into: "State | None" = None) -> "State":
+        """Snapshot of the whole simulation state (crp_save_state); `into`, a
+        snapshot of this simulation, is overwritten instead of allocating."""
+        st = into if into is not None else State(self.lib)
+        self._check(self.lib.crp_save_state(self.h, ctypes.byref(st.h)))
+        return st
+
+    def load_state(self, st: "State"):
+        self._check(self.lib.crp_load_state(self.h, st.h))
+
+    @property
+    def tuning(self) -> Tuning:
+        t = Tuning()
+        self._check(self.lib.crp_get_tuning(self.h, ctypes.byref(t)))
+        return t
+
+    @tuning.setter
+    def tuning(self, t: Tuning):
+        self._check(self.lib.crp_set_tuning(self.h, ctypes.byref(t)))
+
     def field(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
         """Dense copy of a field; into `out` (float64, C-contiguous, the field's
         shape) when given, e.g. a pinned host buffer."""
@@ -369,6 +415,22 @@ class Sim:
         self.close()
 
 
+class State:
+    """A snapshot taken by Sim.save_state (device memory, freed with the object)."""
+
+    def __init__(self, lib):
+        self.lib = lib
+        self.h = ctypes.c_void_p()
+
+    def free(self):
+        if getattr(self, "h", None):
+            self.lib.crp_state_free(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        self.free()
+
+
 class _BatchSim(Sim):
     """A simulation owned by a Batch (not destroyed on its own)."""
 
@@ -410,6 +472,26 @@ class Batch:
             bad = [k for k, v in enumerate(per) if v]
             raise CrpError(st, f"simulations {bad} failed: {self.lib.crp_status_string(st).decode()}")
         return per
+
+    @property
+    def tuning(self) -> BatchTuning:
+        t = BatchTuning()
+        self._check(self.lib.crp_batch_get_tuning(self.h, ctypes.byref(t)))
+        return t
+
+    @tuning.setter
+    def tuning(self, t: BatchTuning):
+        self._check(self.lib.crp_batch_set_tuning(self.h, ctypes.byref(t)))
+
+    def tune(self, trial_steps: int = 10) -> tuple[BatchTuning, list[BatchTuning]]:
+        """crp_batch_tune: the fastest setting (applied) and every setting timed."""
+        best, tried, n = BatchTuning(), (BatchTuning * 16)(), c_int()
+        self._check(self.lib.crp_batch_tune(self.h, trial_steps, ctypes.byref(best), tried, 16, ctypes.byref(n)))
+        return best, [tried[k] for k in range(min(n.value, 16))]
+
+    def _check(self, st: int):
+        if st:
+            raise CrpError(st, self.lib.crp_status_string(st).decode())
 
     def close(self):
         if getattr(self, "h", None):

@@ -60,4 +60,15 @@ struct MinMax {
 };
 MinMax& sim_minmax(crp_sim* h);
 
+// Graph-queued steps for crp_batch (sim.cu): whether the next step of a 2-D
+// simulation may run as a graph, the batch's override of ext.graphs, and the
+// two halves of a run of graph steps (queue on the simulation's stream; wait
+// and take the device's step state).
+bool sim_graph_ready(const crp_sim* h);
+void sim_allow_graphs(crp_sim* h, bool on);
+// Host waits inside a 2-D step: spin (default) or block on an event.
+crp_status sim_blocking_waits(crp_sim* h, bool on);
+crp_status sim_graphs_enqueue(crp_sim* h, int n);
+crp_status sim_graphs_finish(crp_sim* h);
+
 }  // namespace crp

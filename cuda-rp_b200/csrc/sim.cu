@@ -1676,6 +1676,8 @@ struct Sim {
   int* d_moved = nullptr;
   Scalars* h_scalars = nullptr;  // pinned
   cudaEvent_t ev_scalars = nullptr;  // the prediction's scalars have reached h_scalars
+  cudaEvent_t ev_block = nullptr;    // the same, for blocking waits (set_blocking_waits)
+  bool blocking_waits = false;
   double picard_tol = 1.0e-7f;
   // Cell boxes {i0, j0, i1, j1} (empty when i0 > i1).  supp[q] bounds the
   // nonzero void fraction of step n-1-q; the coupling kernel updates only the
@@ -1718,7 +1720,18 @@ struct Sim {
     int* order;   // n
   } lpt{};
   int rp_grid = 1;
+  int rp_grid_full = 1;       // the radius kernel's grid at one lane per bubble, up to the occupancy limit
   int couple_graph_grid = 1;  // blocks of the graph steps' coupling launch (striding over the box's tiles)
+  // Launch tuning (crp_set_tuning): rows per FDTD strip chunk and the radius
+  // kernel's block count (0: rp_grid_full).
+  int strip_rows = kStripRows;
+  int rp_blocks_req = 0;
+  // Graph steps queued by graphs_enqueue and not yet completed by graphs_finish.
+  struct Pending {
+    bool on = false;
+    int64_t steps0 = 0;
+    int cur_v = 0, cur_p = 0, fg_a = 0, fg_b = 1, fg_c = 2;
+  } pend;
 
   MinMax mm;       // running min/max of written rawdata values
   int cur_v = 0;   // velocity buffer holding the latest velocities
@@ -1869,7 +1882,8 @@ struct Sim {
       else
         CRP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
             &per_sm, rk ? bubble_rk45<PrecFP64> : bubble_rp<PrecFP64>, kRpThreads, 0));
-      rp_grid = std::max(1, std::min(sms * std::max(per_sm, 1), (hs.nb + kRpThreads - 1) / kRpThreads));
+      rp_grid_full = std::max(1, std::min(sms * std::max(per_sm, 1), (hs.nb + kRpThreads - 1) / kRpThreads));
+      rp_grid = rp_grid_full;
       couple_graph_grid = 4 * sms;
     }
     // PML profiles and metrics.
@@ -2139,8 +2153,22 @@ struct Sim {
 
   crp_status read_scalars() {
     CRP_CUDA(cudaMemcpyAsync(h_scalars, d_scalars, sizeof(Scalars), cudaMemcpyDeviceToHost, stream));
-    CRP_CUDA(cudaStreamSynchronize(stream));
+    CRP_CUDA(wait_stream());
     prof.resolve();
+    return CRP_OK;
+  }
+
+  // The host's waits inside a step: spinning (the default: the shortest
+  // wake-up), or blocking on an event that yields the CPU core (crp_batch with
+  // more host threads than cores).
+  cudaError_t wait_stream() {
+    if (!blocking_waits) return cudaStreamSynchronize(stream);
+    cudaError_t e = cudaEventRecord(ev_block, stream);
+    return e != cudaSuccess ? e : cudaEventSynchronize(ev_block);
+  }
+  crp_status set_blocking_waits(bool on) {
+    if (on && !ev_block) CRP_CUDA(cudaEventCreateWithFlags(&ev_block, cudaEventDisableTiming | cudaEventBlockingSync));
+    blocking_waits = on;
     return CRP_OK;
   }
 
@@ -2176,14 +2204,15 @@ struct Sim {
     const bool ahead = hs.nb > 0 && !bins_stale && cfg.ext_picard_cap > 0;
     CRP_CUDA(cudaMemcpyAsync(h_scalars, d_scalars, sizeof(Scalars), cudaMemcpyDeviceToHost, stream));
     if (ahead) {
-      CRP_CUDA(cudaEventRecord(ev_scalars, stream));
+      cudaEvent_t ev = blocking_waits ? ev_block : ev_scalars;
+      CRP_CUDA(cudaEventRecord(ev, stream));
       if (substep_prev > kLptMinSubsteps) CRP_CUDA(build_order());
       CRP_CUDA(launch(kClassOther,
                       [&] { picard_gate<<<1, 1, 0, stream>>>(d_scalars, gp.P_inf, picard_tol, hs.nb); }));
       CRP_CUDA(mixed ? launch_rp<PrecMixed>() : launch_rp<PrecFP64>());
-      CRP_CUDA(cudaEventSynchronize(ev_scalars));
+      CRP_CUDA(cudaEventSynchronize(ev));
     } else {
-      CRP_CUDA(cudaStreamSynchronize(stream));
+      CRP_CUDA(wait_stream());
       prof.resolve();
     }
     crp_status st = CRP_OK;
@@ -2475,6 +2504,20 @@ struct Sim {
 
   // n steps through the graph path; one read-back at the end.
   crp_status step_graphs(int n) {
+    const crp_status st = graphs_enqueue(n);
+    if (st != CRP_OK) return st;
+    return graphs_finish();
+  }
+
+  // The next step may run as a graph (crp_step runs the others from the host).
+  bool graph_ready() const {
+    return !(stats.steps == 0 || prof.on || !graphs_on || hs.nb == 0 || debug_picard || temperature_on);
+  }
+
+  // Queues n graph steps and the read-back of the device scalars on the
+  // simulation's stream without waiting for them; graphs_finish completes them.
+  crp_status graphs_enqueue(int n) {
+    if (pend.on) return fail(CRP_ERR_INVALID, "graph steps already queued");
     if (!h_push) CRP_CUDA(cudaMallocHost(&h_push, sizeof(Scalars)));
     for (int k = 0; k < 6; k++)
       if (!step_exec[k]) {
@@ -2495,15 +2538,24 @@ struct Sim {
         cur_v = sv, cur_p = sp, fg_a = sa, fg_b = sb, fg_c = sc;
         break;
       }
-    const int64_t steps0 = stats.steps;
-    const int sv = cur_v, sp = cur_p, sa = fg_a, sb = fg_b, sc = fg_c;
+    pend.steps0 = stats.steps;
+    pend.cur_v = cur_v, pend.cur_p = cur_p, pend.fg_a = fg_a, pend.fg_b = fg_b, pend.fg_c = fg_c;
     CRP_CUDA(push_ctl());
     for (int k = 0; k < n; k++) {
       CRP_CUDA(cudaGraphLaunch(step_exec[phase()], stream));
       rotate_once();
     }
     CRP_CUDA(cudaMemcpyAsync(h_scalars, d_scalars, sizeof(Scalars), cudaMemcpyDeviceToHost, stream));
+    pend.on = true;
+    return CRP_OK;
+  }
+
+  crp_status graphs_finish() {
+    if (!pend.on) return CRP_OK;
+    pend.on = false;
     CRP_CUDA(cudaStreamSynchronize(stream));
+    const int64_t steps0 = pend.steps0;
+    const int sv = pend.cur_v, sp = pend.cur_p, sa = pend.fg_a, sb = pend.fg_b, sc = pend.fg_c;
     const Scalars& d = *h_scalars;
     t_prev = d.t[0];
     tstep = d.t[1];
@@ -2538,6 +2590,8 @@ struct Sim {
   // crp_step: the first step (initial mixture density), profiled steps and
   // simulations without bubbles run from the host; the rest as graphs.
   crp_status step_n(int n) {
+    const crp_status pst = graphs_finish();
+    if (pst != CRP_OK) return pst;
     int k = 0;
     while (k < n && (stats.steps == 0 || prof.on || !graphs_on || hs.nb == 0 || debug_picard || temperature_on)) {
       const crp_status st = step_once();
@@ -2625,10 +2679,15 @@ struct Sim {
       int* perr = &d_scalars->pipe_err;
       e = launch(kClassFdtd, [&] { fdtd_tile<P><<<grid, block, smem, stream>>>(gp, fa, m, ntx, nt, perr); });
     } else {
-      const int strips = (gp.f.X + kStripCells - 1) / kStripCells;
+      const int strips = (gp.f.X + kStripCells - 1) / kStripCells, rows = strip_rows;
       dim3 block(32, kStripWarps);
-      dim3 grid((strips + kStripWarps - 1) / kStripWarps, (gp.f.Y + kStripRows - 1) / kStripRows);
-      e = launch(kClassFdtd, [&] { fdtd_strip<P><<<grid, block, 0, stream>>>(gp, fa); });
+      dim3 grid((strips + kStripWarps - 1) / kStripWarps, (gp.f.Y + rows - 1) / rows);
+      if (rows == 4)
+        e = launch(kClassFdtd, [&] { fdtd_strip<P, kStripStages, 4><<<grid, block, 0, stream>>>(gp, fa); });
+      else if (rows == 16)
+        e = launch(kClassFdtd, [&] { fdtd_strip<P, kStripStages, 16><<<grid, block, 0, stream>>>(gp, fa); });
+      else
+        e = launch(kClassFdtd, [&] { fdtd_strip<P><<<grid, block, 0, stream>>>(gp, fa); });
     }
     if (e != cudaSuccess) return e;
     if (hs.nb > 0) return cudaSuccess;  // bubble_move, which follows, writes the ghost cells
@@ -2841,16 +2900,110 @@ struct Sim {
     return CRP_OK;
   }
 
-  ~Sim() {
+  // Executable graphs hold the launch shapes: rebuilt on next use after a change.
+  void drop_graphs() {
     for (int k = 0; k < 6; k++) {
       if (step_exec[k]) cudaGraphExecDestroy(step_exec[k]);
       if (step_graph[k]) cudaGraphDestroy(step_graph[k]);
+      step_exec[k] = nullptr;
+      step_graph[k] = nullptr;
     }
+  }
+
+  crp_status set_tuning(const crp_tuning& t) {
+    if (t.fdtd_rows != 4 && t.fdtd_rows != 8 && t.fdtd_rows != 16)
+      return fail(CRP_ERR_INVALID, "tuning: fdtd_rows must be 4, 8 or 16");
+    if (t.rp_blocks < 0) return fail(CRP_ERR_INVALID, "tuning: rp_blocks must be >= 0");
+    const int grid = t.rp_blocks > 0 ? std::min(t.rp_blocks, rp_grid_full) : rp_grid_full;
+    if (t.fdtd_rows != strip_rows || grid != rp_grid) drop_graphs();
+    strip_rows = t.fdtd_rows;
+    rp_blocks_req = t.rp_blocks;
+    rp_grid = grid;
+    return CRP_OK;
+  }
+  void get_tuning(crp_tuning* t) const {
+    t->fdtd_rows = strip_rows;
+    t->rp_blocks = rp_blocks_req;
+    t->rp_blocks_max = rp_grid_full;
+  }
+
+  // Snapshots (crp_save_state / crp_load_state): the device pool holds every
+  // device array of the handle; this is the host-side step state beside it.
+  struct HostState {
+    int cur_v, cur_p, fg_a, fg_b, fg_c, cur_t, bins_stale;
+    double tstep, tstepx, t_prev;
+    crp_stats stats;
+    Box supp[3], couple_box;
+    Scalars hsc;
+    crp_focus_state focus;
+    MinMax mm;
+    size_t n_focal, n_control;
+  };
+  size_t state_bytes() const { return pool_bytes; }
+
+  crp_status save_state(void* blob, std::vector<unsigned char>& host) {
+    CRP_CUDA(cudaMemcpyAsync(blob, pool, pool_bytes, cudaMemcpyDeviceToDevice, stream));
+    CRP_CUDA(cudaStreamSynchronize(stream));
+    HostState h{};
+    h.cur_v = cur_v, h.cur_p = cur_p, h.fg_a = fg_a, h.fg_b = fg_b, h.fg_c = fg_c, h.cur_t = cur_t;
+    h.bins_stale = bins_stale ? 1 : 0;
+    h.tstep = tstep, h.tstepx = tstepx, h.t_prev = t_prev;
+    h.stats = stats;
+    for (int q = 0; q < 3; q++) h.supp[q] = supp[q];
+    h.couple_box = couple_box;
+    h.hsc = *h_scalars;
+    h.focus = focus;
+    h.mm = mm;
+    h.n_focal = focal_hist.size();
+    h.n_control = control_hist.size();
+    host.resize(sizeof(HostState) + sizeof(double) * (h.n_focal + h.n_control));
+    std::memcpy(host.data(), &h, sizeof(HostState));
+    if (h.n_focal) std::memcpy(host.data() + sizeof(HostState), focal_hist.data(), sizeof(double) * h.n_focal);
+    if (h.n_control)
+      std::memcpy(host.data() + sizeof(HostState) + sizeof(double) * h.n_focal, control_hist.data(),
+                  sizeof(double) * h.n_control);
+    return CRP_OK;
+  }
+
+  crp_status load_state(const void* blob, const std::vector<unsigned char>& host) {
+    HostState h{};
+    if (host.size() < sizeof(HostState)) return fail(CRP_ERR_INVALID, "state: no host part");
+    std::memcpy(&h, host.data(), sizeof(HostState));
+    if (host.size() != sizeof(HostState) + sizeof(double) * (h.n_focal + h.n_control))
+      return fail(CRP_ERR_INVALID, "state: host part of the wrong size");
+    CRP_CUDA(cudaMemcpyAsync(pool, blob, pool_bytes, cudaMemcpyDeviceToDevice, stream));
+    CRP_CUDA(cudaStreamSynchronize(stream));
+    cur_v = h.cur_v, cur_p = h.cur_p, fg_a = h.fg_a, fg_b = h.fg_b, fg_c = h.fg_c, cur_t = h.cur_t;
+    bins_stale = h.bins_stale != 0;
+    tstep = h.tstep, tstepx = h.tstepx, t_prev = h.t_prev;
+    // The simulation's state returns; the counters of work done do not.
+    const crp_stats keep = stats;
+    stats = h.stats;
+    stats.kernel_launches = keep.kernel_launches;
+    stats.fdtd_launches = keep.fdtd_launches;
+    stats.rp_launches = keep.rp_launches;
+    stats.couple_launches = keep.couple_launches;
+    stats.ms_fdtd = keep.ms_fdtd, stats.ms_rp = keep.ms_rp, stats.ms_couple = keep.ms_couple;
+    stats.ms_other = keep.ms_other;
+    for (int q = 0; q < 3; q++) supp[q] = h.supp[q];
+    couple_box = h.couple_box;
+    *h_scalars = h.hsc;
+    focus = h.focus;
+    mm = h.mm;
+    const double* hist = reinterpret_cast<const double*>(host.data() + sizeof(HostState));
+    focal_hist.assign(hist, hist + h.n_focal);
+    control_hist.assign(hist + h.n_focal, hist + h.n_focal + h.n_control);
+    return CRP_OK;
+  }
+
+  ~Sim() {
+    drop_graphs();
     if (cap_stream) cudaStreamDestroy(cap_stream);
     if (h_push) cudaFreeHost(h_push);
     if (pool) cudaFree(pool);
     if (h_scalars) cudaFreeHost(h_scalars);
     if (ev_scalars) cudaEventDestroy(ev_scalars);
+    if (ev_block) cudaEventDestroy(ev_block);
     if (h_focal) cudaFreeHost(h_focal);
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
@@ -3087,6 +3240,15 @@ cudaError_t Sim::launch_couple(bool pressure) {
 }  // namespace crp
 
 // ---------------------------------------------------------------------------
+// A snapshot (crp_save_state): the device pool's copy and the host-side state.
+struct crp_state {
+  int device = 0;
+  int dims = 2;
+  size_t bytes = 0;
+  void* blob = nullptr;
+  std::vector<unsigned char> host;
+};
+
 struct crp_sim {
   crp::Sim s;
   crp::Sim3Impl* s3 = nullptr;  // a 3-D grid (ext.grid_z > 0) runs here instead of s
@@ -3316,6 +3478,75 @@ crp_status crp_write_sph(crp_sim* h, const char* dir) {
   return crp::write_sph(h, dir);
 }
 
+size_t crp_state_bytes(const crp_sim* h) {
+  if (!h) return 0;
+  return h->s3 ? crp::sim3_state_bytes(h->s3) : h->s.state_bytes();
+}
+
+crp_status crp_save_state(crp_sim* h, crp_state** out) {
+  if (!h || !out) return CRP_ERR_INVALID;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
+  const size_t bytes = crp_state_bytes(h);
+  const int dims = h->s3 ? 3 : 2;
+  crp_state* st = *out;
+  if (st && (st->bytes != bytes || st->dims != dims || st->device != h->device())) return CRP_ERR_INVALID;
+  if (!st) {
+    st = new (std::nothrow) crp_state();
+    if (!st) return CRP_ERR_ALLOC;
+    st->bytes = bytes;
+    st->dims = dims;
+    st->device = h->device();
+    if (cudaMalloc(&st->blob, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      delete st;
+      return CRP_ERR_ALLOC;
+    }
+  }
+  const crp_status r =
+      h->s3 ? crp::sim3_save_state(h->s3, st->blob, st->host) : h->s.save_state(st->blob, st->host);
+  if (r != CRP_OK) {
+    if (!*out) crp_state_free(st);
+    return r;
+  }
+  *out = st;
+  return CRP_OK;
+}
+
+crp_status crp_load_state(crp_sim* h, const crp_state* st) {
+  if (!h || !st) return CRP_ERR_INVALID;
+  if (st->bytes != crp_state_bytes(h) || st->dims != (h->s3 ? 3 : 2) || st->device != h->device())
+    return CRP_ERR_INVALID;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
+  return h->s3 ? crp::sim3_load_state(h->s3, st->blob, st->host) : h->s.load_state(st->blob, st->host);
+}
+
+void crp_state_free(crp_state* st) {
+  if (!st) return;
+  int prev = 0;
+  const bool have = cudaGetDevice(&prev) == cudaSuccess;
+  if (cudaSetDevice(st->device) == cudaSuccess && st->blob) cudaFree(st->blob);
+  if (have) cudaSetDevice(prev);
+  delete st;
+}
+
+crp_status crp_get_tuning(const crp_sim* h, crp_tuning* t) {
+  if (!h || !t) return CRP_ERR_INVALID;
+  if (h->s3)
+    crp::sim3_get_tuning(h->s3, t);
+  else
+    h->s.get_tuning(t);
+  return CRP_OK;
+}
+
+crp_status crp_set_tuning(crp_sim* h, const crp_tuning* t) {
+  if (!h || !t) return CRP_ERR_INVALID;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
+  return h->s3 ? crp::sim3_set_tuning(h->s3, t) : h->s.set_tuning(*t);
+}
+
 }  // extern "C"
 
 namespace crp {
@@ -3323,7 +3554,29 @@ namespace crp {
 crp_status sim_read_field(crp_sim* h, crp_field f, double* host) { return h->s.read_field(f, host); }
 crp_status sim_read_bubbles(crp_sim* h, crp_bubble_field w, double* host) { return h->s.read_bubbles(w, host); }
 const crp_config& sim_config(const crp_sim* h) { return h->s.cfg; }
-int64_t sim_step_count(const crp_sim* h) { return h->s.stats.steps; }
+int64_t sim_step_count(const crp_sim* h) { return h->s3 ? sim3_stats(h->s3).steps : h->s.stats.steps; }
+
+// Graph-queued steps for crp_batch (batch.cpp).
+bool sim_graph_ready(const crp_sim* h) { return !h->s3 && h->s.graph_ready(); }
+void sim_allow_graphs(crp_sim* h, bool on) {
+  if (!h->s3) h->s.graphs_on = on;
+}
+crp_status sim_blocking_waits(crp_sim* h, bool on) {
+  if (h->s3) return CRP_OK;
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
+  return h->s.set_blocking_waits(on);
+}
+crp_status sim_graphs_enqueue(crp_sim* h, int n) {
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
+  return h->s.graphs_enqueue(n);
+}
+crp_status sim_graphs_finish(crp_sim* h) {
+  DeviceScope dev(h);
+  if (!dev.ok()) return CRP_ERR_CUDA;
+  return h->s.graphs_finish();
+}
 double sim_time(const crp_sim* h) { return h->s.tstep; }
 MinMax& sim_minmax(crp_sim* h) { return h->s.mm; }
 }  // namespace crp

@@ -785,6 +785,7 @@ struct Sim3Impl {
   bool mixed = false;
   std::string err;
   char* pool = nullptr;
+  size_t pool_bytes = 0;
   size_t cells = 0;
   void *vx[2]{}, *vy[2]{}, *vz[2]{}, *px[2]{}, *py[2]{}, *pz[2]{}, *fg[3]{};
   double* d_fac = nullptr;  // PML factors
@@ -806,6 +807,8 @@ struct Sim3Impl {
   double picard_tol = 1.0e-7f;
   bool bins_stale = true;
   int rp_grid = 1;
+  int rp_grid_full = 1;  // one lane per bubble, up to 4 blocks per SM
+  int rp_blocks_req = 0;  // crp_set_tuning (0: rp_grid_full)
   int supp[3][6];
   crp_stats stats{};
   int64_t launches = 0;
@@ -1074,7 +1077,7 @@ crp_status Sim3Impl::create(const crp_config& c, const crp_bubbles_in* bin, void
     }
   }
   const int nb = (int)bx.size();
-  size_t pool_bytes = layout(true, nb);
+  pool_bytes = layout(true, nb);
   C3(cudaMalloc(&pool, pool_bytes));
   layout(false, nb);
   C3(cudaMemsetAsync(pool, 0, pool_bytes, stream));
@@ -1185,7 +1188,8 @@ crp_status Sim3Impl::create(const crp_config& c, const crp_bubbles_in* bin, void
   }
   int sms = 0;
   C3(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-  rp_grid = std::max(1, std::min(sms * 4, (nb + d3::kRpThreads3 - 1) / d3::kRpThreads3));
+  rp_grid_full = std::max(1, std::min(sms * 4, (nb + d3::kRpThreads3 - 1) / d3::kRpThreads3));
+  rp_grid = rp_grid_full;
   C3(cudaStreamSynchronize(stream));
   return CRP_OK;
 }
@@ -1562,6 +1566,66 @@ const crp_stats& sim3_stats(const Sim3Impl* s) { return s->stats; }
 const char* sim3_error(const Sim3Impl* s) { return s->err.c_str(); }
 crp_status sim3_set_profiling(Sim3Impl* s, int on) { return s->set_profiling(on != 0); }
 void* sim3_stream(Sim3Impl* s) { return (void*)s->stream; }
+
+// Snapshots: the device pool, and the host-side step state beside it.
+struct HostState3 {
+  int cur_v, cur_p, fg_a, fg_b, fg_c, bins_stale;
+  double tstep, tstepx, t_prev;
+  int supp[3][6];
+  crp_stats stats;
+  d3::Scalars3 hsc;
+};
+size_t sim3_state_bytes(const Sim3Impl* s) { return s->pool_bytes; }
+crp_status sim3_save_state(Sim3Impl* s, void* blob, std::vector<unsigned char>& host) {
+  if (cudaMemcpyAsync(blob, s->pool, s->pool_bytes, cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->stream) != cudaSuccess)
+    return s->fail(CRP_ERR_CUDA, "state: device copy");
+  HostState3 h{};
+  h.cur_v = s->cur_v, h.cur_p = s->cur_p, h.fg_a = s->fg_a, h.fg_b = s->fg_b, h.fg_c = s->fg_c;
+  h.bins_stale = s->bins_stale ? 1 : 0;
+  h.tstep = s->tstep, h.tstepx = s->tstepx, h.t_prev = s->t_prev;
+  std::memcpy(h.supp, s->supp, sizeof(h.supp));
+  h.stats = s->stats;
+  h.hsc = *s->h_sc;
+  host.resize(sizeof(HostState3));
+  std::memcpy(host.data(), &h, sizeof(HostState3));
+  return CRP_OK;
+}
+crp_status sim3_load_state(Sim3Impl* s, const void* blob, const std::vector<unsigned char>& host) {
+  if (host.size() != sizeof(HostState3)) return s->fail(CRP_ERR_INVALID, "state: host part of the wrong size");
+  HostState3 h;
+  std::memcpy(&h, host.data(), sizeof(HostState3));
+  if (cudaMemcpyAsync(s->pool, blob, s->pool_bytes, cudaMemcpyDeviceToDevice, s->stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->stream) != cudaSuccess)
+    return s->fail(CRP_ERR_CUDA, "state: device copy");
+  s->cur_v = h.cur_v, s->cur_p = h.cur_p, s->fg_a = h.fg_a, s->fg_b = h.fg_b, s->fg_c = h.fg_c;
+  s->bins_stale = h.bins_stale != 0;
+  s->tstep = h.tstep, s->tstepx = h.tstepx, s->t_prev = h.t_prev;
+  std::memcpy(s->supp, h.supp, sizeof(h.supp));
+  const crp_stats keep = s->stats;
+  s->stats = h.stats;
+  s->stats.kernel_launches = keep.kernel_launches;
+  s->stats.fdtd_launches = keep.fdtd_launches;
+  s->stats.rp_launches = keep.rp_launches;
+  s->stats.couple_launches = keep.couple_launches;
+  s->stats.ms_fdtd = keep.ms_fdtd, s->stats.ms_rp = keep.ms_rp, s->stats.ms_couple = keep.ms_couple;
+  s->stats.ms_other = keep.ms_other;
+  *s->h_sc = h.hsc;
+  return CRP_OK;
+}
+crp_status sim3_set_tuning(Sim3Impl* s, const crp_tuning* t) {
+  if (t->fdtd_rows != 4 && t->fdtd_rows != 8 && t->fdtd_rows != 16)
+    return s->fail(CRP_ERR_INVALID, "tuning: fdtd_rows must be 4, 8 or 16");
+  if (t->rp_blocks < 0) return s->fail(CRP_ERR_INVALID, "tuning: rp_blocks must be >= 0");
+  s->rp_blocks_req = t->rp_blocks;
+  s->rp_grid = t->rp_blocks > 0 ? std::min(t->rp_blocks, s->rp_grid_full) : s->rp_grid_full;
+  return CRP_OK;
+}
+void sim3_get_tuning(const Sim3Impl* s, crp_tuning* t) {
+  t->fdtd_rows = 8;
+  t->rp_blocks = s->rp_blocks_req;
+  t->rp_blocks_max = s->rp_grid_full;
+}
 int sim3_device(const Sim3Impl* s) { return s->device; }
 
 }  // namespace crp

@@ -1,6 +1,7 @@
 // The 3-D Cartesian simulation (sim3d.cu) as seen by the C ABI in sim.cu.
 #pragma once
 #include <string>
+#include <vector>
 
 #include "crp.h"
 
@@ -21,5 +22,10 @@ const char* sim3_error(const Sim3Impl* s);
 crp_status sim3_set_profiling(Sim3Impl* s, int on);
 void* sim3_stream(Sim3Impl* s);
 int sim3_device(const Sim3Impl* s);
+size_t sim3_state_bytes(const Sim3Impl* s);
+crp_status sim3_save_state(Sim3Impl* s, void* blob, std::vector<unsigned char>& host);
+crp_status sim3_load_state(Sim3Impl* s, const void* blob, const std::vector<unsigned char>& host);
+crp_status sim3_set_tuning(Sim3Impl* s, const crp_tuning* t);
+void sim3_get_tuning(const Sim3Impl* s, crp_tuning* t);
 
 }  // namespace crp

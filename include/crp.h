@@ -393,20 +393,90 @@ typedef struct crp_output_plan {
 } crp_output_plan;
 crp_status crp_run(crp_sim* sim, const crp_output_plan* plan, const crp_config* cfg);
 
+/* State snapshots (no reference counterpart: the reference keeps no
+ * checkpoints).  crp_save_state copies every device array of the simulation
+ * (fields, void-fraction ring, bubbles, bins, source elements, device scalars:
+ * crp_state_bytes bytes) into a device blob on the simulation's GPU, and keeps
+ * the host-side step state (time, buffer phases, statistics, coupling boxes,
+ * focal history) beside it.  *state == NULL allocates a snapshot; an existing
+ * one, taken from this simulation, is overwritten.  crp_load_state puts a
+ * snapshot back into the simulation it was taken from (or one created from the
+ * same configuration and bubbles on the same GPU): the run then continues bit
+ * for bit as it did after the save.  The counters of work done (launch counts,
+ * profiling times) are not rewound.  Both calls wait for the copy. */
+typedef struct crp_state crp_state;
+size_t crp_state_bytes(const crp_sim* sim);
+crp_status crp_save_state(crp_sim* sim, crp_state** state);
+crp_status crp_load_state(crp_sim* sim, const crp_state* state);
+void crp_state_free(crp_state* state);
+
+/* Launch shapes (no reference counterpart), chosen by crp_batch_tune or set
+ * directly; results are bit for bit the same under every setting.
+ * fdtd_rows: rows per chunk of the 2-D FDTD strip kernel, 4, 8 (default) or 16
+ * (the 3-D path accepts the value and ignores it).  rp_blocks: blocks of the
+ * persistent radius kernel (0, the default: one lane per bubble up to the
+ * occupancy limit, rp_blocks_max, which crp_get_tuning reports; larger
+ * values are clamped to it). */
+typedef struct crp_tuning {
+  int32_t fdtd_rows;
+  int32_t rp_blocks;
+  int32_t rp_blocks_max; /* output of crp_get_tuning; ignored by crp_set_tuning */
+} crp_tuning;
+crp_status crp_get_tuning(const crp_sim* sim, crp_tuning* tuning);
+crp_status crp_set_tuning(crp_sim* sim, const crp_tuning* tuning);
+
 /* Batched sweep: count independent simulations (cfgs[k], bubbles[k] or NULL /
  * n = 0 for the configuration's own seeding), each with its own stream, run
  * concurrently.  Replaces re-running `bubbles` over a list of configuration
  * files (scripts/executor.sh:28-47).  crp_batch_run advances simulation k by
- * steps[k] mixture steps from a pool of host threads (threads <= 0: up to 32),
- * largest cells x steps first; per_sim (may be NULL) receives each status and
- * the first non-OK status in index order is returned.  The simulations are
- * crp_sim handles (crp_batch_sim) for reading fields, stats and rawdata. */
+ * steps[k] mixture steps, largest cells x steps first; per_sim (may be NULL)
+ * receives each status and the first non-OK status in index order is
+ * returned.  threads > 0: a pool of that many host threads, each driving its
+ * simulations' steps and Picard loops; threads = 0: the batch's tuning
+ * (crp_batch_set_tuning / crp_batch_tune; by default a pool of up to 32
+ * threads).  The simulations are crp_sim handles (crp_batch_sim) for reading
+ * fields, stats and rawdata. */
 typedef struct crp_batch crp_batch;
 crp_status crp_batch_create(int32_t count, const crp_config* cfgs, const crp_bubbles_in* bubbles, crp_batch** out);
 crp_status crp_batch_run(crp_batch* batch, const int32_t* steps, int32_t threads, crp_status* per_sim);
 int32_t crp_batch_count(const crp_batch* batch);
 crp_sim* crp_batch_sim(crp_batch* batch, int32_t k);
 void crp_batch_destroy(crp_batch* batch);
+
+/* How crp_batch_run drives a batch (threads = 0).
+ * CRP_BATCH_THREADS: host threads, each running its simulations' steps with
+ * the host-driven Picard loop.  CRP_BATCH_GRAPHS: one host thread queues every
+ * simulation's steps as CUDA graphs with the Picard loop decided on the device
+ * (ext.graphs) on each simulation's stream, then waits for all; simulations
+ * that cannot run as graphs (3-D grids, no bubbles, the first step, debug.T)
+ * run those steps on a host thread meanwhile.  fdtd_rows and
+ * rp_bubbles_per_lane are applied to every simulation: the radius kernel gets
+ * ceil(n_bubbles / (128 rp_bubbles_per_lane)) blocks (at most its occupancy
+ * limit; 1 is the default grid).  ms_per_step: the wall-clock time per batch
+ * step crp_batch_tune measured for this setting (0 when not measured). */
+typedef enum crp_batch_mode { CRP_BATCH_THREADS = 0, CRP_BATCH_GRAPHS = 1 } crp_batch_mode;
+typedef struct crp_batch_tuning {
+  int32_t mode;
+  int32_t threads;              /* CRP_BATCH_THREADS: pool size (0: min(count, 32)) */
+  int32_t blocking;             /* CRP_BATCH_THREADS: 1 = the host threads block on events inside a
+                                   step instead of spinning (for more threads than host cores) */
+  int32_t fdtd_rows;            /* 4, 8 or 16 */
+  int32_t rp_bubbles_per_lane;  /* >= 1 */
+  double ms_per_step;
+} crp_batch_tuning;
+crp_status crp_batch_get_tuning(const crp_batch* batch, crp_batch_tuning* tuning);
+crp_status crp_batch_set_tuning(crp_batch* batch, const crp_batch_tuning* tuning);
+/* The autotuner: times trial_steps batch steps (after 2 untimed ones) under
+ * each candidate setting, searched one parameter at a time from the defaults
+ * (mode; threads min(count, 32), count or 16, spinning or blocking; fdtd_rows
+ * 4, 8, 16; rp_bubbles_per_lane 1, 4, 16), restoring every simulation's state
+ * (crp_save_state / crp_load_state) after each trial, and applies the
+ * fastest.  The batch's
+ * simulations end where they started.  n_tried (may be NULL) receives the
+ * number of settings timed; tried (may be NULL, capacity entries) their
+ * timings. */
+crp_status crp_batch_tune(crp_batch* batch, int32_t trial_steps, crp_batch_tuning* best,
+                          crp_batch_tuning* tried, int32_t capacity, int32_t* n_tried);
 
 /* Phased-array source and its adjoint.  Neither has a counterpart in the
  * reference (its source is one focused aperture, src/bubble_CUDA.cu:542-551,

@@ -81,3 +81,59 @@ def test_handles_run_from_other_host_threads():
             assert np.array_equal(a, b)
         for a, b in zip(_state(batch.sims[0]), ref):
             assert np.array_equal(a, b)
+
+
+def _batch_state(batch):
+    return [(_state(s), s.stats().steps, s.stats().picard_total) for s in batch.sims]
+
+
+def _equal(u, v):
+    for (fa, sa, pa), (fb, sb, pb) in zip(u, v):
+        assert (sa, pa) == (sb, pb)
+        for a, b in zip(fa, fb):
+            assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("setting", [dict(mode=crp.BATCH_GRAPHS), dict(fdtd_rows=4), dict(fdtd_rows=16),
+                                     dict(rp_bubbles_per_lane=16), dict(blocking=1, threads=8),
+                                     dict(mode=crp.BATCH_GRAPHS, fdtd_rows=16, rp_bubbles_per_lane=4)])
+def test_batch_settings_give_the_same_results(setting):
+    """Graph-queued steps (device-side Picard control, one host thread) and
+    other launch shapes give the thread-pool run's results bit for bit,
+    including a simulation without bubbles (host steps beside the graphs)."""
+    cfgs = _configs()
+    steps = [60, 45, 30, 80]
+    runs = []
+    for s in (None, setting):
+        with crp.Batch(cfgs) as batch:
+            if s is not None:
+                t = batch.tuning
+                for k, v in s.items():
+                    setattr(t, k, v)
+                batch.tuning = t
+            batch.run(steps[:2] + [10, 10])
+            batch.run([a - b for a, b in zip(steps, steps[:2] + [10, 10])])
+            runs.append(_batch_state(batch))
+    _equal(*runs)
+
+
+def test_batch_tune_restores_and_applies():
+    """crp_batch_tune times its candidate settings on the batch itself and
+    leaves every simulation where it was; the tuned run equals an untuned one."""
+    cfgs = _configs()
+    with crp.Batch(cfgs) as ref:
+        ref.run([20] * 4)
+        ref.run([30] * 4)
+        want = _batch_state(ref)
+    with crp.Batch(cfgs) as batch:
+        batch.run([20] * 4)
+        before = _batch_state(batch)
+        best, tried = batch.tune(trial_steps=5)
+        print(best.as_dict(), [t.as_dict() for t in tried])
+        assert len(tried) == 8  # default, graphs, 16 threads, blocking waits, rows 4 and 16, lanes 4 and 16
+        assert all(t.ms_per_step > 0 for t in tried)
+        assert best.ms_per_step == min(t.ms_per_step for t in tried)
+        _equal(_batch_state(batch), before)
+        assert batch.tuning.as_dict() == best.as_dict()
+        batch.run([30] * 4)
+        _equal(_batch_state(batch), want)
