@@ -716,13 +716,14 @@ __device__ __forceinline__ double gather_pl(const GridParams& g, const BubblePar
 
 // With `reuse` (a radius solve of this step has completed with the current
 // bins), a bubble whose gathered pressure has the bit pattern of the last
-// solve's is not set up: every input of its solve is unchanged, so its stored
-// results are what the solve would write; returns false for it.
+// solve's needs no solve: every input of its solve is unchanged, so its stored
+// results are what the solve would write; returns false for it.  The set-up
+// runs either way (a branch around it costs the radius kernel registers).
 template <typename S>
 __device__ __forceinline__ bool rp_begin(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
                                          const S& px, const S& py, double t_cur, int n, RpState& s, bool reuse) {
   const double PLp = gather_pl(g, bp, b, px, py, t_cur, n);
-  if (reuse && __double_as_longlong(PLp) == __double_as_longlong(b.PL_p[n])) return false;
+  const bool same = reuse && __double_as_longlong(PLp) == __double_as_longlong(b.PL_p[n]);
   b.PL_p[n] = PLp;
   s.r = bubble_r0(bp, b.R0[n]);
   const double dt = g.dt;
@@ -742,7 +743,7 @@ __device__ __forceinline__ bool rp_begin(const GridParams& g, const BubbleParams
   s.heat = 0.0;
   s.vis = 0.0;
   s.count = 0;
-  return true;
+  return !same;
 }
 
 
@@ -806,10 +807,14 @@ constexpr int rp_min_blocks() {
   return sizeof(typename P::T) == sizeof(double) ? 6 : 5;
 }
 
-// Solves kept by rp_begin/rk_begin, summed per warp into one counter.
-__device__ __forceinline__ void count_kept(unsigned long long kept, unsigned long long* reused) {
-  for (int o = 16; o > 0; o >>= 1) kept += __shfl_xor_sync(0xffffffffu, kept, o);
-  if ((threadIdx.x & 31) == 0 && kept) atomicAdd(reused, kept);
+// Lanes whose claimed bubble kept its last solve (n == -2) are counted, one
+// atomic per warp, and return to claiming (n = -1).  Called by the whole warp.
+__device__ __forceinline__ void count_kept(int& n, unsigned long long* reused) {
+  const unsigned kept = __ballot_sync(0xffffffffu, n == -2);
+  if (kept) {
+    if ((threadIdx.x & 31) == 0) atomicAdd(reused, (unsigned long long)__popc(kept));
+    if (n == -2) n = -1;
+  }
 }
 
 template <typename P>
@@ -827,7 +832,6 @@ __global__ void __launch_bounds__(kRpThreads, rp_min_blocks<P>()) bubble_rp(cons
   int n = -1;
   bool drained = false;
   long long worst = 0;
-  unsigned long long kept = 0;
   const int lane = threadIdx.x & 31;
   for (;;) {
     // Lanes without a bubble claim the next ones from the queue together:
@@ -842,14 +846,12 @@ __global__ void __launch_bounds__(kRpThreads, rp_min_blocks<P>()) bubble_rp(cons
         const int q = base + __popc(need & ((1u << lane) - 1u));
         if (q < b.n) {
           n = order[q];
-          if (!rp_begin(g, bp, b, px, py, t_cur, n, s, reuse)) {
-            n = -1;
-            kept++;
-          }
+          if (!rp_begin(g, bp, b, px, py, t_cur, n, s, reuse)) n = -2;  // kept: counted below
         } else {
           drained = true;
         }
       }
+      count_kept(n, reused);
     }
     if (!__any_sync(0xffffffffu, n >= 0 || !drained)) break;
     if (n >= 0) {
@@ -865,7 +867,6 @@ __global__ void __launch_bounds__(kRpThreads, rp_min_blocks<P>()) bubble_rp(cons
   }
   for (int o = 16; o > 0; o >>= 1) worst = max(worst, __shfl_xor_sync(0xffffffffu, worst, o));
   if ((threadIdx.x & 31) == 0 && worst > 0) atomicMax(substep_max, worst);
-  count_kept(kept, reused);
 }
 
 }  // namespace crp
@@ -880,7 +881,7 @@ template <typename S>
 __device__ __forceinline__ bool rk_begin(const GridParams& g, const BubbleParams& bp, const BubbleArrays& b,
                                          const S& px, const S& py, double t_cur, int n, RkState& s, bool reuse) {
   const double PLp = gather_pl(g, bp, b, px, py, t_cur, n);
-  if (reuse && __double_as_longlong(PLp) == __double_as_longlong(b.PL_p[n])) return false;
+  const bool same = reuse && __double_as_longlong(PLp) == __double_as_longlong(b.PL_p[n]);
   b.PL_p[n] = PLp;
   s.r = bubble_r0(bp, b.R0[n]);
   const double dt = g.dt;
@@ -898,7 +899,7 @@ __device__ __forceinline__ bool rk_begin(const GridParams& g, const BubbleParams
   s.PC1 = 0.5 * (PLp - PLm) / dt;
   s.PC2 = 0.5 * (PLp + PLm - 2.0 * PLn) / (dt * dt);
   s.K = 3.0 * (bp.gam - 1.0) * bp.K0 * bp.T0 * s.r.inv_PG0;
-  return true;
+  return !same;
 }
 
 // Results of the integration in the arrays the reference scheme fills: the
@@ -942,7 +943,6 @@ __global__ void __launch_bounds__(kRpThreads, rk_min_blocks<P>()) bubble_rk45(co
   int n = -1;
   bool drained = false;
   long long worst = 0;
-  unsigned long long kept = 0;
   const int lane = threadIdx.x & 31;
   for (;;) {
     const unsigned need = __ballot_sync(0xffffffffu, n < 0 && !drained);
@@ -955,14 +955,12 @@ __global__ void __launch_bounds__(kRpThreads, rk_min_blocks<P>()) bubble_rk45(co
         const int q = base + __popc(need & ((1u << lane) - 1u));
         if (q < b.n) {
           n = order[q];
-          if (!rk_begin(g, bp, b, px, py, t_cur, n, s, reuse)) {
-            n = -1;
-            kept++;
-          }
+          if (!rk_begin(g, bp, b, px, py, t_cur, n, s, reuse)) n = -2;  // kept: counted below
         } else {
           drained = true;
         }
       }
+      count_kept(n, reused);
     }
     if (!__any_sync(0xffffffffu, n >= 0 || !drained)) break;
     if (n >= 0) {
@@ -978,7 +976,6 @@ __global__ void __launch_bounds__(kRpThreads, rk_min_blocks<P>()) bubble_rk45(co
   }
   for (int o = 16; o > 0; o >>= 1) worst = max(worst, __shfl_xor_sync(0xffffffffu, worst, o));
   if ((threadIdx.x & 31) == 0 && worst > 0) atomicMax(substep_max, worst);
-  count_kept(kept, reused);
 }
 
 // Work order for the next radius solves: bubbles bucketed by the binary
