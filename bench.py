@@ -482,6 +482,46 @@ def adjoint_cost(cfg):
                     "differences and the oracle in tests/test_adjoint_gpu.py"}
 
 
+def adjoint_cost3(cfg):
+    """adjoint_cost on a 3-D grid: the bowl's own elements (amplitude 1, focusing
+    phases), FP64, bubbles off, over the steps until 100 after the burst reaches
+    the focus (array radius / c)."""
+    import torch
+
+    import crp
+
+    c = crp.Config.from_buffer_copy(cfg)
+    c.bub_enable = 0
+    c.ext_precision = 0
+    ne = c.ext_array_elements
+    with crp.Sim(c) as probe:
+        dt = probe.dims3.dt
+    steps = int(np.ceil(c.ext_array_radius / c.ext_c_inf / dt)) + 100
+
+    def timed(fn, sim):
+        st = torch.cuda.ExternalStream(sim.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        out = fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    with crp.Sim(c) as fwd:
+        fwd.step(1)
+        ms_fwd, _ = timed(lambda: fwd.step(steps - 1), fwd)
+    with crp.Sim(c) as adj:
+        ms_adj, (J, ga, gp) = timed(lambda: adj.adjoint(steps, 2.0e-3, ne), adj)
+    ms_fwd *= steps / (steps - 1)
+    return {"steps": steps, "focal_radius_m": 2.0e-3, "elements": ne, "precision": "fp64", "bubbles": 0,
+            "forward_ms": ms_fwd, "adjoint_ms": ms_adj, "adjoint_over_forward": ms_adj / ms_fwd,
+            "J": J, "grad_amp_norm": float(np.linalg.norm(ga)), "grad_phase_norm": float(np.linalg.norm(gp)),
+            "note": "crp_adjoint on the 3-D grid (its forward with the focal record, the objective and the reverse "
+                    "sweep) over the forward's device time on the same grid and steps; gradients checked against "
+                    "finite differences and the oracle in tests/test_adjoint3_gpu.py"}
+
+
 def focal_compare_step(cfg):
     """Mixture step 100 steps after the focused burst reaches the focus: the
     source delays make every element's wave arrive there at t = focal_dist / c."""
@@ -624,8 +664,8 @@ def run_ours(args, rank, world, dist):
     prof = {k: (getattr(p1s, k) - getattr(p0s, k)) for k in ("ms_fdtd", "ms_rp", "ms_couple", "ms_other")}
 
     e2e = guarded(e2e_run, cfg, bub, args, nb) if rank == 0 and not args.no_e2e else None
-    adjoint = (guarded(adjoint_cost, cfg) if rank == 0 and world == 1 and not args.no_adjoint and not is3d(cfg)
-               else None)
+    adjoint = (guarded(adjoint_cost3 if is3d(cfg) else adjoint_cost, cfg)
+               if rank == 0 and world == 1 and not args.no_adjoint else None)
     driven = guarded(driven_sample, sim, args, cells, nb) if with_driven else None
     driven_rk45 = guarded(driven_rk45_sample, cfg, bub, args, cells, nb, sim) if with_driven else None
     focal = None

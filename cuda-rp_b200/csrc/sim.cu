@@ -3424,9 +3424,9 @@ crp_status crp_set_source_elements(crp_sim* h, int32_t n, const double* amp, con
 
 crp_status crp_adjoint(crp_sim* h, const crp_objective* obj, double* J, double* grad_amp, double* grad_phase) {
   if (!h) return CRP_ERR_INVALID;
-  if (h->s3) return CRP_ERR_UNSUPPORTED;
   DeviceScope dev(h);
   if (!dev.ok()) return CRP_ERR_CUDA;
+  if (h->s3) return crp::sim3_adjoint(h->s3, obj, J, grad_amp, grad_phase);
   return h->s.adjoint(obj, J, grad_amp, grad_phase);
 }
 

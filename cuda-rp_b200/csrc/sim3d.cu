@@ -770,6 +770,143 @@ struct PMix {
   static constexpr int kIndex = 1;
 };
 
+// ---------------------------------------------------------------------------
+// Discrete adjoint of the bubble-free 3-D step (crp_adjoint).  Without bubbles
+// the step is linear in the state:
+//   v'_f  = (v_f va - dt_rho rd (p0_b - p0_a)) vb           every computed face f
+//                                                            between cells a and b,
+//   p'_c  = p_c pa_c - s3p pb_c (v'_east - v'_west) rd_c     interior cells, c = x, y, z,
+//   p'_x  = s_e(t), p'_y = p'_z = 0                         source cells,
+// with p0 = px + py + pz (0 in the ghost cells, which are never written).  The
+// reverse of one step, given the adjoint of the state after it:
+//   1. adj3_source: the source cells' share of the gradient, their adjoint zeroed;
+//   2. adj3_faces:  the face adjoints take the pressure update's transpose;
+//   3. adj3_cells:  component adjoints pa_c M_c plus the velocity update's
+//                   transpose into p0 (the same for all three components);
+//   4. adj3_vscale: the face adjoints times va vb;
+// then adj3_force adds 2 dt w p0 of the step before for the focal cells.
+struct Adj3 {
+  double *LX, *LY, *LZ;  // adjoints of vx, vy, vz (frame layout)
+  double *MX, *MY, *MZ;  // adjoints of px, py, pz
+};
+struct Box3 {
+  int i0, j0, k0, nx, ny, nz;
+  const double* w;  // weight of each box cell (0 outside the focal sphere)
+};
+
+__device__ __forceinline__ bool frame_pos(const Frame3& f, long t, int& i, int& j, int& k) {
+  // t over (X+2)(Y+2)(Z+2) positions: i, j, k in [0, N+1].
+  const long nx = f.X + 2, ny = f.Y + 2;
+  if (t >= nx * ny * (long)(f.Z + 2)) return false;
+  i = (int)(t % nx);
+  j = (int)((t / nx) % ny);
+  k = (int)(t / (nx * ny));
+  return true;
+}
+
+template <typename S>
+__global__ void adj3_record(const Frame3 f, const S px, const S py, const S pz, const Box3 b, double* out) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= (long)b.nx * b.ny * b.nz) return;
+  const int i = b.i0 + (int)(t % b.nx), j = b.j0 + (int)((t / b.nx) % b.ny), k = b.k0 + (int)(t / ((long)b.nx * b.ny));
+  const long q = f.idx(i, j, k);
+  out[t] = px.get(q) + py.get(q) + pz.get(q);
+}
+
+__global__ void adj3_objective(const Box3 b, const double* p0, double* Jn) {
+  // One block per recorded step: sum of w p0^2 in a fixed order.
+  __shared__ double part[256];
+  const long n = (long)b.nx * b.ny * b.nz;
+  const double* p = p0 + blockIdx.x * n;
+  double s = 0.0;
+  for (long t = threadIdx.x; t < n; t += blockDim.x) s += b.w[t] * p[t] * p[t];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) Jn[blockIdx.x] = part[0];
+}
+
+__global__ void adj3_force(const Frame3 f, const Adj3 a, const Box3 b, const double* p0, double two_dt) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= (long)b.nx * b.ny * b.nz) return;
+  const double w = b.w[t];
+  if (w == 0.0) return;
+  const int i = b.i0 + (int)(t % b.nx), j = b.j0 + (int)((t / b.nx) % b.ny), k = b.k0 + (int)(t / ((long)b.nx * b.ny));
+  const long q = f.idx(i, j, k);
+  const double d = two_dt * w * p0[t];
+  a.MX[q] += d;
+  a.MY[q] += d;
+  a.MZ[q] += d;
+}
+
+// Source cell c (frame index cells[c], element elem[c]) at the step's time t:
+// d p'_x / d amp_e and d p'_x / d phase_e times the adjoint of p'_x, summed
+// over the steps per cell; the cell's adjoints then end (the forced values do
+// not depend on the state).
+__global__ void adj3_source(const __grid_constant__ Grid3 g, const Adj3 a, const long* cells, const int* elem, int n,
+                            double t, double* gA, double* gP) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const long q = cells[c];
+  const double m = a.MX[q];
+  a.MX[q] = 0.0;
+  a.MY[q] = 0.0;
+  a.MZ[q] = 0.0;
+  if (!(t > 0.0)) return;
+  const double tau = fmod(t, g.period);
+  if (!(tau <= g.on_time)) return;
+  const int e = elem[c];
+  double sn, cs;
+  sincos(g.omega * t + g.elem_phase[e], &sn, &cs);
+  const double env = g.pamp * burst_env(g, tau);
+  gA[c] += m * env * sn;
+  gP[c] += m * env * g.elem_amp[e] * cs;
+}
+
+// Computed faces: vx for i in [0, X] (j, k interior), vy for j in [0, Y], vz for k in [0, Z].
+__global__ void adj3_faces(const __grid_constant__ Grid3 g, const Adj3 a) {
+  const Frame3& f = g.f;
+  int i, j, k;
+  if (!frame_pos(f, blockIdx.x * (long)blockDim.x + threadIdx.x, i, j, k)) return;
+  const int X = f.X, Y = f.Y, Z = f.Z;
+  const long q = f.idx(i, j, k);
+  const double c = -g.s3p;
+  if (i <= X && j >= 1 && j <= Y && k >= 1 && k <= Z)
+    a.LX[q] += c * g.rdx * (g.pbx[i] * a.MX[q] - g.pbx[i + 1] * a.MX[f.idx(i + 1, j, k)]);
+  if (j <= Y && i >= 1 && i <= X && k >= 1 && k <= Z)
+    a.LY[q] += c * g.rdy * (g.pby[j] * a.MY[q] - g.pby[j + 1] * a.MY[f.idx(i, j + 1, k)]);
+  if (k <= Z && i >= 1 && i <= X && j >= 1 && j <= Y)
+    a.LZ[q] += c * g.rdz * (g.pbz[k] * a.MZ[q] - g.pbz[k + 1] * a.MZ[f.idx(i, j, k + 1)]);
+}
+
+__global__ void adj3_cells(const __grid_constant__ Grid3 g, const Adj3 a) {
+  const Frame3& f = g.f;
+  int i, j, k;
+  if (!frame_pos(f, blockIdx.x * (long)blockDim.x + threadIdx.x, i, j, k)) return;
+  if (i < 1 || i > f.X || j < 1 || j > f.Y || k < 1 || k > f.Z) return;
+  const long q = f.idx(i, j, k);
+  const double lp0 = g.dt_rho * (g.rdx * (g.vbx[i + 1] * a.LX[q] - g.vbx[i] * a.LX[f.idx(i - 1, j, k)]) +
+                                 g.rdy * (g.vby[j + 1] * a.LY[q] - g.vby[j] * a.LY[f.idx(i, j - 1, k)]) +
+                                 g.rdz * (g.vbz[k + 1] * a.LZ[q] - g.vbz[k] * a.LZ[f.idx(i, j, k - 1)]));
+  a.MX[q] = g.pax[i] * a.MX[q] + lp0;
+  a.MY[q] = g.pay[j] * a.MY[q] + lp0;
+  a.MZ[q] = g.paz[k] * a.MZ[q] + lp0;
+}
+
+__global__ void adj3_vscale(const __grid_constant__ Grid3 g, const Adj3 a) {
+  const Frame3& f = g.f;
+  int i, j, k;
+  if (!frame_pos(f, blockIdx.x * (long)blockDim.x + threadIdx.x, i, j, k)) return;
+  const int X = f.X, Y = f.Y, Z = f.Z;
+  const long q = f.idx(i, j, k);
+  if (i <= X && j >= 1 && j <= Y && k >= 1 && k <= Z) a.LX[q] *= g.vax[i + 1] * g.vbx[i + 1];
+  if (j <= Y && i >= 1 && i <= X && k >= 1 && k <= Z) a.LY[q] *= g.vay[j + 1] * g.vby[j + 1];
+  if (k <= Z && i >= 1 && i <= X && j >= 1 && j <= Y) a.LZ[q] *= g.vaz[k + 1] * g.vbz[k + 1];
+}
+
 }  // namespace d3
 
 // ---------------------------------------------------------------------------
@@ -903,6 +1040,11 @@ struct Sim3Impl {
   }
   crp_status read_field(crp_field w, double* host);
   crp_status read_bubbles(crp_bubble_field w, double* host);
+  crp_status adjoint(const crp_objective* obj, double* J, double* grad_amp, double* grad_phase);
+  // Source cells (frame index, element) in frame order, and the focus the bowl's phases aim at.
+  std::vector<long> src_list;
+  std::vector<int> src_elem;
+  double focus[3] = {0.0, 0.0, 0.0};
   crp_status set_elements(int n, const double* amp, const double* phase);
   ~Sim3Impl();
 };
@@ -1018,6 +1160,9 @@ crp_status Sim3Impl::create(const crp_config& c, const crp_bubbles_in* bin, void
     const double cx = 0.5 * X * g.dx, cy = 0.5 * Y * g.dy, cz = 0.5 * Z * g.dz;
     const double golden = pi * (3.0 - std::sqrt(5.0));
     const double fx = cx + c.ext_array_focus_dx;
+    focus[0] = fx;
+    focus[1] = cy;
+    focus[2] = cz;
     if (elem_n > 32767) return fail(CRP_ERR_UNSUPPORTED, "more than 32767 array elements");
     for (int e = 0; e < elem_n; e++) {
       const double ct = -((double)e + 0.5) / (double)elem_n;
@@ -1051,6 +1196,8 @@ crp_status Sim3Impl::create(const crp_config& c, const crp_bubbles_in* bin, void
               if (dd < bd) bd = dd, best = e;
             }
             src[f.idx(i, j, k)] = (short)(best + 1);
+            src_list.push_back(f.idx(i, j, k));
+            src_elem.push_back(best);
             src_cells++;
           }
     }
@@ -1440,6 +1587,144 @@ crp_status Sim3Impl::step_once() {
 
 // Dense copies (x fastest) of a field's logical window: cells [0, N+1] per
 // axis, staggered components one more along their axis from -1.
+// crp_adjoint on the 3-D grid: the forward steps with the focal p0 recorded
+// after each, the objective, then the reverse sweep of the kernels above.
+crp_status Sim3Impl::adjoint(const crp_objective* obj, double* J, double* grad_amp, double* grad_phase) {
+  if (!obj || obj->steps <= 0 || !(obj->focal_radius > 0.0))
+    return fail(CRP_ERR_INVALID, "adjoint: steps > 0 and focal_radius > 0 are required");
+  if ((grad_amp || grad_phase) && elem_n == 0)
+    return fail(CRP_ERR_INVALID, "adjoint: gradients need ext.array_elements > 0");
+  if (bub.n > 0) return fail(CRP_ERR_UNSUPPORTED, "adjoint: bubbles off only");
+  const d3::Frame3& f = g.f;
+  const int N = obj->steps;
+  const double r = obj->focal_radius;
+  // Focal box: cell centres within r of the focus along each axis.
+  const int n3[3] = {f.X, f.Y, f.Z};
+  const double h3[3] = {g.dx, g.dy, g.dz};
+  int lo[3], hi[3];
+  bool empty = false;
+  for (int ax = 0; ax < 3; ax++) {
+    lo[ax] = n3[ax] + 1;
+    hi[ax] = 0;
+    for (int m = 1; m <= n3[ax]; m++)
+      if (std::fabs(((double)m - 0.5) * h3[ax] - focus[ax]) <= r) lo[ax] = std::min(lo[ax], m), hi[ax] = std::max(hi[ax], m);
+    if (hi[ax] < lo[ax]) empty = true;
+  }
+  if (empty)
+    for (int ax = 0; ax < 3; ax++) lo[ax] = hi[ax] = 1;  // one cell of weight 0
+  const int bx = hi[0] - lo[0] + 1, by = hi[1] - lo[1] + 1, bz = hi[2] - lo[2] + 1;
+  const size_t box_n = (size_t)bx * by * bz;
+  std::vector<double> w(box_n, 0.0);
+  if (!empty)
+    for (int kk = 0; kk < bz; kk++)
+      for (int jj = 0; jj < by; jj++)
+        for (int ii = 0; ii < bx; ii++) {
+          const int i = lo[0] + ii, j = lo[1] + jj, k = lo[2] + kk;
+          const double x = ((double)i - 0.5) * g.dx - focus[0], y = ((double)j - 0.5) * g.dy - focus[1],
+                       z = ((double)k - 0.5) * g.dz - focus[2];
+          if (x * x + y * y + z * z > r * r) continue;
+          if (std::binary_search(src_list.begin(), src_list.end(), f.idx(i, j, k))) continue;  // forced cells
+          w[((size_t)kk * by + jj) * bx + ii] = g.dx * g.dy * g.dz;
+        }
+  const size_t hist_n = (size_t)N * box_n;
+  if (hist_n * sizeof(double) > ((size_t)32 << 30))
+    return fail(CRP_ERR_TOO_LARGE, "adjoint: focal history above 32 GiB (steps x focal cells)");
+  const int ns = (int)src_list.size(), ns1 = std::max(ns, 1);
+  // Six adjoint frames, per-source-cell gradients, weights, history, objective
+  // per step; then the source cells' frame indices and elements.
+  const size_t n_doubles = 6 * cells + 2 * (size_t)ns1 + box_n + hist_n + (size_t)N;
+  const size_t bytes = n_doubles * sizeof(double) + (size_t)ns1 * (sizeof(long) + sizeof(int));
+  char* buf = nullptr;
+  if (cudaMalloc(&buf, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(CRP_ERR_ALLOC, "adjoint: device memory");
+  }
+  struct Free {  // on every return: let the queued work finish, then release the buffer
+    char* p;
+    cudaStream_t st;
+    ~Free() {
+      cudaStreamSynchronize(st);
+      cudaFree(p);
+    }
+  } guard{buf, stream};
+  double* base = reinterpret_cast<double*>(buf);
+  d3::Adj3 ad{base, base + cells, base + 2 * cells, base + 3 * cells, base + 4 * cells, base + 5 * cells};
+  double* gA = base + 6 * cells;
+  double* gP = gA + ns1;
+  double* d_w = gP + ns1;
+  double* hist = d_w + box_n;
+  double* d_Jn = hist + hist_n;
+  long* d_cells = reinterpret_cast<long*>(base + n_doubles);
+  int* d_el = reinterpret_cast<int*>(d_cells + ns1);
+  C3(cudaMemsetAsync(buf, 0, n_doubles * sizeof(double), stream));
+  C3(cudaMemcpyAsync(d_w, w.data(), sizeof(double) * box_n, cudaMemcpyHostToDevice, stream));
+  if (ns > 0) {
+    C3(cudaMemcpyAsync(d_cells, src_list.data(), sizeof(long) * ns, cudaMemcpyHostToDevice, stream));
+    C3(cudaMemcpyAsync(d_el, src_elem.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, stream));
+  }
+  const d3::Box3 box{lo[0], lo[1], lo[2], bx, by, bz, d_w};
+  const int rb = (int)((box_n + 255) / 256);
+  // Forward, recording the focal p0 after every step.
+  std::vector<double> times((size_t)N + 1);
+  times[0] = tstep;
+  for (int n = 1; n <= N; n++) {
+    const crp_status st = step_once();
+    if (st != CRP_OK) return st;
+    double* out = hist + (size_t)(n - 1) * box_n;
+    if (mixed)
+      d3::adj3_record<F32c><<<rb, 256, 0, stream>>>(f, view<F32c>(px[cur_p]), view<F32c>(py[cur_p]),
+                                                      view<F32c>(pz[cur_p]), box, out);
+    else
+      d3::adj3_record<F64><<<rb, 256, 0, stream>>>(f, view<F64>(px[cur_p]), view<F64>(py[cur_p]),
+                                                     view<F64>(pz[cur_p]), box, out);
+    C3(cudaGetLastError());
+    launches++;
+    times[n] = tstep;
+  }
+  // Objective.
+  d3::adj3_objective<<<N, 256, 0, stream>>>(box, hist, d_Jn);
+  C3(cudaGetLastError());
+  std::vector<double> Jn(N);
+  C3(cudaMemcpyAsync(Jn.data(), d_Jn, sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
+  C3(cudaStreamSynchronize(stream));
+  double Jsum = 0.0;
+  for (int n = 0; n < N; n++) Jsum += Jn[n];
+  if (J) *J = g.dt * Jsum;
+  // Reverse sweep.
+  const long npos = (long)(f.X + 2) * (f.Y + 2) * (f.Z + 2);
+  const int gb = (int)((npos + 255) / 256), sb = (ns + 255) / 256;
+  const double two_dt = 2.0 * g.dt;
+  d3::adj3_force<<<rb, 256, 0, stream>>>(f, ad, box, hist + (size_t)(N - 1) * box_n, two_dt);
+  for (int n = N; n >= 1; n--) {
+    if (ns > 0) d3::adj3_source<<<sb, 256, 0, stream>>>(g, ad, d_cells, d_el, ns, times[n], gA, gP);
+    d3::adj3_faces<<<gb, 256, 0, stream>>>(g, ad);
+    d3::adj3_cells<<<gb, 256, 0, stream>>>(g, ad);
+    d3::adj3_vscale<<<gb, 256, 0, stream>>>(g, ad);
+    if (n >= 2) d3::adj3_force<<<rb, 256, 0, stream>>>(f, ad, box, hist + (size_t)(n - 2) * box_n, two_dt);
+    C3(cudaGetLastError());
+    launches += 5;
+  }
+  if (elem_n > 0 && ns > 0) {
+    std::vector<double> ca(ns), cp(ns);
+    C3(cudaMemcpyAsync(ca.data(), gA, sizeof(double) * ns, cudaMemcpyDeviceToHost, stream));
+    C3(cudaMemcpyAsync(cp.data(), gP, sizeof(double) * ns, cudaMemcpyDeviceToHost, stream));
+    C3(cudaStreamSynchronize(stream));
+    std::vector<double> sa(elem_n, 0.0), sp(elem_n, 0.0);
+    for (int c = 0; c < ns; c++) {
+      sa[src_elem[c]] += ca[c];
+      sp[src_elem[c]] += cp[c];
+    }
+    if (grad_amp) std::copy(sa.begin(), sa.end(), grad_amp);
+    if (grad_phase) std::copy(sp.begin(), sp.end(), grad_phase);
+  } else {
+    C3(cudaStreamSynchronize(stream));
+    if (grad_amp) std::fill(grad_amp, grad_amp + elem_n, 0.0);
+    if (grad_phase) std::fill(grad_phase, grad_phase + elem_n, 0.0);
+  }
+  stats.kernel_launches = launches;
+  return CRP_OK;
+}
+
 crp_status Sim3Impl::read_field(crp_field w, double* host) {
   const d3::Frame3& f = g.f;
   void* buf = nullptr;
@@ -1620,6 +1905,9 @@ crp_status sim3_set_tuning(Sim3Impl* s, const crp_tuning* t) {
   s->rp_blocks_req = t->rp_blocks;
   s->rp_grid = t->rp_blocks > 0 ? std::min(t->rp_blocks, s->rp_grid_full) : s->rp_grid_full;
   return CRP_OK;
+}
+crp_status sim3_adjoint(Sim3Impl* s, const crp_objective* obj, double* J, double* grad_amp, double* grad_phase) {
+  return s->adjoint(obj, J, grad_amp, grad_phase);
 }
 void sim3_get_tuning(const Sim3Impl* s, crp_tuning* t) {
   t->fdtd_rows = 8;

@@ -27,5 +27,6 @@ crp_status sim3_save_state(Sim3Impl* s, void* blob, std::vector<unsigned char>& 
 crp_status sim3_load_state(Sim3Impl* s, const void* blob, const std::vector<unsigned char>& host);
 crp_status sim3_set_tuning(Sim3Impl* s, const crp_tuning* t);
 void sim3_get_tuning(const Sim3Impl* s, crp_tuning* t);
+crp_status sim3_adjoint(Sim3Impl* s, const crp_objective* obj, double* J, double* grad_amp, double* grad_phase);
 
 }  // namespace crp

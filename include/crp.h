@@ -499,7 +499,12 @@ crp_status crp_batch_tune(crp_batch* batch, int32_t trial_steps, crp_batch_tunin
  * Supported: bubbles off, pressure sources (plane or focused), any PML faces;
  * otherwise CRP_ERR_UNSUPPORTED (the temperature branch, when on, runs with the
  * forward steps; it does not act on the pressure).  grad_amp and
- * grad_phase receive cfg.ext_elements values each (either may be NULL). */
+ * grad_phase receive cfg.ext_elements values each (either may be NULL).
+ * On a 3-D grid (ext.grid_z > 0, bubbles off) the focus is the point the
+ * bowl's phases aim at, w = dx dy dz (the bowl's source cells excluded), and
+ * the parameters are the ext.array_elements elements' amplitude factors and
+ * phases (crp_set_source_elements sets them; the phases are absolute there,
+ * the focusing delays included). */
 typedef struct crp_objective {
   int32_t steps;        /* mixture steps to run and differentiate over */
   double focal_radius;  /* [m] radius of the focal region around the source's focus */
