@@ -675,6 +675,7 @@ __global__ void __launch_bounds__(256) couple3(const __grid_constant__ Grid3 g, 
   if (i <= a.box[3] && j <= a.box[4] && k <= a.box[5]) {
     const long o = f.idx(i, j, k);
     double fgv;
+    bool same = false;  // the FDTD pass's pressure is already this cell's final value
     if (a.gather) {
       fgv = 0.0;
       for (int ci = 0; ci < 2; ci++)
@@ -689,11 +690,16 @@ __global__ void __launch_bounds__(256) couple3(const __grid_constant__ Grid3 g, 
             fgv += run;
           }
       fgv = G::stored(fgv);
-      a.fg.put(o, fgv);
+      // No bubble touches the cell and its void fraction was zero in the
+      // prediction and the step before: the gathered value is the stored 0
+      // and the pressure evaluation would repeat the FDTD pass's (no
+      // void-fraction rate), so the cell is left as it is.
+      same = fgv == 0.0 && a.fg.get(o) == 0.0 && a.fgn.get(o) == 0.0;
+      if (!same) a.fg.put(o, fgv);
     } else {
       fgv = a.fg.get(o);
     }
-    if (a.pressure && i >= 1 && i <= f.X && j >= 1 && j <= f.Y && k >= 1 && k <= f.Z) {
+    if (!same && a.pressure && i >= 1 && i <= f.X && j >= 1 && j <= f.Y && k >= 1 && k <= f.Z) {
       const double t_cur = a.tdev[1];
       const double h = void_half3(g, fgv, a.fgn.get(o));
       const long ox = o - 1, oy = o - f.pitch, oz = o - (long)(f.Y + 4) * f.pitch;
