@@ -37,6 +37,7 @@
 #include "crp_device.cuh"
 #include "radius.cuh"
 #include "rk45.cuh"
+#include "lpt.cuh"
 #include "sim3d.h"
 
 namespace crp {
@@ -539,7 +540,8 @@ template <typename P, bool RK>
 __global__ void __launch_bounds__(kRpThreads3) radius3(const __grid_constant__ Grid3 g,
                                                        const __grid_constant__ BubbleParams bp, Bub3 b,
                                                        const typename P::S px, const typename P::S py,
-                                                       const typename P::S pz, Scalars3* sc, int reuse) {
+                                                       const typename P::S pz, Scalars3* sc, int reuse,
+                                                       const int* __restrict__ order) {
   const double dt = g.dt;
   RpState s;
   RkState r;
@@ -557,13 +559,14 @@ __global__ void __launch_bounds__(kRpThreads3) radius3(const __grid_constant__ G
       base = __shfl_sync(0xffffffffu, base, leader);
       if (need & (1u << lane)) {
         const int q = base + __popc(need & ((1u << lane) - 1u));
-        const double PLp = q < b.n ? gather_pl3(g, bp, b, px, py, pz, q) : 0.0;
-        if (q >= b.n) {
+        const int bn = q < b.n ? (order ? order[q] : q) : -1;  // heaviest first once an order is built
+        const double PLp = bn >= 0 ? gather_pl3(g, bp, b, px, py, pz, bn) : 0.0;
+        if (bn < 0) {
           drained = true;
-        } else if (reuse && __double_as_longlong(PLp) == __double_as_longlong(b.PL_p[q])) {
+        } else if (reuse && __double_as_longlong(PLp) == __double_as_longlong(b.PL_p[bn])) {
           kept++;
         } else {
-          n = q;
+          n = bn;
           b.PL_p[n] = PLp;
           const double PLn = b.PL_n[n], PLm = b.PL_m[n];
           const double PC0 = PLn + bp.PL0, PC1 = 0.5 * (PLp - PLm) / dt,
@@ -949,6 +952,10 @@ struct Sim3Impl {
   double tstep = 0.0, tstepx = 0.0, t_prev = 0.0;
   double picard_tol = 1.0e-7f;
   bool bins_stale = true;
+  int* lpt_hist = nullptr;    // solve order (lpt.cuh): bucket counts, cursors, order
+  int* lpt_cursor = nullptr;
+  int* lpt_order = nullptr;
+  bool use_order = false;     // the order was built for this step's radius solves
   int rp_grid = 1;
   int rp_grid_full = 1;  // one lane per bubble, up to 4 blocks per SM
   int rp_blocks_req = 0;  // crp_set_tuning (0: rp_grid_full)
@@ -1018,6 +1025,9 @@ struct Sim3Impl {
       bin_start = carve<int>(nbins + 1, off, dry);
       bin_idx = carve<int>(std::max(n, 1), off, dry);
       bin_partial = carve<int>((nbins + d3::kScan - 1) / d3::kScan + 1, off, dry);
+      lpt_hist = carve<int>(kLptBuckets, off, dry);
+      lpt_cursor = carve<int>(kLptBuckets, off, dry);
+      lpt_order = carve<int>(n, off, dry);
     }
     return off;
   }
@@ -1038,6 +1048,7 @@ struct Sim3Impl {
   template <typename P>
   crp_status launch_couple(bool gather, bool pressure, const int box[6]);
   crp_status build_bins();
+  crp_status build_order();
   void bubble_box(int box[6]) const;
   static double as_double(unsigned long long b) {
     double d;
@@ -1453,17 +1464,30 @@ crp_status Sim3Impl::launch_move() {
   return CRP_OK;
 }
 
+crp_status Sim3Impl::build_order() {
+  const int n = bub.n;
+  lpt_count<<<(n + 255) / 256, 256, 0, stream>>>(bub.nsub, n, lpt_hist);
+  lpt_scan<<<1, 32, 0, stream>>>(lpt_hist, lpt_cursor);
+  lpt_scatter<<<(n + kLptScatterThreads - 1) / kLptScatterThreads, kLptScatterThreads, 0, stream>>>(
+      bub.nsub, n, lpt_cursor, lpt_order);
+  C3(cudaGetLastError());
+  launches += 3;
+  return CRP_OK;
+}
+
 template <typename P>
 crp_status Sim3Impl::launch_radius(int done) {
   using S = typename P::S;
   const int reuse = bp.reuse && done > 0 ? 1 : 0;
+  const int* order = use_order ? lpt_order : nullptr;
   C3(cudaMemsetAsync(&d_sc->next, 0, sizeof(int), stream));
   if (cfg.ext_rp_scheme == CRP_RP_RK45)
     d3::radius3<P, true><<<rp_grid, d3::kRpThreads3, 0, stream>>>(g, bp, bub, view<S>(px[cur_p]), view<S>(py[cur_p]),
-                                                                   view<S>(pz[cur_p]), d_sc, reuse);
+                                                                   view<S>(pz[cur_p]), d_sc, reuse, order);
   else
     d3::radius3<P, false><<<rp_grid, d3::kRpThreads3, 0, stream>>>(g, bp, bub, view<S>(px[cur_p]),
-                                                                    view<S>(py[cur_p]), view<S>(pz[cur_p]), d_sc, reuse);
+                                                                    view<S>(py[cur_p]), view<S>(pz[cur_p]), d_sc, reuse,
+                                                                    order);
   C3(cudaGetLastError());
   launches++;
   return CRP_OK;
@@ -1546,6 +1570,13 @@ crp_status Sim3Impl::step_once() {
   box_union(box, u1, u2);
   if (bub.n > 0 && res > picard_tol && bins_stale) {
     st = build_bins();
+    if (st != CRP_OK) return st;
+  }
+  // Heaviest-first solve order from the last solves' sub-step counts, once
+  // some bubble has needed more than the quiet phase's.
+  use_order = bub.n > 0 && res > picard_tol && h_sc->substep_max > kLptMinSubsteps;
+  if (use_order) {
+    st = build_order();
     if (st != CRP_OK) return st;
   }
   if (bub.n > 0) {
