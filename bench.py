@@ -390,25 +390,50 @@ def driven_sample(sim, args, cells, nb):
     return out
 
 
-def driven_rk45_sample(cfg, bub, args, cells, nb, ref_sim):
+def driven_rk45_sample(cfg, bub, args, cells, nb, ref_sim, rtol=1e-6, acc_sim=None, keep=False):
     """The driven sample of the same workload with the radius integrated by the
-    rk45 scheme (ext.rp_scheme = rk45, default tolerance), in the primary
+    rk45 scheme (ext.rp_scheme = rk45, relative tolerance rtol), in the primary
     precision: a fresh run taken untimed to the sample's start, then the same
     chunks timed one by one; its radii compared with the reference scheme's run
-    at the same step (the difference is the reference scheme's truncation
-    error, which the rk45 scheme's tolerance bounds far below)."""
+    at the same step (the difference is mostly the reference scheme's
+    truncation error) and, with acc_sim, with a tighter-tolerance rk45 run (this
+    run's own error).  keep: also return the simulation, left open."""
     import crp
 
     c = crp.Config.from_buffer_copy(cfg)
     c.ext_rp_scheme = 1
-    with crp.Sim(c, bub) as sim:
+    c.ext_rp_tol = rtol
+    sim = crp.Sim(c, bub)
+    try:
         out = driven_sample(sim, args, cells, nb)
-        out["scheme"] = "rk45"
-        out["rtol"] = c.ext_rp_tol or 1e-6
-        if ref_sim is not None and ref_sim.stats().steps == sim.stats().steps:
-            out["R_t_rel_l2_vs_reference_scheme"] = rel_l2(sim.bubbles("R_t"), ref_sim.bubbles("R_t"))
-            out["p0_rel_l2_vs_reference_scheme"] = rel_l2(sim.field("p0"), ref_sim.field("p0"))
-        return out
+    except Exception:
+        sim.close()
+        raise
+    out["scheme"] = "rk45"
+    out["rtol"] = rtol
+    steps = sim.stats().steps
+    if ref_sim is not None and ref_sim.stats().steps == steps:
+        out["R_t_rel_l2_vs_reference_scheme"] = rel_l2(sim.bubbles("R_t"), ref_sim.bubbles("R_t"))
+        out["p0_rel_l2_vs_reference_scheme"] = rel_l2(sim.field("p0"), ref_sim.field("p0"))
+    if acc_sim is not None and acc_sim.stats().steps == steps:
+        key = f"vs_rk45_rtol_{acc_sim._keep[0].ext_rp_tol:g}"
+        out["R_t_rel_l2_" + key] = rel_l2(sim.bubbles("R_t"), acc_sim.bubbles("R_t"))
+        out["p0_rel_l2_" + key] = rel_l2(sim.field("p0"), acc_sim.field("p0"))
+    if keep:
+        return out, sim
+    sim.close()
+    return out
+
+
+def driven_rk45_legs(cfg, bub, args, cells, nb, ref_sim):
+    """rk45 at its default tolerance (1e-6) and at 1e-4, the second compared
+    with the first: the accuracy a faster tolerance keeps."""
+    accurate, acc_sim = driven_rk45_sample(cfg, bub, args, cells, nb, ref_sim, 1e-6, keep=True)
+    try:
+        fast = guarded(driven_rk45_sample, cfg, bub, args, cells, nb, ref_sim, 1e-4, acc_sim)
+    finally:
+        acc_sim.close()
+    return accurate, fast
 
 
 def max_over_ranks(x, dist):
@@ -667,7 +692,8 @@ def run_ours(args, rank, world, dist):
     adjoint = (guarded(adjoint_cost3 if is3d(cfg) else adjoint_cost, cfg)
                if rank == 0 and world == 1 and not args.no_adjoint else None)
     driven = guarded(driven_sample, sim, args, cells, nb) if with_driven else None
-    driven_rk45 = guarded(driven_rk45_sample, cfg, bub, args, cells, nb, sim) if with_driven else None
+    legs = guarded(driven_rk45_legs, cfg, bub, args, cells, nb, sim) if with_driven else None
+    driven_rk45, driven_rk45_fast = legs if isinstance(legs, tuple) else (legs, None)
     focal = None
     if with_driven and all("sim" in r for r in runs.values()) and len(runs) > 1 and not is3d(cfg):
         focal = guarded(compare_at, {p: r["sim"] for p, r in runs.items()}, cfg)
@@ -694,7 +720,8 @@ def run_ours(args, rank, world, dist):
         result["config"]["bubbles"] = nb
         if prof_err:
             result["roofline"]["error"] = prof_err["error"]
-        for key, obj in (("driven", driven), ("driven_rk45", driven_rk45), ("e2e", e2e), ("adjoint", adjoint)):
+        for key, obj in (("driven", driven), ("driven_rk45", driven_rk45), ("driven_rk45_rtol_1e-4", driven_rk45_fast),
+                         ("e2e", e2e), ("adjoint", adjoint)):
             if obj is not None:
                 result[key] = obj
         for prec, r in runs.items():
