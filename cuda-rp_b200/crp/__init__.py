@@ -441,6 +441,9 @@ class _BatchSim(Sim):
         self.dims = Dims()
         self._check(self.lib.crp_get_dims(self.h, ctypes.byref(self.dims)))
         self.dims3 = None
+        if keep[0].ext_grid_z > 0:
+            self.dims3 = Dims3()
+            self._check(self.lib.crp_get_dims3(self.h, ctypes.byref(self.dims3)))
 
     def close(self):
         self.h = None

@@ -137,3 +137,25 @@ def test_batch_tune_restores_and_applies():
         assert batch.tuning.as_dict() == best.as_dict()
         batch.run([30] * 4)
         _equal(_batch_state(batch), want)
+
+
+def test_batch_with_a_3d_simulation():
+    """A 3-D simulation in a batch runs its host-driven steps beside the 2-D
+    simulations' graph-queued ones, with the same results as in thread mode."""
+    from test_cart3d import cfg3
+
+    c3 = cfg3(bubbles=100, tr_amp=0.3e6 / (998 * 1482))
+    cfgs = [_configs()[0], c3]
+    bubs = [None, crp.seed_bubbles3(c3)]
+    runs = []
+    for mode in (crp.BATCH_THREADS, crp.BATCH_GRAPHS):
+        with crp.Batch(cfgs, bubs) as batch:
+            t = batch.tuning
+            t.mode = mode
+            batch.tuning = t
+            batch.run([40, 40])
+            runs.append([batch.sims[0].field("p0"), batch.sims[1].field("p0"), batch.sims[1].bubbles("R_t"),
+                         batch.sims[1].stats().steps])
+    for a, b in zip(*runs):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
+    assert runs[0][3] == 40
