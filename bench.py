@@ -12,7 +12,7 @@ The timed window stays inside the quiet phase of the workload whatever W and K
 are (`window`): S = min(100, QUIET_END // (W + K + 1)), so mixture steps
 [W S, (W + K) S) plus one profiling chunk end before the burst drives the
 bubble cloud (QUIET_END: mixture step 1700 of the 1024 x 2048 workload, 900 of
-256 x 512).  Both BASELINE drives later grow the cloud until the mixture model
+256 x 512).  Both benchmark drives later grow the cloud until the mixture model
 stops converging (the Picard loop at step 2187 of 1024 x 2048, 1219 of
 256 x 512; the FP64 oracle does the same), so a window that reached there would
 time a failing run.  The "driven" object then continues the same run untimed to

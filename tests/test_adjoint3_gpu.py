@@ -14,7 +14,7 @@ import pytest
 
 import _bind as B
 import crp
-from test_cart3d import cfg3
+from test_cart3d import cart3d_small
 
 pytestmark = pytest.mark.gpu
 
@@ -25,7 +25,7 @@ H = 2e-4
 
 
 def _cfg(**over):
-    return cfg3(N=40, elems=ELEMS, **over)
+    return cart3d_small(N=40, elems=ELEMS, **over)
 
 
 def _params():

@@ -142,9 +142,9 @@ def test_batch_tune_restores_and_applies():
 def test_batch_with_a_3d_simulation():
     """A 3-D simulation in a batch runs its host-driven steps beside the 2-D
     simulations' graph-queued ones, with the same results as in thread mode."""
-    from test_cart3d import cfg3
+    from test_cart3d import cart3d_small
 
-    c3 = cfg3(bubbles=100, tr_amp=0.3e6 / (998 * 1482))
+    c3 = cart3d_small(bubbles=100, tr_amp=0.3e6 / (998 * 1482))
     cfgs = [_configs()[0], c3]
     bubs = [None, crp.seed_bubbles3(c3)]
     runs = []

@@ -1,6 +1,6 @@
-"""Parity on the benchmark's own configurations, not only on small grids.
+"""Parity on the benchmark's own workloads, not only on small grids.
 
-Configuration 1 (axisym_256x512: 256 x 512 axisymmetric grid, 4096 seeded
+The 256 x 512 workload (axisym_256x512: 256 x 512 axisymmetric grid, 4096 seeded
 bubbles, 0.5 MPa focused burst) is run from t = 0 on the CUDA path in FP64 and
 in the mixed form, and on the FP64 oracle, in lockstep, until each stops.  The
 drive grows the bubble cloud until the mixture model stops converging; the
@@ -15,7 +15,7 @@ is 5e-7 at the focal arrival and 4e-5 fifty steps later (the 1e-4 target), and
 grows past it from step 1060; it stops at step 1172 (its Picard threshold is
 1e-5, since FP32 storage of f_g leaves a residual floor near 7e-7).
 
-Configuration 2 (axisym_1024x2048, 262144 bubbles) is compared over a bounded
+The 1024 x 2048 workload (axisym_1024x2048, 262144 bubbles) is compared over a bounded
 window from t = 0, the oracle's time being about 0.1 s per step.
 """
 import os
@@ -50,8 +50,8 @@ def focal_mask(dims, cfg, radius=2e-3):
 
 
 @pytest.fixture(scope="module")
-def cfg1_run():
-    """Lockstep run of configuration 1: errors at checkpoints and the steps at
+def run_256x512():
+    """Lockstep run of the 256 x 512 workload: errors at checkpoints and the steps at
     which each path stopped."""
     path = os.path.join(CONF, "axisym_256x512.conf")
     cfg = crp.parse_file(path)
@@ -93,39 +93,39 @@ def cfg1_run():
         for name in ("fp64", "mixed"):
             sims[name].close()
         oracle.close()
-    print("cfg1 checkpoints", records, "stopped", stopped)
+    print("256x512 checkpoints", records, "stopped", stopped)
     return {"records": records, "stopped": stopped, "status": status}
 
 
-def test_cfg1_fp64_matches_oracle_through_focal_arrival(cfg1_run):
+def test_256x512_fp64_matches_oracle_through_focal_arrival(run_256x512):
     for step in (500, FOCAL_ARRIVAL):
-        r = cfg1_run["records"][step]["fp64"]
+        r = run_256x512["records"][step]["fp64"]
         assert r["p0"] < TOL and r["vx"] < TOL and r["R_t"] < TOL, (step, r)
-        assert r["picard"] == cfg1_run["records"][step]["picard_oracle"]
+        assert r["picard"] == run_256x512["records"][step]["picard_oracle"]
 
 
-def test_cfg1_driven_phase_stays_close_until_the_cloud_amplifies(cfg1_run):
+def test_256x512_driven_phase_stays_close_until_the_cloud_amplifies(run_256x512):
     # 100 steps after the arrival the driven cloud has amplified rounding
     # differences by about 1e3 (measured 5e-8); still far below the physics.
-    r = cfg1_run["records"][1100]["fp64"]
+    r = run_256x512["records"][1100]["fp64"]
     assert r["p0"] < 1e-5 and r["R_t"] < 1e-5, r
-    assert abs(r["picard"] - cfg1_run["records"][1100]["picard_oracle"]) <= 2
+    assert abs(r["picard"] - run_256x512["records"][1100]["picard_oracle"]) <= 2
 
 
-def test_cfg1_cuda_and_oracle_stop_at_the_same_step(cfg1_run):
-    st, code = cfg1_run["stopped"], cfg1_run["status"]
+def test_256x512_cuda_and_oracle_stop_at_the_same_step(run_256x512):
+    st, code = run_256x512["stopped"], run_256x512["status"]
     assert "fp64" in st and "oracle" in st, st
     assert code["fp64"] == 6 and code["oracle"] == 6  # CRP_ERR_PICARD
     assert st["fp64"] == st["oracle"], st
 
 
-def test_cfg1_mixed_focal_error_at_arrival(cfg1_run):
+def test_256x512_mixed_focal_error_at_arrival(run_256x512):
     for step in (FOCAL_ARRIVAL, 1050):
-        r = cfg1_run["records"][step]["mixed"]
+        r = run_256x512["records"][step]["mixed"]
         assert r["focal_l2"] < 1e-4, (step, r)
 
 
-def test_cfg2_fp64_window_matches_oracle():
+def test_1024x2048_fp64_window_matches_oracle():
     path = os.path.join(CONF, "axisym_1024x2048.conf")
     cfg = crp.parse_file(path)
     ocfg = B.oracle_parse_file(path)
@@ -142,7 +142,7 @@ def test_cfg2_fp64_window_matches_oracle():
                         "vy": rel_max(gpu.field("vy"), oracle.field("vy"), 1e-9),
                         "f_g": rel_max(gpu.field("f_g"), oracle.field("f_g"), 1e-12),
                         "R_t": rel_max(gpu.bubbles("R_t"), oracle.bubbles("R_t"), 1e-9)}
-                print("cfg2 step", gpu.stats().steps, errs)
+                print("1024x2048 step", gpu.stats().steps, errs)
                 assert all(v < TOL for v in errs.values()), errs
                 assert gpu.stats().picard_total == oracle.stats().picard_total
     finally:

@@ -13,7 +13,7 @@ import crp
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def cfg3(N=40, h=2e-4, elems=32, bubbles=0, **over):
+def cart3d_small(N=40, h=2e-4, elems=32, bubbles=0, **over):
     """A small 3-D case: N^3 cells of h, a PML of 6 cells on every face, a bowl
     of `elems` elements 7 cells inside the PML, 1 MHz, 0.2 MPa."""
     c = crp.Config()
@@ -38,7 +38,7 @@ def cfg3(N=40, h=2e-4, elems=32, bubbles=0, **over):
 
 @pytest.mark.parametrize("dx_focus", [0.0, 1.0e-3])
 def test_bowl_focuses_at_its_focus(dx_focus):
-    c = cfg3(ext_array_focus_dx=dx_focus)
+    c = cart3d_small(ext_array_focus_dx=dx_focus)
     o = B.OracleSim3(c)
     assert o.dims3.source_cells > 100
     peak = np.zeros(o.field("p0").shape)
@@ -55,7 +55,7 @@ def test_bowl_focuses_at_its_focus(dx_focus):
 
 
 def test_void_fraction_conservation_3d():
-    c = cfg3(bubbles=300)
+    c = cart3d_small(bubbles=300)
     o = B.OracleSim3(c, B.oracle_seed_bubbles3(c))
     fg = o.field("f_g")
     R, nb = o.bubbles("R_t"), o.bubbles("n_B")
@@ -66,14 +66,14 @@ def test_void_fraction_conservation_3d():
 
 @pytest.mark.parametrize("shape", [0, 1, 2])
 def test_seeding3_matches(shape):
-    c = cfg3(bubbles=2049, ext_cloud_shape=shape, ext_cloud_h=2e-3, ext_array_focus_dx=5e-4)
+    c = cart3d_small(bubbles=2049, ext_cloud_shape=shape, ext_cloud_h=2e-3, ext_array_focus_dx=5e-4)
     a, b = crp.seed_bubbles3(c), B.oracle_seed_bubbles3(c)
     for u, v in zip((a.x, a.y, a.z, a.r0, a.n_b), (b.x, b.y, b.z, b.r0, b.n_b)):
         assert np.array_equal(u.view(np.uint64), v.view(np.uint64))
 
 
 def test_3d_bubbles_at_rest_stay():
-    c = cfg3(bubbles=100, tr_amp=0.0)
+    c = cart3d_small(bubbles=100, tr_amp=0.0)
     o = B.OracleSim3(c, B.oracle_seed_bubbles3(c))
     o.step(30)
     R, R0 = o.bubbles("R_t"), o.bubbles("R0")

@@ -7,7 +7,7 @@ import pytest
 
 import _bind as B
 import crp
-from test_cart3d import cfg3
+from test_cart3d import cart3d_small
 from test_mixed_gpu import TOL_BUBBLE, TOL_FIELD, rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -58,7 +58,7 @@ def test_3d_fp64_matches_oracle(name):
     over, nb, steps = CASES[name]
     over = dict(over)
     N = over.pop("N", 40)
-    cfg = cfg3(N=N, bubbles=nb, **over)
+    cfg = cart3d_small(N=N, bubbles=nb, **over)
     bub = crp.seed_bubbles3(cfg) if nb else None
     cpu = B.OracleSim3(cfg, bub)
     with crp.Sim(cfg, bub) as gpu:
@@ -80,7 +80,7 @@ def test_3d_mixed_matches_oracle():
     # the cloud to collapse at 0.2 MPa and above, and a collapsing cloud
     # amplifies the FP32 void-fraction storage error (6e-8) as it amplifies
     # FP64 rounding (1e5-fold over 70 steps, measured): 8e-4 at 0.2 MPa.
-    cfg = cfg3(bubbles=300, tr_amp=0.05e6 / (998 * 1482))
+    cfg = cart3d_small(bubbles=300, tr_amp=0.05e6 / (998 * 1482))
     bub = crp.seed_bubbles3(cfg)
     cpu = B.OracleSim3(cfg, bub)
     cpu.step(70)
@@ -95,7 +95,7 @@ def test_3d_mixed_matches_oracle():
 
 
 def test_3d_is_deterministic():
-    cfg = cfg3(bubbles=300, tr_amp=1.0e6 / (998 * 1482))
+    cfg = cart3d_small(bubbles=300, tr_amp=1.0e6 / (998 * 1482))
     bub = crp.seed_bubbles3(cfg)
     out = []
     for _ in range(2):

@@ -10,7 +10,7 @@ import pytest
 
 import _bind as B
 import crp
-from test_cart3d import cfg3
+from test_cart3d import cart3d_small
 from test_parity_gpu import CASES
 
 pytestmark = pytest.mark.gpu
@@ -64,7 +64,7 @@ def test_reuse_is_bit_exact_2d(name, prec, scheme, graphs):
 def test_reuse_is_bit_exact_3d(prec, scheme):
     res = []
     for reuse in (0, 1):
-        cfg = cfg3(bubbles=300, tr_amp=0.6e6 / (998 * 1482), ext_precision=prec, ext_rp_scheme=scheme,
+        cfg = cart3d_small(bubbles=300, tr_amp=0.6e6 / (998 * 1482), ext_precision=prec, ext_rp_scheme=scheme,
                    ext_rp_reuse=reuse)
         res.append(_run(cfg, 70, crp.seed_bubbles3(cfg)))
     r_off, r_on = _same(*res)

@@ -8,7 +8,7 @@ import pytest
 
 import _bind as B
 import crp
-from test_cart3d import cfg3
+from test_cart3d import cart3d_small
 from test_parity_gpu import CASES
 
 pytestmark = pytest.mark.gpu
@@ -78,7 +78,7 @@ def test_temperature_branch_and_focus_history():
 
 @pytest.mark.parametrize("prec", [0, 1])
 def test_3d_load_continues_bit_for_bit(prec):
-    cfg = cfg3(bubbles=300, tr_amp=0.6e6 / (998 * 1482), ext_precision=prec)
+    cfg = cart3d_small(bubbles=300, tr_amp=0.6e6 / (998 * 1482), ext_precision=prec)
     bub = crp.seed_bubbles3(cfg)
     with crp.Sim(cfg, bub) as sim:
         sim.step(30)
