@@ -1880,8 +1880,8 @@ struct Sim {
   }
 
   // Tensor maps (2-D, the whole frame, boxes of kBoxX x kBoxY) of
-  // every field buffer, for the TMA-fed FDTD pass.  The encoder is the driver's
-  // cuTensorMapEncodeTiled, reached through the runtime's entry-point query.
+  // every field buffer, for the TMA-fed FDTD pass.  The encoder is the CUDA
+  // driver API's cuTensorMapEncodeTiled, reached through the runtime's entry-point query.
   crp_status make_tensor_maps() {
     using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,

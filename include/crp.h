@@ -39,7 +39,7 @@ extern "C" {
 typedef enum crp_status {
   CRP_OK = 0,
   CRP_ERR_INVALID = 1,      /* bad argument or configuration value */
-  CRP_ERR_UNSUPPORTED = 2,  /* configuration outside what this build implements */
+  CRP_ERR_UNSUPPORTED = 2,  /* configuration outside what this library implements */
   CRP_ERR_CUDA = 3,         /* a CUDA runtime call failed; see crp_last_error */
   CRP_ERR_ALLOC = 4,        /* device or host allocation failed */
   CRP_ERR_RP_STEPS = 5,     /* a bubble exceeded the Rayleigh–Plesset sub-step cap */

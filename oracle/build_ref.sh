@@ -1,7 +1,7 @@
 #!/usr/bin/env bash
 # Builds oracle/_ref/libcrp_ref.so from the reference's own sources, where they
 # lie, plus the stand-in headers in oracle/ref_stubs and the harness in
-# oracle/ref_harness.inc.  Test infrastructure only (the checker); nothing in
+# oracle/ref_harness.inc.  Test infrastructure only; nothing in
 # the product links it.  Output goes to oracle/_ref/ only.
 #
 # Usage: oracle/build_ref.sh [REFERENCE_ROOT]

@@ -2,7 +2,7 @@
  *
  * An FP64 host restatement of the reference's initialisers, kernels and main
  * loop (src/bubble_CUDA.cu, inc/bubble_CUDA_kernel.cuh, inc/complex.cuh,
- * inc/double_vector_math.cuh), used by the tests as the checker and by
+ * inc/double_vector_math.cuh), used by the tests to check the CUDA path and by
  * bench.py as the timed CPU baseline.  The product never links or calls it.
  *
  * Parity pin: the initialisers and bubble-physics functions are compared
