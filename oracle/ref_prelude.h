@@ -2,7 +2,8 @@
  * which pulls in inc/bubble_CUDA_kernel.cuh) with CUDA 12.9 for sm_100a.
  *
  * Test infrastructure only: the library built from it (oracle/_ref/libcrp_ref.so)
- * pins the oracle and the CUDA path to the reference's own arithmetic.  It is never linked into the product.
+ * pins the oracle and the CUDA path to the reference's own arithmetic.  It is
+ * never linked into the product.
  *
  * Two incompatibilities between the 2010-era reference and CUDA 12.9 are
  * neutralised here without touching the reference's text:
