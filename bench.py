@@ -555,23 +555,33 @@ def focal_compare_step(cfg):
 
 
 def compare_at(sims, cfg):
-    """Advance the FP64 and mixed simulations (untimed) to focal_compare_step and
-    compare the mixed p0 with the FP64 p0 over the grid and within 2 mm of the
-    focus, and the bubble radii."""
+    """Advance the FP64 and mixed simulations (untimed) to the focal arrival and
+    50 and 100 steps after it (focal_compare_step), comparing the mixed p0 with
+    the FP64 p0 over the grid and within 2 mm of the focus, and the bubble radii,
+    at each; the last comparison is the result, the earlier ones its history."""
     import crp
 
-    step = max(max(int(s.stats().steps) for s in sims.values()), focal_compare_step(cfg))
-    for prec, sim in sims.items():
-        try:
-            if sim.stats().steps < step:
-                sim.step(step - int(sim.stats().steps))
-        except crp.CrpError as e:
-            return {"at_step": step, "error": f"{prec} path: {e}"}
-    a, b = sims["mixed"].field("p0"), sims["fp64"].field("p0")
-    m = focal_mask(sims["fp64"], cfg)
-    return {"at_step": step, "p0_rel_l2": rel_l2(a, b), "p0_focal_rel_l2": rel_l2(a[m], b[m]),
-            "p0_focal_max_pa": float(np.max(np.abs(b[m]))),
-            "R_t_rel_l2": rel_l2(sims["mixed"].bubbles("R_t"), sims["fp64"].bubbles("R_t"))}
+    last = focal_compare_step(cfg)
+    history = []
+    for step in (last - 100, last - 50, last):
+        step = max(step, max(int(s.stats().steps) for s in sims.values()))
+        for prec, sim in sims.items():
+            try:
+                if sim.stats().steps < step:
+                    sim.step(step - int(sim.stats().steps))
+            except crp.CrpError as e:
+                out = {"at_step": step, "error": f"{prec} path: {e}"}
+                if history:
+                    out["history"] = history
+                return out
+        a, b = sims["mixed"].field("p0"), sims["fp64"].field("p0")
+        m = focal_mask(sims["fp64"], cfg)
+        history.append({"at_step": step, "p0_rel_l2": rel_l2(a, b), "p0_focal_rel_l2": rel_l2(a[m], b[m]),
+                        "p0_focal_max_pa": float(np.max(np.abs(b[m]))),
+                        "R_t_rel_l2": rel_l2(sims["mixed"].bubbles("R_t"), sims["fp64"].bubbles("R_t"))})
+    out = dict(history[-1])
+    out["history"] = history[:-1]
+    return out
 
 
 def rel_l2(a, b):
