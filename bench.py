@@ -129,7 +129,7 @@ def window(workload, warmup, steps, chunk=None):
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
-    def __init__(self, gpu_index: int, period_ms: int = 50):
+    def __init__(self, gpu_index: int, period_ms: int = 20):
         self.gpu = gpu_index
         self.period = period_ms
         self.samples = []
