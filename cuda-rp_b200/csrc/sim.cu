@@ -2114,24 +2114,65 @@ struct Sim {
     return CRP_OK;
   }
 
-  crp_status step_once() {
-    // Compensated time sum, src/bubble_CUDA.cu:208-212.
+  // The first part of every step: the step's times (compensated sum,
+  // src/bubble_CUDA.cu:208-212), set_time and the FDTD pass, with the buffer
+  // rotations.
+  cudaError_t queue_fdtd_step() {
     t_prev = tstep;
     double s1 = tstep;
     tstep = tstep + gp.dt + tstepx;
     double s2 = tstep - s1;
     tstepx = gp.dt + tstepx - s2;
-    CRP_CUDA(launch(kClassOther, [&] { set_time<<<1, 1, 0, stream>>>(d_scalars, t_prev, tstep, tstepx); }));
-
+    cudaError_t e = launch(kClassOther, [&] { set_time<<<1, 1, 0, stream>>>(d_scalars, t_prev, tstep, tstepx); });
+    if (e != cudaSuccess) return e;
     const int nv = cur_v ^ 1, np = cur_p ^ 1;
     // Ring rotation of store_variables: the predicted f_g goes to the f_gm buffer.
     const int a = fg_a, b = fg_b, c = fg_c;
-    CRP_CUDA(mixed ? launch_fdtd<PrecMixed>(nv, np, a, b, c) : launch_fdtd<PrecFP64>(nv, np, a, b, c));
+    e = mixed ? launch_fdtd<PrecMixed>(nv, np, a, b, c) : launch_fdtd<PrecFP64>(nv, np, a, b, c);
+    if (e != cudaSuccess) return e;
     cur_v = nv;
     cur_p = np;
     fg_a = c;  // predicted f_g
     fg_b = a;  // f_gn
     fg_c = b;  // f_gm
+    return cudaSuccess;
+  }
+
+  // Steps of a simulation without bubbles (no temperature branch, profiling or
+  // Picard trace): nothing the host decides depends on a step's scalars, so
+  // queue_plain queues the steps back to back and finish_plain reads the
+  // scalars once, after the last.  The FDTD pass's error flag is sticky and
+  // a non-finite pressure stays non-finite in the linear bubble-free step, so
+  // the last step's scalars carry what step_once would have found at any step.
+  bool plain_ok() const { return hs.nb == 0 && !temperature_on && !prof.on && !debug_picard && stats.steps > 0; }
+  crp_status queue_plain() {
+    CRP_CUDA(queue_fdtd_step());
+    // The support boxes as step_once leaves them without bubbles.
+    const Box snow = box_union(supp[0], box_union(supp[1], supp[2]));
+    couple_box = box_union(box_union(Box{1, 1, 0, 0}, supp[0]), box_union(supp[1], supp[2]));
+    supp[2] = supp[1];
+    supp[1] = supp[0];
+    supp[0] = snow;
+    stats.steps++;
+    stats.time = tstep;
+    stats.picard_last = 0;
+    return CRP_OK;
+  }
+  crp_status finish_plain() {
+    CRP_CUDA(cudaMemcpyAsync(h_scalars, d_scalars, sizeof(Scalars), cudaMemcpyDeviceToHost, stream));
+    CRP_CUDA(wait_stream());
+    if (h_scalars->pipe_err) return fail(CRP_ERR_CUDA, "an mbarrier wait of the FDTD pass timed out");
+    const double resimax = __longlong_as_double_host(h_scalars->residual) / gp.P_inf;
+    if (std::isnan(resimax)) return fail(CRP_ERR_NONFINITE, "non-finite pressure");
+    stats.residual_last = resimax;
+    stats.rp_substeps_max = h_scalars->substep_max;
+    stats.rp_reused = (int64_t)h_scalars->reused;
+    fill_launch_stats();
+    return CRP_OK;
+  }
+
+  crp_status step_once() {
+    CRP_CUDA(queue_fdtd_step());
     if (hs.nb > 0) CRP_CUDA(mixed ? launch_move<PrecMixed>() : launch_move<PrecFP64>());
     // The first radius solve is queued right behind the read-back of the
     // prediction's scalars, and picard_gate decides on the device whether it
@@ -2536,6 +2577,13 @@ struct Sim {
     if (pst != CRP_OK) return pst;
     int k = 0;
     while (k < n && (stats.steps == 0 || prof.on || !graphs_on || hs.nb == 0 || debug_picard || temperature_on)) {
+      if (plain_ok()) {
+        for (; k < n; k++) {
+          const crp_status st = queue_plain();
+          if (st != CRP_OK) return st;
+        }
+        return finish_plain();
+      }
       const crp_status st = step_once();
       if (st != CRP_OK) return st;
       k++;
@@ -2938,8 +2986,33 @@ struct Sim {
     return CRP_OK;
   }
 
+  // crp_adjoint's device workspace: kept for the next call (an optimisation
+  // loop calls it over and over) and released with the simulation, so that a
+  // call neither waits for a device-wide free nor pays for a new allocation.
+  void* adj_ws = nullptr;
+  size_t adj_ws_bytes = 0;
+  crp_status adjoint_workspace(size_t bytes, void** out) {
+    if (adj_ws_bytes < bytes) {
+      if (adj_ws) {
+        CRP_CUDA(cudaStreamSynchronize(stream));
+        cudaFree(adj_ws);
+        adj_ws = nullptr;
+        adj_ws_bytes = 0;
+      }
+      if (cudaMalloc(&adj_ws, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        adj_ws = nullptr;
+        return fail(CRP_ERR_ALLOC, "adjoint: device memory");
+      }
+      adj_ws_bytes = bytes;
+    }
+    *out = adj_ws;
+    return CRP_OK;
+  }
+
   ~Sim() {
     drop_graphs();
+    if (adj_ws) cudaFree(adj_ws);
     if (cap_stream) cudaStreamDestroy(cap_stream);
     if (h_push) cudaFreeHost(h_push);
     if (pool) cudaFree(pool);
@@ -3046,8 +3119,8 @@ cudaError_t Sim::launch_couple_t(bool pressure) {
 }
 
 // crp_adjoint: obj->steps forward steps recording the focal p0, the
-// objective, then the reverse sweep of adj_faces / adj_cells / adj_force
-// (adjoint.cuh) and the per-element sums of the per-column gradients.
+// objective, then the reverse sweep (adj_force for the last step, one adj_step
+// per step, adjoint.cuh) and the per-element sums of the per-column gradients.
 crp_status Sim::adjoint(const crp_objective* obj, double* J, double* grad_amp, double* grad_phase) {
   if (!obj || obj->steps <= 0 || !(obj->focal_radius > 0.0))
     return fail(CRP_ERR_INVALID, "adjoint: steps > 0 and focal_radius > 0 are required");
@@ -3079,35 +3152,30 @@ crp_status Sim::adjoint(const crp_objective* obj, double* J, double* grad_amp, d
       if ((xm - cx) * (xm - cx) + (ym - cy) * (ym - cy) > r * r) continue;
       w[(size_t)jj * bw + ii] = gp.cyl ? 2.0 * pi * xm * gp.dx * gp.dy : gp.dx * gp.dy;
     }
-  // Device buffers: six adjoint frames, two per-column gradients, weights,
-  // the focal history and the per-step objective.
+  // Device buffers: two sets of four adjoint frames, two per-column
+  // gradients, weights, the focal history and the per-step objective.
   const size_t hist_n = (size_t)N * cells_box;
   if (hist_n * sizeof(double) > ((size_t)32 << 30))
     return fail(CRP_ERR_TOO_LARGE, "adjoint: focal history above 32 GiB (steps x focal cells)");
-  const size_t n_doubles = 6 * cells + 2 * (size_t)(X + 2) + cells_box + hist_n + (size_t)N;
+  const size_t n_doubles = 8 * cells + 2 * (size_t)(X + 2) + cells_box + hist_n + (size_t)N;
   double* buf = nullptr;
-  if (cudaMalloc(&buf, n_doubles * sizeof(double)) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(CRP_ERR_ALLOC, "adjoint: device memory");
+  {
+    const crp_status ws = adjoint_workspace(n_doubles * sizeof(double), reinterpret_cast<void**>(&buf));
+    if (ws != CRP_OK) return ws;
   }
-  struct Free {  // on every return: let the queued work finish, then release the buffers
-    double* p;
+  struct Drain {  // on every return: the queued work has finished
     cudaStream_t st;
-    ~Free() {
-      cudaStreamSynchronize(st);
-      cudaFree(p);
-    }
-  } guard{buf, stream};
-  AdjBuffers ab;
-  ab.LX = buf;
-  ab.LY = ab.LX + cells;
-  ab.LXt = ab.LY + cells;
-  ab.LYt = ab.LXt + cells;
-  ab.MX = ab.LYt + cells;
-  ab.MY = ab.MX + cells;
-  ab.gA = ab.MY + cells;
-  ab.gP = ab.gA + (X + 2);
-  double* d_w = ab.gP + (X + 2);
+    ~Drain() { cudaStreamSynchronize(st); }
+  } guard{stream};
+  AdjFrames fr[2];
+  for (int s = 0; s < 2; s++) {
+    double* base = buf + (size_t)s * 4 * cells;
+    fr[s] = AdjFrames{base, base + cells, base + 2 * cells, base + 3 * cells};
+  }
+  AdjGrad gr;
+  gr.gA = buf + 8 * cells;
+  gr.gP = gr.gA + (X + 2);
+  double* d_w = gr.gP + (X + 2);
   double* hist = d_w + cells_box;
   double* d_Jn = hist + hist_n;
   CRP_CUDA(cudaMemsetAsync(buf, 0, n_doubles * sizeof(double), stream));
@@ -3117,9 +3185,12 @@ crp_status Sim::adjoint(const crp_objective* obj, double* J, double* grad_amp, d
   // Forward, recording the focal p0 after every step.
   std::vector<double> times((size_t)N + 1);
   times[0] = tstep;
+  bool queued = false;  // steps queued by queue_plain, checked by finish_plain
   for (int n = 1; n <= N; n++) {
-    const crp_status st = step_once();
+    const bool plain = plain_ok();
+    const crp_status st = plain ? queue_plain() : step_once();
     if (st != CRP_OK) return st;
+    queued = queued || plain;
     double* out = hist + (size_t)(n - 1) * cells_box;
     cudaError_t e;
     if (mixed) {
@@ -3132,6 +3203,10 @@ crp_status Sim::adjoint(const crp_objective* obj, double* J, double* grad_amp, d
     CRP_CUDA(e);
     times[n] = tstep;
   }
+  if (queued) {
+    const crp_status st = finish_plain();
+    if (st != CRP_OK) return st;
+  }
   // Objective.
   CRP_CUDA(launch(kClassOther, [&] { adj_objective<<<N, kAdjSumThreads, 0, stream>>>(box, hist, d_Jn); }));
   std::vector<double> Jn(N);
@@ -3140,23 +3215,20 @@ crp_status Sim::adjoint(const crp_objective* obj, double* J, double* grad_amp, d
   double Jsum = 0.0;
   for (int n = 0; n < N; n++) Jsum += Jn[n];
   if (J) *J = gp.dt * Jsum;
-  // Reverse sweep.
-  const dim3 blk(32, 8);
-  const dim3 gfaces((X + 2 + 31) / 32, (Y + 2 + 7) / 8), gcells((X + 31) / 32, (Y + 7) / 8);
-  CRP_CUDA(launch(kClassOther, [&] { adj_force<<<rb, 256, 0, stream>>>(gp, ab, box, hist + (size_t)(N - 1) * cells_box); }));
-  for (int n = N; n >= 1; n--) {
-    CRP_CUDA(launch(kClassOther, [&] { adj_faces<<<gfaces, blk, 0, stream>>>(gp, ab); }));
+  // Reverse sweep: reverse step n reads frame set s and writes set s ^ 1.
+  const dim3 blk(32, 8), gcells((X + 31) / 32, (Y + 7) / 8);
+  CRP_CUDA(launch(kClassOther, [&] { adj_force<<<rb, 256, 0, stream>>>(gp, fr[0], box, hist + (size_t)(N - 1) * cells_box); }));
+  int s = 0;
+  for (int n = N; n >= 1; n--, s ^= 1) {
     const double t_src = times[n - 1];
-    CRP_CUDA(launch(kClassOther, [&] { adj_cells<<<gcells, blk, 0, stream>>>(gp, ab, t_src); }));
-    if (n >= 2) {
-      const double* p0 = hist + (size_t)(n - 2) * cells_box;
-      CRP_CUDA(launch(kClassOther, [&] { adj_force<<<rb, 256, 0, stream>>>(gp, ab, box, p0); }));
-    }
+    const double* p0 = n >= 2 ? hist + (size_t)(n - 2) * cells_box : nullptr;
+    CRP_CUDA(launch(kClassOther,
+                    [&] { adj_step<<<gcells, blk, 0, stream>>>(gp, fr[s], fr[s ^ 1], gr, t_src, box, p0); }));
   }
   if (gp.elem_n > 0) {
     std::vector<double> gA(X + 2), gPh(X + 2);
-    CRP_CUDA(cudaMemcpyAsync(gA.data(), ab.gA, sizeof(double) * (X + 2), cudaMemcpyDeviceToHost, stream));
-    CRP_CUDA(cudaMemcpyAsync(gPh.data(), ab.gP, sizeof(double) * (X + 2), cudaMemcpyDeviceToHost, stream));
+    CRP_CUDA(cudaMemcpyAsync(gA.data(), gr.gA, sizeof(double) * (X + 2), cudaMemcpyDeviceToHost, stream));
+    CRP_CUDA(cudaMemcpyAsync(gPh.data(), gr.gP, sizeof(double) * (X + 2), cudaMemcpyDeviceToHost, stream));
     CRP_CUDA(cudaStreamSynchronize(stream));
     const int ne = gp.elem_n;
     std::vector<double> sa(ne, 0.0), sp(ne, 0.0);

@@ -789,11 +789,16 @@ struct PMix {
 // with p0 = px + py + pz (0 in the ghost cells, which are never written).  The
 // reverse of one step, given the adjoint of the state after it:
 //   1. adj3_source: the source cells' share of the gradient, their adjoint zeroed;
-//   2. adj3_faces:  the face adjoints take the pressure update's transpose;
-//   3. adj3_cells:  component adjoints pa_c M_c plus the velocity update's
-//                   transpose into p0 (the same for all three components);
-//   4. adj3_vscale: the face adjoints times va vb;
-// then adj3_force adds 2 dt w p0 of the step before for the focal cells.
+//   2. adj3_step, one pass from one set of adjoint frames into the other:
+//      the face adjoints take the pressure update's transpose; the component
+//      adjoints become pa_c M_c plus the velocity update's transpose into p0
+//      (the same for all three components); the face adjoints are multiplied
+//      by va vb; and 2 dt w p0 of the step before is added for the focal cells
+//      (adj3_force adds the last step's before the sweep).
+// Each cell forms the transposed values of its six faces (its west, south and
+// bottom faces by the same expression as the neighbour that owns them), so a
+// step reads 6 doubles per cell (L and M; neighbours through L1/L2) and
+// writes 6: 96 bytes.
 struct Adj3 {
   double *LX, *LY, *LZ;  // adjoints of vx, vy, vz (frame layout)
   double *MX, *MY, *MZ;  // adjoints of px, py, pz
@@ -802,16 +807,6 @@ struct Box3 {
   int i0, j0, k0, nx, ny, nz;
   const double* w;  // weight of each box cell (0 outside the focal sphere)
 };
-
-__device__ __forceinline__ bool frame_pos(const Frame3& f, long t, int& i, int& j, int& k) {
-  // t over (X+2)(Y+2)(Z+2) positions: i, j, k in [0, N+1].
-  const long nx = f.X + 2, ny = f.Y + 2;
-  if (t >= nx * ny * (long)(f.Z + 2)) return false;
-  i = (int)(t % nx);
-  j = (int)((t / nx) % ny);
-  k = (int)(t / (nx * ny));
-  return true;
-}
 
 template <typename S>
 __global__ void adj3_record(const Frame3 f, const S px, const S py, const S pz, const Box3 b, double* out) {
@@ -875,45 +870,67 @@ __global__ void adj3_source(const __grid_constant__ Grid3 g, const Adj3 a, const
   gP[c] += m * env * g.elem_amp[e] * cs;
 }
 
-// Computed faces: vx for i in [0, X] (j, k interior), vy for j in [0, Y], vz for k in [0, Z].
-__global__ void adj3_faces(const __grid_constant__ Grid3 g, const Adj3 a) {
+// The pressure update's transpose at one face (computed faces: vx for i in
+// [0, X] with j, k interior; vy for j in [0, Y]; vz for k in [0, Z]).
+__device__ __forceinline__ double adj3_lxt(const Grid3& g, const Adj3& a, int i, int j, int k) {
   const Frame3& f = g.f;
-  int i, j, k;
-  if (!frame_pos(f, blockIdx.x * (long)blockDim.x + threadIdx.x, i, j, k)) return;
-  const int X = f.X, Y = f.Y, Z = f.Z;
   const long q = f.idx(i, j, k);
-  const double c = -g.s3p;
-  if (i <= X && j >= 1 && j <= Y && k >= 1 && k <= Z)
-    a.LX[q] += c * g.rdx * (g.pbx[i] * a.MX[q] - g.pbx[i + 1] * a.MX[f.idx(i + 1, j, k)]);
-  if (j <= Y && i >= 1 && i <= X && k >= 1 && k <= Z)
-    a.LY[q] += c * g.rdy * (g.pby[j] * a.MY[q] - g.pby[j + 1] * a.MY[f.idx(i, j + 1, k)]);
-  if (k <= Z && i >= 1 && i <= X && j >= 1 && j <= Y)
-    a.LZ[q] += c * g.rdz * (g.pbz[k] * a.MZ[q] - g.pbz[k + 1] * a.MZ[f.idx(i, j, k + 1)]);
+  return a.LX[q] + (-g.s3p) * g.rdx * (g.pbx[i] * a.MX[q] - g.pbx[i + 1] * a.MX[f.idx(i + 1, j, k)]);
+}
+__device__ __forceinline__ double adj3_lyt(const Grid3& g, const Adj3& a, int i, int j, int k) {
+  const Frame3& f = g.f;
+  const long q = f.idx(i, j, k);
+  return a.LY[q] + (-g.s3p) * g.rdy * (g.pby[j] * a.MY[q] - g.pby[j + 1] * a.MY[f.idx(i, j + 1, k)]);
+}
+__device__ __forceinline__ double adj3_lzt(const Grid3& g, const Adj3& a, int i, int j, int k) {
+  const Frame3& f = g.f;
+  const long q = f.idx(i, j, k);
+  return a.LZ[q] + (-g.s3p) * g.rdz * (g.pbz[k] * a.MZ[q] - g.pbz[k + 1] * a.MZ[f.idx(i, j, k + 1)]);
 }
 
-__global__ void adj3_cells(const __grid_constant__ Grid3 g, const Adj3 a) {
+// One reverse step after adj3_source, from `in` into `out`; p0 (the focal
+// pressures of the step before, or null) adds that step's objective term.
+// Blocks of 32 x 8 cells of one plane (blockIdx.z); each interior cell writes
+// its east, north and top faces, the first column, row and plane also the
+// 0 faces.
+__global__ void adj3_step(const __grid_constant__ Grid3 g, const Adj3 in, const Adj3 out, const Box3 b,
+                          const double* __restrict__ p0, double two_dt) {
   const Frame3& f = g.f;
-  int i, j, k;
-  if (!frame_pos(f, blockIdx.x * (long)blockDim.x + threadIdx.x, i, j, k)) return;
-  if (i < 1 || i > f.X || j < 1 || j > f.Y || k < 1 || k > f.Z) return;
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x, j = 1 + blockIdx.y * blockDim.y + threadIdx.y,
+            k = 1 + blockIdx.z;
+  if (i > f.X || j > f.Y || k > f.Z) return;
   const long q = f.idx(i, j, k);
-  const double lp0 = g.dt_rho * (g.rdx * (g.vbx[i + 1] * a.LX[q] - g.vbx[i] * a.LX[f.idx(i - 1, j, k)]) +
-                                 g.rdy * (g.vby[j + 1] * a.LY[q] - g.vby[j] * a.LY[f.idx(i, j - 1, k)]) +
-                                 g.rdz * (g.vbz[k + 1] * a.LZ[q] - g.vbz[k] * a.LZ[f.idx(i, j, k - 1)]));
-  a.MX[q] = g.pax[i] * a.MX[q] + lp0;
-  a.MY[q] = g.pay[j] * a.MY[q] + lp0;
-  a.MZ[q] = g.paz[k] * a.MZ[q] + lp0;
-}
-
-__global__ void adj3_vscale(const __grid_constant__ Grid3 g, const Adj3 a) {
-  const Frame3& f = g.f;
-  int i, j, k;
-  if (!frame_pos(f, blockIdx.x * (long)blockDim.x + threadIdx.x, i, j, k)) return;
-  const int X = f.X, Y = f.Y, Z = f.Z;
-  const long q = f.idx(i, j, k);
-  if (i <= X && j >= 1 && j <= Y && k >= 1 && k <= Z) a.LX[q] *= g.vax[i + 1] * g.vbx[i + 1];
-  if (j <= Y && i >= 1 && i <= X && k >= 1 && k <= Z) a.LY[q] *= g.vay[j + 1] * g.vby[j + 1];
-  if (k <= Z && i >= 1 && i <= X && j >= 1 && j <= Y) a.LZ[q] *= g.vaz[k + 1] * g.vbz[k + 1];
+  const double xe = adj3_lxt(g, in, i, j, k), xw = adj3_lxt(g, in, i - 1, j, k);
+  const double yn = adj3_lyt(g, in, i, j, k), ys = adj3_lyt(g, in, i, j - 1, k);
+  const double zt = adj3_lzt(g, in, i, j, k), zb = adj3_lzt(g, in, i, j, k - 1);
+  const double lp0 = g.dt_rho * (g.rdx * (g.vbx[i + 1] * xe - g.vbx[i] * xw) +
+                                 g.rdy * (g.vby[j + 1] * yn - g.vby[j] * ys) +
+                                 g.rdz * (g.vbz[k + 1] * zt - g.vbz[k] * zb));
+  double mx = g.pax[i] * in.MX[q] + lp0;
+  double my = g.pay[j] * in.MY[q] + lp0;
+  double mz = g.paz[k] * in.MZ[q] + lp0;
+  if (p0) {
+    const int bi = i - b.i0, bj = j - b.j0, bk = k - b.k0;
+    if (bi >= 0 && bi < b.nx && bj >= 0 && bj < b.ny && bk >= 0 && bk < b.nz) {
+      const long t = bi + (long)b.nx * (bj + (long)b.ny * bk);
+      const double w = b.w[t];
+      if (w != 0.0) {
+        const double d = two_dt * w * p0[t];
+        mx += d;
+        my += d;
+        mz += d;
+      }
+    }
+  }
+  out.MX[q] = mx;
+  out.MY[q] = my;
+  out.MZ[q] = mz;
+  out.LX[q] = xe * (g.vax[i + 1] * g.vbx[i + 1]);
+  out.LY[q] = yn * (g.vay[j + 1] * g.vby[j + 1]);
+  out.LZ[q] = zt * (g.vaz[k + 1] * g.vbz[k + 1]);
+  if (i == 1) out.LX[f.idx(0, j, k)] = xw * (g.vax[1] * g.vbx[1]);
+  if (j == 1) out.LY[f.idx(i, 0, k)] = ys * (g.vay[1] * g.vby[1]);
+  if (k == 1) out.LZ[f.idx(i, j, 0)] = zb * (g.vaz[1] * g.vbz[1]);
 }
 
 }  // namespace d3
@@ -1058,6 +1075,8 @@ struct Sim3Impl {
   crp_status read_field(crp_field w, double* host);
   crp_status read_bubbles(crp_bubble_field w, double* host);
   crp_status adjoint(const crp_objective* obj, double* J, double* grad_amp, double* grad_phase);
+  void* adj_ws = nullptr;  // crp_adjoint's device workspace, kept between calls
+  size_t adj_ws_bytes = 0;
   // Source cells (frame index, element) in frame order, and the focus the bowl's phases aim at.
   std::vector<long> src_list;
   std::vector<int> src_elem;
@@ -1080,6 +1099,7 @@ F32 Sim3Impl::view<F32>(void* p) const {
 }
 
 Sim3Impl::~Sim3Impl() {
+  if (adj_ws) cudaFree(adj_ws);
   if (ev_f0) cudaEventDestroy(ev_f0);
   if (ev_f1) cudaEventDestroy(ev_f1);
   if (pool) cudaFree(pool);
@@ -1667,26 +1687,38 @@ crp_status Sim3Impl::adjoint(const crp_objective* obj, double* J, double* grad_a
   if (hist_n * sizeof(double) > ((size_t)32 << 30))
     return fail(CRP_ERR_TOO_LARGE, "adjoint: focal history above 32 GiB (steps x focal cells)");
   const int ns = (int)src_list.size(), ns1 = std::max(ns, 1);
-  // Six adjoint frames, per-source-cell gradients, weights, history, objective
-  // per step; then the source cells' frame indices and elements.
-  const size_t n_doubles = 6 * cells + 2 * (size_t)ns1 + box_n + hist_n + (size_t)N;
+  // Two sets of six adjoint frames, per-source-cell gradients, weights,
+  // history, objective per step; then the source cells' frame indices and
+  // elements.
+  const size_t n_doubles = 12 * cells + 2 * (size_t)ns1 + box_n + hist_n + (size_t)N;
   const size_t bytes = n_doubles * sizeof(double) + (size_t)ns1 * (sizeof(long) + sizeof(int));
-  char* buf = nullptr;
-  if (cudaMalloc(&buf, bytes) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(CRP_ERR_ALLOC, "adjoint: device memory");
-  }
-  struct Free {  // on every return: let the queued work finish, then release the buffer
-    char* p;
-    cudaStream_t st;
-    ~Free() {
-      cudaStreamSynchronize(st);
-      cudaFree(p);
+  // The workspace is kept for the next call and released with the simulation.
+  if (adj_ws_bytes < bytes) {
+    if (adj_ws) {
+      C3(cudaStreamSynchronize(stream));
+      cudaFree(adj_ws);
+      adj_ws = nullptr;
+      adj_ws_bytes = 0;
     }
-  } guard{buf, stream};
+    if (cudaMalloc(&adj_ws, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      adj_ws = nullptr;
+      return fail(CRP_ERR_ALLOC, "adjoint: device memory");
+    }
+    adj_ws_bytes = bytes;
+  }
+  char* buf = static_cast<char*>(adj_ws);
+  struct Drain {  // on every return: the queued work has finished
+    cudaStream_t st;
+    ~Drain() { cudaStreamSynchronize(st); }
+  } guard{stream};
   double* base = reinterpret_cast<double*>(buf);
-  d3::Adj3 ad{base, base + cells, base + 2 * cells, base + 3 * cells, base + 4 * cells, base + 5 * cells};
-  double* gA = base + 6 * cells;
+  d3::Adj3 fr[2];
+  for (int s = 0; s < 2; s++) {
+    double* b = base + (size_t)s * 6 * cells;
+    fr[s] = d3::Adj3{b, b + cells, b + 2 * cells, b + 3 * cells, b + 4 * cells, b + 5 * cells};
+  }
+  double* gA = base + 12 * cells;
   double* gP = gA + ns1;
   double* d_w = gP + ns1;
   double* hist = d_w + box_n;
@@ -1727,19 +1759,22 @@ crp_status Sim3Impl::adjoint(const crp_objective* obj, double* J, double* grad_a
   double Jsum = 0.0;
   for (int n = 0; n < N; n++) Jsum += Jn[n];
   if (J) *J = g.dt * Jsum;
-  // Reverse sweep.
-  const long npos = (long)(f.X + 2) * (f.Y + 2) * (f.Z + 2);
-  const int gb = (int)((npos + 255) / 256), sb = (ns + 255) / 256;
+  // Reverse sweep: reverse step n reads frame set s and writes set s ^ 1.
+  const dim3 sblk(32, 8), sgrid((f.X + 31) / 32, (f.Y + 7) / 8, f.Z);
+  const int sb = (ns + 255) / 256;
   const double two_dt = 2.0 * g.dt;
-  d3::adj3_force<<<rb, 256, 0, stream>>>(f, ad, box, hist + (size_t)(N - 1) * box_n, two_dt);
-  for (int n = N; n >= 1; n--) {
-    if (ns > 0) d3::adj3_source<<<sb, 256, 0, stream>>>(g, ad, d_cells, d_el, ns, times[n], gA, gP);
-    d3::adj3_faces<<<gb, 256, 0, stream>>>(g, ad);
-    d3::adj3_cells<<<gb, 256, 0, stream>>>(g, ad);
-    d3::adj3_vscale<<<gb, 256, 0, stream>>>(g, ad);
-    if (n >= 2) d3::adj3_force<<<rb, 256, 0, stream>>>(f, ad, box, hist + (size_t)(n - 2) * box_n, two_dt);
+  d3::adj3_force<<<rb, 256, 0, stream>>>(f, fr[0], box, hist + (size_t)(N - 1) * box_n, two_dt);
+  launches++;
+  int s = 0;
+  for (int n = N; n >= 1; n--, s ^= 1) {
+    if (ns > 0) {
+      d3::adj3_source<<<sb, 256, 0, stream>>>(g, fr[s], d_cells, d_el, ns, times[n], gA, gP);
+      launches++;
+    }
+    const double* p0 = n >= 2 ? hist + (size_t)(n - 2) * box_n : nullptr;
+    d3::adj3_step<<<sgrid, sblk, 0, stream>>>(g, fr[s], fr[s ^ 1], box, p0, two_dt);
     C3(cudaGetLastError());
-    launches += 5;
+    launches++;
   }
   if (elem_n > 0 && ns > 0) {
     std::vector<double> ca(ns), cp(ns);

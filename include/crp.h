@@ -504,7 +504,9 @@ crp_status crp_batch_tune(crp_batch* batch, int32_t trial_steps, crp_batch_tunin
  * bowl's phases aim at, w = dx dy dz (the bowl's source cells excluded), and
  * the parameters are the ext.array_elements elements' amplitude factors and
  * phases (crp_set_source_elements sets them; the phases are absolute there,
- * the focusing delays included). */
+ * the focusing delays included).  The call's device workspace (the adjoint
+ * fields and the focal record) stays allocated for the next call and is
+ * released by crp_destroy. */
 typedef struct crp_objective {
   int32_t steps;        /* mixture steps to run and differentiate over */
   double focal_radius;  /* [m] radius of the focal region around the source's focus */
