@@ -1,6 +1,7 @@
 """Edge cases of the snapshot, tuning and batch entry points: invalid values
 are refused with CRP_ERR_INVALID and change nothing; a radius-kernel width
-above the occupancy limit is clamped; an empty bubble population runs."""
+above the occupancy limit is clamped; an empty bubble population runs; a
+non-finite pressure is reported whether the steps run one per call or queued."""
 import numpy as np
 import pytest
 
@@ -10,6 +11,7 @@ import crp
 pytestmark = pytest.mark.gpu
 
 INVALID = 1
+NONFINITE = 7
 
 
 def test_tuning_values():
@@ -64,3 +66,21 @@ def test_empty_bubble_population():
         sim.load_state(snap)
         sim.step(10)
         assert np.array_equal(p, sim.field("p0"))
+
+
+@pytest.mark.parametrize("per_call", [1, 40])
+def test_non_finite_pressure_is_reported(per_call):
+    # Bubbles off, so no memory index depends on a field value.  After a first
+    # finite step the element amplitudes overflow the source (1e308 x the
+    # surface pressure): the source row becomes infinite, its neighbours
+    # inf - inf = NaN.  Steps without bubbles run queued when more than one is
+    # asked for, and their scalars are read once at the end.
+    cfg = B.small_config(bub_enable=0, ext_elements=4)
+    with crp.Sim(cfg) as sim:
+        sim.step(1)
+        sim.set_source_elements(np.full(4, 1e308), np.zeros(4))
+        with pytest.raises(crp.CrpError) as e:
+            for _ in range(120 // per_call):
+                sim.step(per_call)
+        assert e.value.status == NONFINITE
+        assert not np.isfinite(sim.field("p0")).all()

@@ -13,7 +13,9 @@ once the cloud is driven (R/R0 > 20): 5e-8 at step 1100, 1e-3 at 1200; both
 stop with CRP_ERR_PICARD at step 1220.  The mixed form's focal-pressure error
 is 5e-7 at the focal arrival and 4e-5 fifty steps later (the 1e-4 target), and
 grows past it from step 1060; it stops at step 1172 (its Picard threshold is
-1e-5, since FP32 storage of f_g leaves a residual floor near 7e-7).
+1e-5, since FP32 storage of f_g leaves a residual floor near 7e-7).  FP64 runs
+whose bubble radii or positions differ by one FP32 rounding diverge from the
+FP64 run as fast as the mixed form does.
 
 The 1024 x 2048 workload (axisym_1024x2048, 262144 bubbles) is compared over a bounded
 window from t = 0, the oracle's time being about 0.1 s per step; so is the 3-D
@@ -125,6 +127,47 @@ def test_256x512_mixed_focal_error_at_arrival(run_256x512):
     for step in (FOCAL_ARRIVAL, 1050):
         r = run_256x512["records"][step]["mixed"]
         assert r["focal_l2"] < 1e-4, (step, r)
+
+
+def test_256x512_mixed_error_is_amplified_fp32_sized_differences():
+    # After the focal arrival the driven cloud amplifies any difference about
+    # tenfold per ten steps.  FP64 runs whose bubble radii or positions differ
+    # from the workload's by one FP32 rounding (a factor 1 + 2^-24) leave the
+    # unperturbed FP64 run as fast as the mixed form does (measured focal
+    # rel. L2 against the FP64 run: mixed 3.5e-5 / 2.8e-3 / 1.3e-2 at steps
+    # 1050 / 1075 / 1100; radii x (1 + 2^-24) 4.4e-5 / 9.6e-4 / 3.2e-3;
+    # positions 2.2e-5 / 2.5e-3 / 5.5e-3), and a 2^-40 difference grows the
+    # same way from a 1e5-fold smaller start (1.3e-7 at step 1100).  The
+    # mixed form's error past the 1e-4 target is therefore what FP32-sized
+    # differences become in this flow, not a fault of the mixed arithmetic.
+    path = os.path.join(CONF, "axisym_256x512.conf")
+    cfg = crp.parse_file(path)
+    bub = crp.seed_bubbles(cfg)
+    mcfg = crp.Config.from_buffer_copy(cfg)
+    mcfg.ext_precision = 1
+
+    def perturbed(fx=1.0, fr=1.0):
+        return crp.Bubbles(bub.x * fx, bub.y.copy(), bub.r0 * fr, bub.n_b.copy(), None)
+
+    sims = {"fp64": crp.Sim(cfg, bub), "mixed": crp.Sim(mcfg, bub),
+            "r0_2^-24": crp.Sim(cfg, perturbed(fr=1.0 + 2.0 ** -24)),
+            "x_2^-24": crp.Sim(cfg, perturbed(fx=1.0 + 2.0 ** -24)),
+            "r0_2^-40": crp.Sim(cfg, perturbed(fr=1.0 + 2.0 ** -40))}
+    try:
+        mask = focal_mask(sims["fp64"].dims, cfg)
+        for step in (1050, 1075, 1100):
+            for sim in sims.values():
+                sim.step(step - int(sim.stats().steps))
+            base = sims["fp64"].field("p0")[mask]
+            err = {k: rel_l2(s.field("p0")[mask], base) for k, s in sims.items() if k != "fp64"}
+            print("256x512 focal rel. L2 against the FP64 run at step", step, err)
+            fp32_sized = max(err["r0_2^-24"], err["x_2^-24"])
+            assert err["mixed"] / 10 <= fp32_sized <= 10 * err["mixed"], (step, err)
+            assert err["r0_2^-40"] < 1e-3 * fp32_sized, (step, err)
+        assert fp32_sized > 1e-4  # such differences alone pass the mixed target
+    finally:
+        for sim in sims.values():
+            sim.close()
 
 
 def test_1024x2048_fp64_window_matches_oracle():
