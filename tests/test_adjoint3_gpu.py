@@ -137,3 +137,22 @@ def test_bubbles_are_unsupported():
         with pytest.raises(crp.CrpError) as e:
             sim.adjoint(10, RADIUS, ELEMS)
         assert e.value.status == 2  # CRP_ERR_UNSUPPORTED
+
+
+def test_repeated_calls_reuse_the_workspace():
+    # As on the 2-D grid: the kept workspace, grown and then reused, gives
+    # each call exactly what a fresh handle stepped to the same state gives.
+    cfg = _cfg()
+    amp, _ = _params()
+    with crp.Sim(cfg) as a:
+        a.set_source_elements(amp, default_phases(cfg))
+        got = [a.adjoint(steps, RADIUS, ELEMS) for steps in (30, 60, 20)]
+    before = 0
+    for steps, (J, ga, gp) in zip((30, 60, 20), got):
+        with crp.Sim(cfg) as b:
+            b.set_source_elements(amp, default_phases(cfg))
+            if before:
+                b.step(before)
+            Jb, gab, gpb = b.adjoint(steps, RADIUS, ELEMS)
+        assert J == Jb and np.array_equal(ga, gab) and np.array_equal(gp, gpb), steps
+        before += steps

@@ -172,3 +172,25 @@ def test_mixed_path_forward_gives_the_same_gradient():
     assert abs(Jmx - J64) <= 1e-6 * J64
     assert np.abs(gamx - ga64).max() <= 1e-6 * scale
     assert np.abs(gpmx - gp64).max() <= 1e-6 * scale
+
+
+def test_repeated_calls_reuse_the_workspace():
+    # crp_adjoint keeps its device workspace with the handle.  Calls of 60,
+    # 120 and 40 steps (the workspace grows, then is reused larger than
+    # needed) each continue from the state the previous call left, and give
+    # exactly what a fresh handle advanced to that state by crp_step gives.
+    cfg = _cfg("ghost_row_focused")
+    amp, phase = _params(cfg.ext_elements)
+    n = cfg.ext_elements
+    with crp.Sim(cfg) as a:
+        a.set_source_elements(amp, phase)
+        got = [a.adjoint(steps, RADIUS, n) for steps in (60, 120, 40)]
+    before = 0
+    for steps, (J, ga, gp) in zip((60, 120, 40), got):
+        with crp.Sim(cfg) as b:
+            b.set_source_elements(amp, phase)
+            if before:
+                b.step(before)
+            Jb, gab, gpb = b.adjoint(steps, RADIUS, n)
+        assert J == Jb and np.array_equal(ga, gab) and np.array_equal(gp, gpb), steps
+        before += steps
