@@ -797,14 +797,15 @@ __device__ __forceinline__ void store_contrib(const GridParams& g, const BubbleP
 // while the queue has work.  Each bubble's arithmetic is the same as a
 // thread-per-bubble solve, so results do not depend on the schedule.
 constexpr int kRpThreads = 128;
-// Resident blocks per SM the register budget is set for: 6 for the FP64 path
-// (at most 85 registers a thread), 5 for the mixed path (102): more warps to
+// Resident blocks per SM the register budget is set for: 7 for the FP64 path
+// (at most 73 registers a thread), 5 for the mixed path (102): more warps to
 // hide the FP64 latency chains of the sub-step, measured faster than fewer
-// warps with more registers despite a few spilled values (the mixed path's
-// FP32 thermal model gains nothing from the sixth block).
+// warps with more registers despite the spilled values (FP64, 1024 x 2048
+// quiet phase, per 100 steps: radius solve 17.2 ms at 7 blocks, 17.9 at 6,
+// 17.5 at 5; the mixed path's FP32 thermal model gains nothing from a sixth).
 template <typename P>
 constexpr int rp_min_blocks() {
-  return sizeof(typename P::T) == sizeof(double) ? 6 : 5;
+  return sizeof(typename P::T) == sizeof(double) ? 7 : 5;
 }
 
 // Lanes whose claimed bubble kept its last solve (n == -2) are counted, one
