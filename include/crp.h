@@ -279,7 +279,11 @@ crp_status crp_seed_bubbles3(const crp_config* cfg, double* x, double* y, double
  * stream may be NULL (a stream is created) or a cudaStream_t to run on. */
 crp_status crp_create(const crp_config* cfg, const crp_bubbles_in* bubbles, void* stream, crp_sim** out);
 
-/* Advance n mixture time steps.  Blocks until they are done. */
+/* Advance n mixture time steps.  Blocks until they are done.  Without bubbles
+ * (and without the temperature branch or profiling) the steps after the first
+ * are queued back to back and their state is checked once, after the last: a
+ * non-finite pressure is then reported (CRP_ERR_NONFINITE) at the end of the
+ * call, with the step count including every queued step. */
 crp_status crp_step(crp_sim* sim, int32_t n);
 
 crp_status crp_get_dims(const crp_sim* sim, crp_dims* dims);
